@@ -1,0 +1,303 @@
+// Dense FP64 kernels for the coarsest multigrid level (sm_100a).
+//
+// The reference factors its coarsest Galerkin matrix with cuDSS (sparse FP64
+// Cholesky, deep_frame/topology_multigrid.py:230-283).  Here the coarsest grid
+// is kept small (a few thousand dofs), factored once per hierarchy by a blocked
+// right-looking Cholesky, and the factor is inverted (X = L^-1).  Every
+// coarsest solve in a V-cycle is then two triangular matrix products,
+// x = X^T (X b), one launch each, instead of 2 * n / NB dependent substitution
+// steps.
+#include "tf_common.h"
+#include "tf_dense.h"
+
+namespace tfb {
+
+namespace {
+constexpr int NB = 32;     // panel width
+constexpr int TILE = 64;   // syrk / product tile
+
+// Factor the NB x NB diagonal block at (k0, k0) in place (lower).
+__global__ void potrf_diag_kernel(double* A, int n, int k0, int* info) {
+  __shared__ double s[NB][NB + 1];
+  const int nb = min(NB, n - k0);
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t % nb;
+    s[r][c] = A[(long long)(k0 + r) * n + k0 + c];
+  }
+  __syncthreads();
+  for (int k = 0; k < nb; ++k) {
+    if (threadIdx.x == 0) {
+      const double d = s[k][k];
+      if (!(d > 0.0)) {
+        if (*info == 0) *info = k0 + k + 1;
+        s[k][k] = 1.0;
+      } else {
+        s[k][k] = sqrt(d);
+      }
+    }
+    __syncthreads();
+    for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) s[r][k] /= s[k][k];
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+      const int r = t / nb, c = t % nb;
+      if (r > k && c > k && c <= r) s[r][c] -= s[r][k] * s[c][k];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t % nb;
+    A[(long long)(k0 + r) * n + k0 + c] = (c <= r) ? s[r][c] : 0.0;
+  }
+}
+
+// Rows below the diagonal block: A[i, k0:k0+nb] <- A[i, k0:k0+nb] L_kk^-T.
+__global__ void trsm_panel_kernel(double* A, int n, int k0) {
+  __shared__ double L[NB][NB + 1];
+  const int nb = min(NB, n - k0);
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t % nb;
+    L[r][c] = A[(long long)(k0 + r) * n + k0 + c];
+  }
+  __syncthreads();
+  for (int i = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double x[NB];
+    double* row = A + (long long)i * n + k0;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) x[c] = (c < nb) ? row[c] : 0.0;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+      if (c < nb) {
+        double v = x[c];
+#pragma unroll
+        for (int t = 0; t < NB; ++t)
+          if (t < c) v -= x[t] * L[c][t];
+        x[c] = v / L[c][c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+      if (c < nb) row[c] = x[c];
+  }
+}
+
+// Trailing update of the lower triangle: A[i][j] -= sum_t P[i][t] P[j][t], i >= j >= k0 + nb.
+__global__ void __launch_bounds__(256) syrk_update_kernel(double* A, int n, int k0) {
+  const int nb = min(NB, n - k0);
+  const int start = k0 + nb;
+  const int m = n - start;
+  const int tiles = (m + TILE - 1) / TILE;
+  // map blockIdx.x to a lower-triangular tile pair (ti >= tj)
+  int b = blockIdx.x, ti = 0;
+  while (b >= ti + 1) { b -= ti + 1; ++ti; }
+  const int tj = b;
+  if (ti >= tiles) return;
+  __shared__ double Pi[TILE][NB + 1];
+  __shared__ double Pj[TILE][NB + 1];
+  const int i0 = start + ti * TILE, j0 = start + tj * TILE;
+  for (int t = threadIdx.x; t < TILE * NB; t += blockDim.x) {
+    const int r = t / NB, c = t % NB;
+    Pi[r][c] = (i0 + r < n && c < nb) ? A[(long long)(i0 + r) * n + k0 + c] : 0.0;
+    Pj[r][c] = (j0 + r < n && c < nb) ? A[(long long)(j0 + r) * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  const int tr = (threadIdx.x / 16) * 4, tc = (threadIdx.x % 16) * 4;
+  double acc[4][4] = {};
+  for (int t = 0; t < NB; ++t) {
+    double a[4], bb[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { a[q] = Pi[tr + q][t]; bb[q] = Pj[tc + q][t]; }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * bb[q];
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int i = i0 + tr + p;
+    if (i >= n) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = j0 + tc + q;
+      if (j >= n || j > i) continue;
+      A[(long long)i * n + j] -= acc[p][q];
+    }
+  }
+}
+
+// Invert every NB x NB lower-triangular diagonal block of L into X.
+__global__ void trinv_diag_kernel(const double* L, double* X, int n) {
+  __shared__ double s[NB][NB + 1];
+  __shared__ double x[NB][NB + 1];
+  const int k0 = blockIdx.x * NB;
+  const int nb = min(NB, n - k0);
+  for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+    const int r = t / NB, c = t % NB;
+    s[r][c] = (r < nb && c < nb) ? L[(long long)(k0 + r) * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  // column c of the inverse by forward substitution (one thread per column)
+  for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+    for (int r = 0; r < nb; ++r) {
+      double v = (r == c) ? 1.0 : 0.0;
+      for (int t = c; t < r; ++t) v -= s[r][t] * x[t][c];
+      x[r][c] = (r < c) ? 0.0 : v / s[r][r];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t % nb;
+    X[(long long)(k0 + r) * n + k0 + c] = x[r][c];
+  }
+}
+
+// Block row bi of X = L^-1:  X[bi][bj] = -X[bi][bi] * sum_{bk=bj}^{bi-1} L[bi][bk] X[bk][bj]  (one CTA per bj < bi).
+__global__ void __launch_bounds__(256) trinv_row_kernel(const double* L, double* X, int n, int bi) {
+  const int bj = blockIdx.x;
+  __shared__ double La[NB][NB + 1];
+  __shared__ double Xb[NB][NB + 1];
+  __shared__ double S[NB][NB + 1];
+  const int i0 = bi * NB, j0 = bj * NB;
+  const int ni = min(NB, n - i0);
+  // each thread owns 4 entries of the NB x NB tile
+  double acc[4] = {0, 0, 0, 0};
+  for (int bk = bj; bk < bi; ++bk) {
+    const int k0 = bk * NB;
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+      const int r = t / NB, c = t % NB;
+      La[r][c] = (r < ni) ? L[(long long)(i0 + r) * n + k0 + c] : 0.0;
+      Xb[r][c] = X[(long long)(k0 + r) * n + j0 + c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t = threadIdx.x + q * 256;
+      const int r = t / NB, c = t % NB;
+      double v = 0.0;
+#pragma unroll 8
+      for (int kk = 0; kk < NB; ++kk) v += La[r][kk] * Xb[kk][c];
+      acc[q] += v;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int t = threadIdx.x + q * 256;
+    S[t / NB][t % NB] = acc[q];
+  }
+  // diagonal inverse of block bi
+  for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+    const int r = t / NB, c = t % NB;
+    La[r][c] = (r < ni && c < ni) ? X[(long long)(i0 + r) * n + i0 + c] : 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int t = threadIdx.x + q * 256;
+    const int r = t / NB, c = t % NB;
+    if (r >= ni) continue;
+    double v = 0.0;
+    for (int kk = 0; kk <= r; ++kk) v += La[r][kk] * S[kk][c];
+    X[(long long)(i0 + r) * n + j0 + c] = -v;
+  }
+}
+
+// C[c][i] = sum_k op(X)[i][k] B[c][k] for a lower-triangular X (op = identity or transpose).
+// Columns of B and C are contiguous ([ncol][n]).  Inactive columns are skipped.
+__global__ void __launch_bounds__(256) trimul_kernel(const double* X, const double* B, double* C, int n, int ncol,
+                                                     int transpose, const int* active, const int* colmap) {
+  // tile: 64 rows x 8 columns, K in chunks of 32
+  __shared__ double As[64][33];
+  __shared__ double Bs[8][33];
+  const int r0 = blockIdx.x * 64;
+  const int c0 = blockIdx.y * 8;
+  const int tr = threadIdx.x / 4;        // 0..63 row in tile
+  const int tc = (threadIdx.x % 4) * 2;  // 0,2,4,6 column pair
+  bool any = false;
+  for (int c = c0; c < min(c0 + 8, ncol); ++c) any |= (!active || active[colmap ? colmap[c] : c]);
+  if (!any) return;
+  double acc0 = 0.0, acc1 = 0.0;
+  // lower-triangular X: row i uses k <= i; X^T row i uses k >= i
+  const int kbeg = transpose ? r0 : 0;
+  const int kend = transpose ? n : min(n, r0 + 64);
+  for (int k0 = (kbeg / 32) * 32; k0 < kend; k0 += 32) {
+    for (int t = threadIdx.x; t < 64 * 32; t += blockDim.x) {
+      // keep the global reads contiguous: k fastest for X, row fastest for X^T
+      const int r = transpose ? t % 64 : t / 32;
+      const int k = transpose ? t / 64 : t % 32;
+      const int i = r0 + r, kk = k0 + k;
+      double v = 0.0;
+      if (i < n && kk < n) v = transpose ? X[(long long)kk * n + i] : X[(long long)i * n + kk];
+      As[r][k] = v;
+    }
+    for (int t = threadIdx.x; t < 8 * 32; t += blockDim.x) {
+      const int c = t / 32, k = t % 32;
+      const int col = c0 + c, kk = k0 + k;
+      Bs[c][k] = (col < ncol && kk < n) ? B[(long long)col * n + kk] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const double a = As[tr][k];
+      acc0 += a * Bs[tc][k];
+      acc1 += a * Bs[tc + 1][k];
+    }
+    __syncthreads();
+  }
+  const int i = r0 + tr;
+  if (i < n) {
+    if (c0 + tc < ncol) C[(long long)(c0 + tc) * n + i] = acc0;
+    if (c0 + tc + 1 < ncol) C[(long long)(c0 + tc + 1) * n + i] = acc1;
+  }
+}
+
+__global__ void symmetrize_kernel(double* A, int n) {
+  const long long total = (long long)n * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(t / n), j = static_cast<int>(t % n);
+    if (j < i) {
+      const double v = 0.5 * (A[(long long)i * n + j] + A[(long long)j * n + i]);
+      A[(long long)i * n + j] = v;
+      A[(long long)j * n + i] = v;
+    }
+  }
+}
+}  // namespace
+
+void dense_symmetrize(double* A, int n, cudaStream_t s) {
+  symmetrize_kernel<<<grid_for((long long)n * n, 256), 256, 0, s>>>(A, n);
+  TF_LAUNCH_CHECK("symmetrize_kernel");
+}
+
+void dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s) {
+  for (int k0 = 0; k0 < n; k0 += NB) {
+    potrf_diag_kernel<<<1, 256, 0, s>>>(A, n, k0, info_dev);
+    TF_LAUNCH_CHECK("potrf_diag_kernel");
+    const int below = n - k0 - NB;
+    if (below <= 0) break;
+    trsm_panel_kernel<<<grid_for(below, 128, 4096), 128, 0, s>>>(A, n, k0);
+    TF_LAUNCH_CHECK("trsm_panel_kernel");
+    const int tiles = (below + TILE - 1) / TILE;
+    syrk_update_kernel<<<tiles * (tiles + 1) / 2, 256, 0, s>>>(A, n, k0);
+    TF_LAUNCH_CHECK("syrk_update_kernel");
+  }
+}
+
+void dense_trinv(const double* L, double* X, int n, cudaStream_t s) {
+  TF_CUDA_CHECK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, s));
+  const int blocks = (n + NB - 1) / NB;
+  trinv_diag_kernel<<<blocks, 64, 0, s>>>(L, X, n);
+  TF_LAUNCH_CHECK("trinv_diag_kernel");
+  for (int bi = 1; bi < blocks; ++bi) {
+    trinv_row_kernel<<<bi, 256, 0, s>>>(L, X, n, bi);
+    TF_LAUNCH_CHECK("trinv_row_kernel");
+  }
+}
+
+void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active,
+                  cudaStream_t s) {
+  dim3 grid((n + 63) / 64, (ncol + 7) / 8);
+  trimul_kernel<<<grid, 256, 0, s>>>(X, B, C, n, ncol, transpose, active, nullptr);
+  TF_LAUNCH_CHECK("trimul_kernel");
+}
+
+}  // namespace tfb

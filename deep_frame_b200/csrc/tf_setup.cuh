@@ -1,0 +1,642 @@
+// Hierarchy set-up kernels and the device-side PCG vector kernels.
+#pragma once
+#include "tf_kernels.cuh"
+
+namespace tfb {
+
+constexpr int RED_THREADS = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide reduction of two values (op 0 = sum, 1 = max); result valid in thread 0.
+template <int OP0, int OP1>
+__device__ __forceinline__ void block_reduce2(double& a, double& b) {
+  __shared__ double sa[RED_THREADS / 32], sb[RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  a = OP0 ? warp_max(a) : warp_sum(a);
+  b = OP1 ? warp_max(b) : warp_sum(b);
+  if (lane == 0) { sa[warp] = a; sb[warp] = b; }
+  __syncthreads();
+  if (warp == 0) {
+    a = lane < RED_THREADS / 32 ? sa[lane] : 0.0;
+    b = lane < RED_THREADS / 32 ? sb[lane] : 0.0;
+    a = OP0 ? warp_max(a) : warp_sum(a);
+    b = OP1 ? warp_max(b) : warp_sum(b);
+  }
+  __syncthreads();
+}
+
+// Deterministic cross-block combine: every block stores its partial; the last
+// block of the column sums the partials in block order.  Returns true in
+// thread 0 of the last block, with the totals in a, b.
+template <int OP0, int OP1>
+__device__ __forceinline__ bool last_block_combine(double& a, double& b, double* partial, unsigned* count, int col) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    double* p = partial + 2 * ((long long)col * gridDim.x + blockIdx.x);
+    p[0] = a;
+    p[1] = b;
+    __threadfence();
+    const unsigned t = atomicAdd(&count[col], 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  if (threadIdx.x != 0) return false;
+  __threadfence();
+  double ta = OP0 ? 0.0 : 0.0, tb = 0.0;
+  const double* p = partial + 2 * (long long)col * gridDim.x;
+  for (unsigned q = 0; q < gridDim.x; ++q) {
+    const double pa = __ldcg(p + 2 * q), pb = __ldcg(p + 2 * q + 1);
+    ta = OP0 ? fmax(ta, pa) : ta + pa;
+    tb = OP1 ? fmax(tb, pb) : tb + pb;
+  }
+  count[col] = 0;
+  a = ta;
+  b = tb;
+  return true;
+}
+
+struct PcgState {
+  double* bnorm;
+  double* rho;
+  double* alpha;
+  double* rel;
+  double* scale;
+  double* rzo;
+  double* beta;
+  int* active;
+  int* cand;
+  int* iters;
+  int* flags;              // [0] any candidate this step, [1] number of active columns
+  unsigned long long* hist;  // bit patterns of non-negative doubles, one per step
+  double* partial;         // [ncol][blocks][2]
+  unsigned* count;         // [ncol]
+  int ncol;
+};
+
+// ---------------------------------------------------------------- set-up ----
+
+// Live-dof mask of the finest level: a node is live when an adjacent element
+// has E > 0 (topology_multigrid.py:138-144); fixed dofs are cleared.
+__global__ void fine_mask_kernel(Geo g, const double* __restrict__ E, const uint8_t* __restrict__ fixedbits,
+                                 uint8_t* __restrict__ mask) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nnode; n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_coords(n, g, i, j, k);
+    bool live = false;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int ei = i - 1 + (e >> 2), ej = j - 1 + ((e >> 1) & 1), ek = k - 1 + (e & 1);
+      if ((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez)
+        live |= E[((long long)ei * g.ey + ej) * g.ez + ek] > 0.0;
+    }
+    mask[n] = live ? static_cast<uint8_t>(7u & ~static_cast<unsigned>(fixedbits[n])) : uint8_t(0);
+  }
+}
+
+// Diagonal of the finest operator, sum_e E_e K0_ii (topology_multigrid.py:118-124), times the mask.
+__global__ void fine_diag_kernel(Geo g, const double* __restrict__ E, const uint8_t* __restrict__ mask,
+                                 const double* __restrict__ k0diag, double* __restrict__ diag) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nnode; n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_coords(n, g, i, j, k);
+    double d[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+      const int ei = i - 1 + ox, ej = j - 1 + oy, ek = k - 1 + oz;
+      if ((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez) {
+        const double w = E[((long long)ei * g.ey + ej) * g.ez + ek];
+        const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) d[a] += w * k0diag[3 * cn + a];
+      }
+    }
+    const unsigned m = mask[n];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) diag[3 * n + a] = ((m >> a) & 1u) ? d[a] : 0.0;
+  }
+}
+
+// Diagonal of a Galerkin level: sum_e B_e[ii].
+__global__ void block_diag_kernel(Geo g, const double* __restrict__ B, double* __restrict__ diag) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nnode; n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_coords(n, g, i, j, k);
+    double d[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+      const int ei = i - 1 + ox, ej = j - 1 + oy, ek = k - 1 + oz;
+      if ((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez) {
+        const double* b = B + (((long long)ei * g.ey + ej) * g.ez + ek) * 576;
+        const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) d[a] += b[(3 * cn + a) * 25];
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) diag[3 * n + a] = d[a];
+  }
+}
+
+// max over an array (single column reduction into out[0])
+__global__ void amax_kernel(const double* __restrict__ v, long long n, double* partial, unsigned* count, double* out) {
+  double a = 0.0, b = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    a = fmax(a, fabs(v[t]));
+  block_reduce2<1, 0>(a, b);
+  if (last_block_combine<1, 0>(a, b, partial, count, 0)) out[0] = a;
+}
+
+// Dead-dof mask and inverse diagonal of a Galerkin level (topology_multigrid.py:180-186).
+template <typename T>
+__global__ void coarse_mask_inv_kernel(long long nnode, const double* __restrict__ diag, const double* __restrict__ dmax,
+                                       double ratio, uint8_t* __restrict__ mask, double* __restrict__ inv64, T* __restrict__ invw) {
+  const double thr = ratio * dmax[0];
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < nnode; n += (long long)gridDim.x * blockDim.x) {
+    unsigned m = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double d = diag[3 * n + a];
+      const bool live = d > thr;
+      m |= live ? (1u << a) : 0u;
+      const double iv = live ? 1.0 / (d > 0.0 ? d : 1.0) : 0.0;
+      inv64[3 * n + a] = iv;
+      if (invw) invw[3 * n + a] = static_cast<T>(iv);
+    }
+    mask[n] = static_cast<uint8_t>(m);
+  }
+}
+
+template <typename T>
+__global__ void fine_inv_kernel(long long nnode, const double* __restrict__ diag, const uint8_t* __restrict__ mask,
+                                double* __restrict__ inv64, T* __restrict__ invw) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < nnode; n += (long long)gridDim.x * blockDim.x) {
+    const unsigned m = mask[n];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double d = diag[3 * n + a];
+      const double iv = ((m >> a) & 1u) ? 1.0 / (d > 0.0 ? d : 1.0) : 0.0;
+      inv64[3 * n + a] = iv;
+      if (invw) invw[3 * n + a] = static_cast<T>(iv);
+    }
+  }
+}
+
+// Galerkin coarse blocks  B_C = sym( sum_c P_c^T K_c P_c )  (topology_multigrid.py:125-137,175-179).
+// P_c = W_c (x) I3 with W_c[r][s] the trilinear weight of coarse corner s at
+// child corner r.  From the finest level K_c = E_c g g^T o K0 (g = live mask of
+// the child's 24 dofs); children without a dead dof take the precomputed
+// Q_c = P_c^T K0 P_c.  Deeper levels use the previous level's blocks.
+struct GalerkinParam { double W[8][8][8]; };
+
+__global__ void __launch_bounds__(128) galerkin_kernel(const __grid_constant__ GalerkinParam P, Geo cg, Geo fg, int from_fine,
+                                                       const double* __restrict__ E, const uint8_t* __restrict__ fmask,
+                                                       const double* __restrict__ K0, const double* __restrict__ Q,
+                                                       const double* __restrict__ child_blocks, double* __restrict__ out) {
+  __shared__ double Kc[576];
+  __shared__ double Tm[576];
+  __shared__ double acc[576];
+  __shared__ int gbits[24];
+  __shared__ int fast;
+  const long long ncoarse = (long long)cg.ex * cg.ey * cg.ez;
+  for (long long ce = blockIdx.x; ce < ncoarse; ce += gridDim.x) {
+    const int K = static_cast<int>(ce % cg.ez);
+    const long long r1 = ce / cg.ez;
+    const int J = static_cast<int>(r1 % cg.ey);
+    const int I = static_cast<int>(r1 / cg.ey);
+    for (int t = threadIdx.x; t < 576; t += blockDim.x) acc[t] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < 8; ++c) {
+      const int fi = 2 * I + (c >> 2), fj = 2 * J + ((c >> 1) & 1), fk = 2 * K + (c & 1);
+      const long long fe = ((long long)fi * fg.ey + fj) * fg.ez + fk;
+      double Ec = 0.0;
+      if (from_fine) {
+        Ec = E[fe];
+        if (threadIdx.x < 24) {
+          const int corner = threadIdx.x / 3, comp = threadIdx.x % 3;
+          const int cx = (corner == 1 || corner == 2 || corner == 5 || corner == 6) ? 1 : 0;
+          const int cy = (corner == 2 || corner == 3 || corner == 6 || corner == 7) ? 1 : 0;
+          const int cz = corner >> 2;
+          const long long node = ((long long)(fi + cx) * fg.ny + (fj + cy)) * fg.nz + (fk + cz);
+          gbits[threadIdx.x] = (fmask[node] >> comp) & 1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          int all = 1;
+          for (int q = 0; q < 24; ++q) all &= gbits[q];
+          fast = all;
+        }
+        __syncthreads();
+        if (Ec == 0.0) { __syncthreads(); continue; }
+        if (fast) {
+          const double* q = Q + c * 576;
+          for (int t = threadIdx.x; t < 576; t += blockDim.x) acc[t] += Ec * q[t];
+          __syncthreads();
+          continue;
+        }
+        for (int t = threadIdx.x; t < 576; t += blockDim.x) {
+          const int a = t / 24, b = t % 24;
+          Kc[t] = (gbits[a] && gbits[b]) ? Ec * K0[t] : 0.0;
+        }
+      } else {
+        const double* src = child_blocks + fe * 576;
+        for (int t = threadIdx.x; t < 576; t += blockDim.x) Kc[t] = src[t];
+      }
+      __syncthreads();
+      // Tm = Kc P_c :  Tm[i][3s+y] = sum_r Kc[i][3r+y] W[c][r][s]
+      for (int t = threadIdx.x; t < 576; t += blockDim.x) {
+        const int i = t / 24, col = t % 24, s = col / 3, y = col % 3;
+        double v = 0.0;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v += Kc[i * 24 + 3 * r + y] * P.W[c][r][s];
+        Tm[t] = v;
+      }
+      __syncthreads();
+      // acc += P_c^T Tm :  acc[3s+x][j] += sum_r W[c][r][s] Tm[3r+x][j]
+      for (int t = threadIdx.x; t < 576; t += blockDim.x) {
+        const int row = t / 24, j = t % 24, s = row / 3, x = row % 3;
+        double v = 0.0;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v += P.W[c][r][s] * Tm[(3 * r + x) * 24 + j];
+        acc[t] += v;
+      }
+      __syncthreads();
+    }
+    double* o = out + ce * 576;
+    for (int t = threadIdx.x; t < 576; t += blockDim.x) {
+      const int a = t / 24, b = t % 24;
+      o[t] = 0.5 * (acc[t] + acc[b * 24 + a]);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void cast_kernel(const double* __restrict__ src, T* __restrict__ dst, long long n) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    dst[t] = static_cast<T>(src[t]);
+}
+
+// Deterministic uniform(-0.5, 0.5) start vector of the power iteration, masked.
+__device__ __forceinline__ double hash_uniform(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename T>
+__global__ void power_init_kernel(long long nnode, const uint8_t* __restrict__ mask, T* __restrict__ v) {
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < nnode; n += (long long)gridDim.x * blockDim.x) {
+    const unsigned m = mask[n];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      v[3 * n + a] = ((m >> a) & 1u) ? static_cast<T>(hash_uniform(3 * n + a) - 0.5) : T(0);
+  }
+}
+
+// y <- inv o y, out = ||y||
+template <typename T>
+__global__ void power_scale_kernel(long long ndof, const T* __restrict__ inv, T* __restrict__ y, double* partial,
+                                   unsigned* count, double* out) {
+  double a = 0.0, b = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x) {
+    const T v = inv[t] * y[t];
+    y[t] = v;
+    a += (double)v * (double)v;
+  }
+  block_reduce2<0, 0>(a, b);
+  if (last_block_combine<0, 0>(a, b, partial, count, 0)) out[0] = sqrt(a);
+}
+
+template <typename T>
+__global__ void power_norm_kernel(long long ndof, const T* __restrict__ y, const double* __restrict__ est, T* __restrict__ v) {
+  const double s = 1.0 / est[0];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x)
+    v[t] = static_cast<T>((double)y[t] * s);
+}
+
+// Dense coarsest matrix of the live dofs, assembled node by node (deterministic).
+__global__ void coarsest_assemble_kernel(Geo g, const double* __restrict__ B, const int* __restrict__ live_of_dof,
+                                         const long long* __restrict__ live_dofs, int n, double* __restrict__ A) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long dof = live_dofs[t];
+    const long long node = dof / 3;
+    const int a = static_cast<int>(dof % 3);
+    int i, j, k;
+    node_coords(node, g, i, j, k);
+    double* row = A + t * (long long)n;
+    for (int di = -1; di <= 1; ++di)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int dk = -1; dk <= 1; ++dk) {
+          const int ni = i + di, nj = j + dj, nk = k + dk;
+          if (!((unsigned)ni < (unsigned)g.nx && (unsigned)nj < (unsigned)g.ny && (unsigned)nk < (unsigned)g.nz)) continue;
+          const long long m = ((long long)ni * g.ny + nj) * g.nz + nk;
+          double v[3] = {0.0, 0.0, 0.0};
+          for (int e = 0; e < 8; ++e) {
+            const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+            const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
+            if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
+            const int ei = i - 1 + ox, ej = j - 1 + oy, ek = k - 1 + oz;
+            if (!((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez)) continue;
+            const double* b = B + (((long long)ei * g.ey + ej) * g.ez + ek) * 576;
+            const int cn = corner_id(1 - ox, 1 - oy, 1 - oz), cm = corner_id(cx, cy, cz);
+            for (int q = 0; q < 3; ++q) v[q] += b[(3 * cn + a) * 24 + 3 * cm + q];
+          }
+          for (int q = 0; q < 3; ++q) {
+            const int col = live_of_dof[3 * m + q];
+            if (col >= 0) row[col] = v[q];
+          }
+        }
+  }
+}
+
+// gather live coarsest dofs of the active columns into FP64 [ncol][n]
+template <typename T>
+__global__ void coarsest_gather_kernel(const T* __restrict__ src, long long stride, const long long* __restrict__ live, int n,
+                                       double* __restrict__ dst, const int* __restrict__ active) {
+  const int col = blockIdx.y;
+  if (active && !active[col]) return;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    dst[(long long)col * n + t] = static_cast<double>(src[col * stride + live[t]]);
+}
+
+template <typename T>
+__global__ void coarsest_scatter_kernel(const double* __restrict__ src, const long long* __restrict__ live, int n,
+                                        T* __restrict__ dst, long long stride, const int* __restrict__ active) {
+  const int col = blockIdx.y;
+  if (active && !active[col]) return;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    dst[col * stride + live[t]] = static_cast<T>(src[(long long)col * n + t]);
+}
+
+// ----------------------------------------------------------- elementwise ----
+
+template <typename T>
+__global__ void zero_cols_kernel(T* __restrict__ v, long long stride, const int* __restrict__ active) {
+  const int col = blockIdx.y;
+  if (active && !active[col]) return;
+  T* p = v + col * stride;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < stride; t += (long long)gridDim.x * blockDim.x) p[t] = T(0);
+}
+
+// x = s * inv * b   (first Jacobi sweep from a zero guess)
+template <typename T>
+__global__ void jacobi_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x, T s,
+                                    const int* __restrict__ active) {
+  const int col = blockIdx.y;
+  if (active && !active[col]) return;
+  const long long off = (long long)col * ndof;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x)
+    x[off + t] = s * inv[t] * b[off + t];
+}
+
+// Chebyshev start from a zero guess: res = b, d = inv * res / theta, x = d.
+template <typename T>
+__global__ void cheb_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ res,
+                                  T* __restrict__ d, T* __restrict__ x, T inv_theta, int has_x, const int* __restrict__ active) {
+  const int col = blockIdx.y;
+  if (active && !active[col]) return;
+  const long long off = (long long)col * ndof;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x) {
+    const T r = has_x ? res[off + t] : b[off + t];
+    const T dv = inv[t] * r * inv_theta;
+    res[off + t] = r;
+    d[off + t] = dv;
+    x[off + t] = has_x ? x[off + t] + dv : dv;
+  }
+}
+
+// --------------------------------------------------------------- PCG -------
+
+constexpr int PCG_BLOCKS = 64;   // reduction blocks per column
+
+// bnorm = ||b||; r = b; x = 0 (or r = b - A x computed elsewhere)
+__global__ void pcg_norm_kernel(const double* __restrict__ b, long long n, PcgState st, double* out, int take_sqrt) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const double* p = b + (long long)col * n;
+  double a = 0.0, z = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a += p[t] * p[t];
+  block_reduce2<0, 0>(a, z);
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) out[col] = take_sqrt ? sqrt(a) : a;
+}
+
+// alpha = rho / (p . q)
+__global__ void pcg_alpha_kernel(const double* __restrict__ p, const double* __restrict__ q, long long n, PcgState st) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  double a = 0.0, z = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a += p[off + t] * q[off + t];
+  block_reduce2<0, 0>(a, z);
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) st.alpha[col] = st.rho[col] / a;
+}
+
+// x += alpha p; r -= alpha q; rel = ||r|| / ||b||; candidate when rel < tol (topology_multigrid.py:424-430)
+__global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                                  const double* __restrict__ q, long long n, PcgState st, double tol, int step) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  const double al = st.alpha[col];
+  double a = 0.0, z = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    x[off + t] += al * p[off + t];
+    const double rv = r[off + t] - al * q[off + t];
+    r[off + t] = rv;
+    a += rv * rv;
+  }
+  block_reduce2<0, 0>(a, z);
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) {
+    const double rel = sqrt(a) / st.bnorm[col];
+    st.rel[col] = rel;
+    atomicMax(&st.hist[step - 1], static_cast<unsigned long long>(__double_as_longlong(rel)));
+    if (rel < tol) { st.cand[col] = 1; atomicExch(&st.flags[0], 1); }
+  }
+}
+
+// True-residual recheck (topology_multigrid.py:431-437): when any column is a
+// candidate, every active column's residual is recomputed as t = b - K x; a
+// column converges when ||t|| / ||b|| < tol, the others continue from t.
+__global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, double* __restrict__ r, long long n, PcgState st,
+                                     double tol, int step) {
+  const int col = blockIdx.y;
+  if (!st.flags[0] || !st.active[col]) return;
+  const long long off = (long long)col * n;
+  double a = 0.0, z = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double v = t_res[off + t];
+    a += v * v;
+  }
+  block_reduce2<0, 0>(a, z);
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) {
+    const double rel = sqrt(a) / st.bnorm[col];
+    st.rel[col] = rel;
+    st.cand[col] = (rel < tol) ? 2 : 3;   // 2 = converged, 3 = continue from the true residual
+  }
+}
+
+// r <- t for non-converged columns; retire converged ones; count the active columns.
+__global__ void pcg_retire_kernel(const double* __restrict__ t_res, double* __restrict__ r, long long n, PcgState st, int step) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const int c = st.cand[col];
+  if (c == 3) {
+    const long long off = (long long)col * n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+      r[off + t] = t_res[off + t];
+  }
+}
+
+__global__ void pcg_flags_kernel(PcgState st, int step) {
+  // single block: finalize column states for this step
+  int n_active = 0;
+  for (int col = threadIdx.x; col < st.ncol; col += blockDim.x) {
+    if (st.active[col]) {
+      if (st.cand[col] == 2) {
+        st.active[col] = 0;
+        st.iters[col] = step;
+      }
+    }
+    st.cand[col] = 0;
+    n_active += st.active[col];
+  }
+  __shared__ int tot;
+  if (threadIdx.x == 0) tot = 0;
+  __syncthreads();
+  atomicAdd(&tot, n_active);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st.flags[1] = tot;
+    st.flags[0] = 0;
+  }
+}
+
+// scale = max|r| (clamped at 1e-300) and rzo = r . z_old (topology_multigrid.py:320, :446)
+__global__ void pcg_prep_kernel(const double* __restrict__ r, const double* __restrict__ z, long long n, PcgState st, int want_rzo) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  double mx = 0.0, d = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double rv = r[off + t];
+    mx = fmax(mx, fabs(rv));
+    if (want_rzo) d += rv * z[off + t];
+  }
+  block_reduce2<1, 0>(mx, d);
+  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) {
+    st.scale[col] = fmax(mx, 1e-300);
+    st.rzo[col] = d;
+  }
+}
+
+template <typename T>
+__global__ void pcg_to_work_kernel(const double* __restrict__ r, long long n, PcgState st, T* __restrict__ w) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  const double s = 1.0 / st.scale[col];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    w[off + t] = static_cast<T>(r[off + t] * s);
+}
+
+// z = scale * x_work; rz = r . z; beta = (rz - rzo) / rho (flexible Polak-Ribiere, topology_multigrid.py:445-448)
+template <typename T>
+__global__ void pcg_from_work_kernel(const T* __restrict__ w, const double* __restrict__ r, double* __restrict__ z, long long n,
+                                     PcgState st, int initial) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  const double s = st.scale[col];
+  double d = 0.0, zz = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double v = static_cast<double>(w[off + t]) * s;
+    z[off + t] = v;
+    d += r[off + t] * v;
+  }
+  block_reduce2<0, 0>(d, zz);
+  if (last_block_combine<0, 0>(d, zz, st.partial, st.count, col)) {
+    if (initial) {
+      st.beta[col] = 0.0;
+    } else {
+      st.beta[col] = (d - st.rzo[col]) / st.rho[col];
+    }
+    st.rho[col] = d;
+  }
+}
+
+// p = z + beta p
+__global__ void pcg_direction_kernel(const double* __restrict__ z, double* __restrict__ p, long long n, PcgState st, int initial) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  const double be = st.beta[col];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    p[off + t] = initial ? z[off + t] : z[off + t] + be * p[off + t];
+}
+
+// ------------------------------------------------------- layout copies ----
+
+// padded[c][node_p] <- mask * flat[c][node] for nodes inside the unpadded grid (0 elsewhere)
+__global__ void pad_kernel(const double* __restrict__ flat, long long fstride, Geo un, Geo pd, const uint8_t* __restrict__ mask,
+                           double* __restrict__ out, const int* __restrict__ colmap) {
+  const int col = blockIdx.y;
+  const int src = colmap ? colmap[col] : col;
+  const double* f = flat + (long long)src * fstride;
+  double* o = out + (long long)col * 3 * pd.nnode;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < pd.nnode; n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_coords(n, pd, i, j, k);
+    const bool inside = i < un.nx && j < un.ny && k < un.nz;
+    const unsigned m = mask ? mask[n] : 7u;
+    const long long s = inside ? ((long long)i * un.ny + j) * un.nz + k : 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[3 * n + a] = (inside && ((m >> a) & 1u)) ? f[3 * s + a] : 0.0;
+  }
+}
+
+__global__ void unpad_kernel(const double* __restrict__ padded, Geo un, Geo pd, double* __restrict__ flat, long long fstride,
+                             const int* __restrict__ colmap) {
+  const int col = blockIdx.y;
+  const int dst = colmap ? colmap[col] : col;
+  const double* p = padded + (long long)col * 3 * pd.nnode;
+  double* f = flat + (long long)dst * fstride;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < un.nnode; n += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    node_coords(n, un, i, j, k);
+    const long long s = ((long long)i * pd.ny + j) * pd.nz + k;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[3 * n + a] = p[3 * s + a];
+  }
+}
+
+// per-column norms of a flat block (host decides which columns are zero)
+__global__ void colnorm_kernel(const double* __restrict__ v, long long n, double* __restrict__ out, double* partial, unsigned* count) {
+  const int col = blockIdx.y;
+  double a = 0.0, z = 0.0;
+  const double* p = v + (long long)col * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a += p[t] * p[t];
+  block_reduce2<0, 0>(a, z);
+  if (last_block_combine<0, 0>(a, z, partial, count, col)) out[col] = sqrt(a);
+}
+
+__global__ void zero_flat_cols_kernel(double* __restrict__ v, long long n, const int* __restrict__ cols) {
+  double* p = v + (long long)cols[blockIdx.y] * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) p[t] = 0.0;
+}
+
+}  // namespace tfb

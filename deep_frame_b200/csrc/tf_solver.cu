@@ -1,0 +1,1092 @@
+// Matrix-free hex8 GMG-PCG solver behind the C ABI of include/tf_b200.h.
+//
+// Mirrors deep_frame/topology_multigrid.py (GeometricMultigrid) of the
+// reference: level count and padding (:58-63), finest-level mask (:138-144),
+// Jacobi diagonal (:118-124), Galerkin blocks (:145-208), lambda_max power
+// iteration (:214-223), Jacobi / Chebyshev smoothing (:284-305), V/W cycle
+// (:306-317), residual scaling of the preconditioner (:318-324), batched
+// flexible PCG with the true-residual recheck (:407-454) and FP64 retries of
+// failed columns (:385-406).  Differences by design: every RHS column runs in
+// the same launches (per-column scalars live on the device, converged columns
+// are masked out instead of compacted), and the coarsest level is a dense FP64
+// factor (tf_dense.cu) instead of cuDSS.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <type_traits>
+#include <cmath>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "tf_b200.h"
+#include "tf_common.h"
+#include "tf_dense.h"
+#include "tf_setup.cuh"
+
+using namespace tfb;
+
+namespace {
+
+thread_local std::string g_last_create_error;
+
+constexpr int CB = 4;                    // columns per thread in the Galerkin-level operator
+constexpr long long DENSE_LIMIT = 24000;  // largest dense coarsest factor (4.6 GB in FP64)
+
+struct Level {
+  Geo g{};
+  long long ndof = 0, nelem = 0;
+  DevBuf mask;      // uint8 [nnode]
+  DevBuf blocks64;  // Galerkin blocks [nelem][576] (levels >= 1)
+  DevBuf blocksw;   // FP32 copy of the blocks (FP32 work precision only)
+  DevBuf inv64;     // inverse diagonal [ndof]
+  DevBuf invw;      // FP32 copy (FP32 work precision only)
+  double lambda_max = 1.0;
+};
+
+struct Hierarchy {
+  std::vector<Level> lv;
+  int n_live = 0;
+  DevBuf live;      // int64 [n_live]: live dofs of the coarsest level
+  DevBuf X;         // FP64 [n_live][n_live] inverse Cholesky factor
+  double setup_s = 0.0;
+  bool setup_reported = false;
+};
+
+template <typename T>
+struct VBufs {
+  std::vector<DevBuf> b, x, xa, res, d, da;
+  int cap = 0;
+};
+
+Geo make_geo(long long ex, long long ey, long long ez) {
+  Geo g;
+  g.ex = static_cast<int>(ex);
+  g.ey = static_cast<int>(ey);
+  g.ez = static_cast<int>(ez);
+  g.nx = g.ex + 1;
+  g.ny = g.ey + 1;
+  g.nz = g.ez + 1;
+  g.nnode = (long long)g.nx * g.ny * g.nz;
+  return g;
+}
+
+inline dim3 cols_grid(long long n, int ncol, int block = 256, int cap = 1184) {
+  return dim3(grid_for(n, block, cap), ncol);
+}
+
+}  // namespace
+
+struct tf_handle {
+  tf_settings s{};
+  long long shape[3]{}, padded[3]{};
+  double spacing[3]{};
+  int nlev = 0;
+  std::vector<Geo> geo;
+  Geo un{};
+  double ke[576]{};
+  K0Param<double> k64{};
+  K0Param<float> k32{};
+  GalerkinParam W{};
+  DevBuf Q, K0dev, k0diag;
+  DevBuf moduli_un, moduli64, modulif;
+  bool have_moduli = false;
+  std::map<uint64_t, std::vector<int64_t>> bcs;
+  std::map<uint64_t, Hierarchy> hier;
+  // reduction scratch
+  DevBuf partial, count, scal;
+  // PCG state
+  DevBuf pcg_d, pcg_i, hist, colmap;
+  int pcg_cap = 0, hist_cap = 0;
+  int* host_flags = nullptr;
+  // FP64 PCG vectors [cap][ndof0]
+  DevBuf vb, vx, vr, vz, vp, vq;
+  int vcap = 0;
+  DevBuf cb, cy;  // coarsest work [cap][n_live]
+  size_t ccap = 0;
+  VBufs<float> wf;
+  VBufs<double> wd;
+  std::string err;
+  ~tf_handle() {
+    if (host_flags) cudaFreeHost(host_flags);
+  }
+};
+
+namespace {
+
+bool work_is_double(const tf_handle* h) { return h->s.precision == TF_PRECISION_FLOAT64; }
+
+// ------------------------------------------------------------ buffers -------
+
+void ensure_scratch(tf_handle* h, int ncol) {
+  const size_t need = (size_t)std::max(ncol, 1) * PCG_BLOCKS * 2 * sizeof(double);
+  if (h->partial.bytes < need) {
+    h->partial.alloc(need);
+    h->count.alloc(sizeof(unsigned) * std::max(ncol, 1));
+    TF_CUDA_CHECK(cudaMemset(h->count.p, 0, h->count.bytes));
+  }
+  if (!h->scal.p) h->scal.alloc(64 * sizeof(double));
+}
+
+template <typename T>
+VBufs<T>& vbufs(tf_handle* h);
+template <>
+VBufs<float>& vbufs<float>(tf_handle* h) { return h->wf; }
+template <>
+VBufs<double>& vbufs<double>(tf_handle* h) { return h->wd; }
+
+template <typename T>
+void ensure_vbufs(tf_handle* h, int ncol) {
+  VBufs<T>& v = vbufs<T>(h);
+  if (v.cap >= ncol && (int)v.b.size() == h->nlev) return;
+  const int cap = std::max(ncol, 1);
+  v.b.clear(); v.x.clear(); v.xa.clear(); v.res.clear(); v.d.clear(); v.da.clear();
+  for (int l = 0; l < h->nlev; ++l) {
+    const size_t bytes = sizeof(T) * 3 * (size_t)h->geo[l].nnode * cap;
+    for (auto* vec : {&v.b, &v.x, &v.xa, &v.res, &v.d, &v.da}) {
+      vec->emplace_back(bytes);
+      TF_CUDA_CHECK(cudaMemset(vec->back().p, 0, bytes));
+    }
+  }
+  v.cap = cap;
+}
+
+void ensure_pcg(tf_handle* h, int ncol) {
+  ensure_scratch(h, ncol);
+  if (h->pcg_cap < ncol) {
+    h->pcg_d.alloc(sizeof(double) * 8 * ncol);
+    h->pcg_i.alloc(sizeof(int) * (4 * ncol + 8));
+    h->colmap.alloc(sizeof(int) * ncol);
+    TF_CUDA_CHECK(cudaMemset(h->pcg_d.p, 0, h->pcg_d.bytes));
+    TF_CUDA_CHECK(cudaMemset(h->pcg_i.p, 0, h->pcg_i.bytes));
+    h->pcg_cap = ncol;
+  }
+  const int hneed = h->s.max_iterations + 2;
+  if (h->hist_cap < hneed) {
+    h->hist.alloc(sizeof(unsigned long long) * hneed);
+    h->hist_cap = hneed;
+  }
+  if (!h->host_flags) TF_CUDA_CHECK(cudaMallocHost(&h->host_flags, 64 * sizeof(int)));
+  if (h->vcap < ncol) {
+    const size_t bytes = sizeof(double) * 3 * (size_t)h->geo[0].nnode * ncol;
+    for (DevBuf* b : {&h->vb, &h->vx, &h->vr, &h->vz, &h->vp, &h->vq}) {
+      b->alloc(bytes);
+      TF_CUDA_CHECK(cudaMemset(b->p, 0, bytes));
+    }
+    h->vcap = ncol;
+  }
+}
+
+PcgState pcg_state(tf_handle* h, int ncol) {
+  PcgState st;
+  double* d = h->pcg_d.as<double>();
+  const int c = h->pcg_cap;
+  st.bnorm = d + 0 * c;
+  st.rho = d + 1 * c;
+  st.alpha = d + 2 * c;
+  st.rel = d + 3 * c;
+  st.scale = d + 4 * c;
+  st.rzo = d + 5 * c;
+  st.beta = d + 6 * c;
+  int* i = h->pcg_i.as<int>();
+  st.active = i + 0 * c;
+  st.cand = i + 1 * c;
+  st.iters = i + 2 * c;
+  st.flags = i + 4 * c;
+  st.hist = h->hist.as<unsigned long long>();
+  st.partial = h->partial.as<double>();
+  st.count = h->count.as<unsigned>();
+  st.ncol = ncol;
+  return st;
+}
+
+// --------------------------------------------------------- level apply ------
+
+template <typename T>
+const T* level_E(tf_handle* h, Hierarchy& hy, int l, bool precise) {
+  const bool dbl = std::is_same<T, double>::value;
+  if (l == 0) return static_cast<const T*>(dbl ? h->moduli64.p : h->modulif.p);
+  return static_cast<const T*>(dbl ? hy.lv[l].blocks64.p : hy.lv[l].blocksw.p);
+}
+template <typename T>
+const T* level_inv(Hierarchy& hy, int l) {
+  const bool dbl = std::is_same<T, double>::value;
+  return static_cast<const T*>(dbl ? hy.lv[l].inv64.p : hy.lv[l].invw.p);
+}
+template <typename T> const K0Param<T>& k0param(tf_handle* h);
+template <> const K0Param<double>& k0param<double>(tf_handle* h) { return h->k64; }
+template <> const K0Param<float>& k0param<float>(tf_handle* h) { return h->k32; }
+
+template <typename T>
+void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st) {
+  if (l == 0) {
+    dim3 grid(grid_for(a.g.nnode, 256, 4096), a.ncol);
+    fine_level_kernel<T><<<grid, 256, 0, st>>>(k0param<T>(h), a, mode);
+    TF_LAUNCH_CHECK("fine_level_kernel");
+  } else {
+    dim3 grid(grid_for(a.g.nnode, 128, 4096), (a.ncol + CB - 1) / CB);
+    block_level_kernel<T, CB><<<grid, 128, 0, st>>>(a, mode);
+    TF_LAUNCH_CHECK("block_level_kernel");
+  }
+}
+
+template <typename T>
+LevelArgs<T> level_args(tf_handle* h, Hierarchy& hy, int l, int ncol, const int* active) {
+  LevelArgs<T> a{};
+  a.g = h->geo[l];
+  a.E = level_E<T>(h, hy, l, false);
+  a.mask = hy.lv[l].mask.as<uint8_t>();
+  a.inv = level_inv<T>(hy, l);
+  a.colstride = 3 * a.g.nnode;
+  a.ncol = ncol;
+  a.active = active;
+  a.gate = nullptr;
+  return a;
+}
+
+// ------------------------------------------------------------- V-cycle ------
+
+template <typename T>
+void coarsest_solve(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int ncol, const int* active, cudaStream_t st) {
+  const int l = h->nlev - 1;
+  const long long nd = 3 * h->geo[l].nnode;
+  const int n = hy.n_live;
+  const T* b = vb.b[l].template as<T>();
+  T* x = vb.x[l].template as<T>();
+  dim3 g0 = cols_grid(nd, ncol);
+  zero_cols_kernel<T><<<g0, 256, 0, st>>>(x, nd, active);
+  TF_LAUNCH_CHECK("zero_cols_kernel");
+  if (n == 0) return;
+  dim3 g1 = cols_grid(n, ncol);
+  coarsest_gather_kernel<T><<<g1, 256, 0, st>>>(b, nd, hy.live.as<long long>(), n, h->cb.as<double>(), active);
+  TF_LAUNCH_CHECK("coarsest_gather_kernel");
+  dense_trimul(hy.X.as<double>(), h->cb.as<double>(), h->cy.as<double>(), n, ncol, 0, active, st);
+  dense_trimul(hy.X.as<double>(), h->cy.as<double>(), h->cb.as<double>(), n, ncol, 1, active, st);
+  coarsest_scatter_kernel<T><<<g1, 256, 0, st>>>(h->cb.as<double>(), hy.live.as<long long>(), n, x, nd, active);
+  TF_LAUNCH_CHECK("coarsest_scatter_kernel");
+}
+
+template <typename T>
+void smooth(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, bool first, int ncol, const int* active, cudaStream_t st) {
+  const tf_settings& s = h->s;
+  const long long nd = 3 * h->geo[l].nnode;
+  const double lam = hy.lv[l].lambda_max;
+  const bool jacobi = s.smoother == TF_SMOOTHER_JACOBI;
+  const int base = jacobi ? s.sweeps : s.chebyshev_degree;
+  const int count = std::max(1, (int)std::lround(base * std::pow(s.growth, l)));
+  LevelArgs<T> a = level_args<T>(h, hy, l, ncol, active);
+  dim3 ge = cols_grid(nd, ncol);
+  if (jacobi) {
+    const T step = static_cast<T>(s.damping / lam);
+    int start = 0;
+    if (first) {
+      jacobi_first_kernel<T><<<ge, 256, 0, st>>>(nd, a.inv, vb.b[l].template as<T>(), vb.x[l].template as<T>(), step, active);
+      TF_LAUNCH_CHECK("jacobi_first_kernel");
+      start = 1;
+    }
+    for (int k = start; k < count; ++k) {
+      a.u = vb.x[l].template as<T>();
+      a.b = vb.b[l].template as<T>();
+      a.y = vb.xa[l].template as<T>();
+      a.s = step;
+      launch_level<T>(h, l, a, MODE_JACOBI, st);
+      std::swap(vb.x[l], vb.xa[l]);
+    }
+    return;
+  }
+  const double upper = 1.1 * lam, lower = upper / s.chebyshev_ratio;
+  const double theta = 0.5 * (upper + lower), delta = 0.5 * (upper - lower);
+  const double sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  if (!first) {
+    a.u = vb.x[l].template as<T>();
+    a.b = vb.b[l].template as<T>();
+    a.y = vb.res[l].template as<T>();
+    launch_level<T>(h, l, a, MODE_RESID, st);
+  }
+  cheb_first_kernel<T><<<ge, 256, 0, st>>>(nd, a.inv, vb.b[l].template as<T>(), vb.res[l].template as<T>(),
+                                           vb.d[l].template as<T>(), vb.x[l].template as<T>(), static_cast<T>(1.0 / theta),
+                                           first ? 0 : 1, active);
+  TF_LAUNCH_CHECK("cheb_first_kernel");
+  for (int k = 1; k < count; ++k) {
+    const double rn = 1.0 / (2.0 * sigma - rho);
+    a.u = vb.d[l].template as<T>();
+    a.res = vb.res[l].template as<T>();
+    a.x = vb.x[l].template as<T>();
+    a.y = vb.da[l].template as<T>();
+    a.c1 = static_cast<T>(rn * rho);
+    a.c2 = static_cast<T>(2.0 * rn / delta);
+    launch_level<T>(h, l, a, MODE_CHEB, st);
+    std::swap(vb.d[l], vb.da[l]);
+    rho = rn;
+  }
+}
+
+template <typename T>
+void vcycle(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, int ncol, const int* active, cudaStream_t st) {
+  if (l == h->nlev - 1) {
+    coarsest_solve<T>(h, hy, vb, ncol, active, st);
+    return;
+  }
+  smooth<T>(h, hy, vb, l, true, ncol, active, st);
+  const int reps = (h->s.cycle == TF_CYCLE_W && l + 2 < h->nlev) ? 2 : 1;
+  const Geo& fg = h->geo[l];
+  const Geo& cg = h->geo[l + 1];
+  for (int rep = 0; rep < reps; ++rep) {
+    LevelArgs<T> a = level_args<T>(h, hy, l, ncol, active);
+    a.u = vb.x[l].template as<T>();
+    a.b = vb.b[l].template as<T>();
+    a.y = vb.res[l].template as<T>();
+    launch_level<T>(h, l, a, MODE_RESID, st);
+    restrict_kernel<T><<<cols_grid(cg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.res[l].template as<T>(), 3 * fg.nnode,
+                                                                  vb.b[l + 1].template as<T>(), 3 * cg.nnode,
+                                                                  hy.lv[l + 1].mask.as<uint8_t>(), active);
+    TF_LAUNCH_CHECK("restrict_kernel");
+    vcycle<T>(h, hy, vb, l + 1, ncol, active, st);
+    prolong_add_kernel<T><<<cols_grid(fg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.x[l + 1].template as<T>(), 3 * cg.nnode,
+                                                                     vb.x[l].template as<T>(), 3 * fg.nnode,
+                                                                     hy.lv[l].mask.as<uint8_t>(), active);
+    TF_LAUNCH_CHECK("prolong_add_kernel");
+  }
+  smooth<T>(h, hy, vb, l, false, ncol, active, st);
+}
+
+// ----------------------------------------------------------- hierarchy ------
+
+template <typename T>
+double power_lambda(tf_handle* h, Hierarchy& hy, int l, cudaStream_t st) {
+  VBufs<T>& vb = vbufs<T>(h);
+  const Geo& g = h->geo[l];
+  const long long nd = 3 * g.nnode;
+  T* v = vb.x[l].template as<T>();
+  T* y = vb.res[l].template as<T>();
+  power_init_kernel<T><<<grid_for(g.nnode, 256), 256, 0, st>>>(g.nnode, hy.lv[l].mask.as<uint8_t>(), v);
+  TF_LAUNCH_CHECK("power_init_kernel");
+  double* est = h->scal.as<double>();
+  for (int it = 0; it < h->s.power_iterations; ++it) {
+    LevelArgs<T> a = level_args<T>(h, hy, l, 1, nullptr);
+    a.u = v;
+    a.y = y;
+    launch_level<T>(h, l, a, MODE_APPLY, st);
+    power_scale_kernel<T><<<grid_for(nd, 256, PCG_BLOCKS), 256, 0, st>>>(nd, level_inv<T>(hy, l), y, h->partial.as<double>(),
+                                                                          h->count.as<unsigned>(), est);
+    TF_LAUNCH_CHECK("power_scale_kernel");
+    power_norm_kernel<T><<<grid_for(nd, 256), 256, 0, st>>>(nd, y, est, v);
+    TF_LAUNCH_CHECK("power_norm_kernel");
+  }
+  double host = 1.0;
+  if (h->s.power_iterations > 0) {
+    TF_CUDA_CHECK(cudaMemcpyAsync(&host, est, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TF_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  if (!std::isfinite(host) || host <= 0.0) throw Error(TF_NUMERIC, "lambda_max power iteration broke down on level " + std::to_string(l));
+  return host;
+}
+
+void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st) {
+  auto t0 = std::chrono::steady_clock::now();
+  const bool dbl = work_is_double(h);
+  ensure_scratch(h, 1);
+  hy.lv.clear();
+  hy.lv.resize(h->nlev);
+  const std::vector<int64_t>& fixed = h->bcs.at(key);
+  // level 0
+  Level& f = hy.lv[0];
+  f.g = h->geo[0];
+  f.ndof = 3 * f.g.nnode;
+  f.nelem = (long long)f.g.ex * f.g.ey * f.g.ez;
+  {
+    std::vector<uint8_t> bits(f.g.nnode, 0);
+    const Geo& un = h->un;
+    const long long nd_un = 3 * un.nnode;
+    for (int64_t dof : fixed) {
+      if (dof < 0 || dof >= nd_un) throw Error(TF_INVALID, "fixed dof index out of range");
+      const long long node = dof / 3;
+      const int comp = static_cast<int>(dof % 3);
+      const long long k = node % un.nz, r = node / un.nz, j = r % un.ny, i = r / un.ny;
+      const long long pn = (i * f.g.ny + j) * f.g.nz + k;
+      bits[pn] |= static_cast<uint8_t>(1u << comp);
+    }
+    DevBuf dbits(bits.size());
+    TF_CUDA_CHECK(cudaMemcpyAsync(dbits.p, bits.data(), bits.size(), cudaMemcpyHostToDevice, st));
+    f.mask.alloc(f.g.nnode);
+    fine_mask_kernel<<<grid_for(f.g.nnode, 256), 256, 0, st>>>(f.g, h->moduli64.as<double>(), dbits.as<uint8_t>(), f.mask.as<uint8_t>());
+    TF_LAUNCH_CHECK("fine_mask_kernel");
+    DevBuf diag(sizeof(double) * f.ndof);
+    fine_diag_kernel<<<grid_for(f.g.nnode, 256), 256, 0, st>>>(f.g, h->moduli64.as<double>(), f.mask.as<uint8_t>(),
+                                                               h->k0diag.as<double>(), diag.as<double>());
+    TF_LAUNCH_CHECK("fine_diag_kernel");
+    f.inv64.alloc(sizeof(double) * f.ndof);
+    if (!dbl) f.invw.alloc(sizeof(float) * f.ndof);
+    fine_inv_kernel<float><<<grid_for(f.g.nnode, 256), 256, 0, st>>>(f.g.nnode, diag.as<double>(), f.mask.as<uint8_t>(),
+                                                                     f.inv64.as<double>(), dbl ? nullptr : f.invw.as<float>());
+    TF_LAUNCH_CHECK("fine_inv_kernel");
+    TF_CUDA_CHECK(cudaStreamSynchronize(st));  // dbits / diag go out of scope
+  }
+  for (int l = 1; l < h->nlev; ++l) {
+    Level& c = hy.lv[l];
+    Level& p = hy.lv[l - 1];
+    c.g = h->geo[l];
+    c.ndof = 3 * c.g.nnode;
+    c.nelem = (long long)c.g.ex * c.g.ey * c.g.ez;
+    c.blocks64.alloc(sizeof(double) * 576 * c.nelem);
+    galerkin_kernel<<<grid_for(c.nelem, 1, 148 * 16), 128, 0, st>>>(h->W, c.g, p.g, l == 1 ? 1 : 0, h->moduli64.as<double>(),
+                                                                     hy.lv[0].mask.as<uint8_t>(), h->K0dev.as<double>(),
+                                                                     h->Q.as<double>(), l == 1 ? nullptr : p.blocks64.as<double>(),
+                                                                     c.blocks64.as<double>());
+    TF_LAUNCH_CHECK("galerkin_kernel");
+    DevBuf diag(sizeof(double) * c.ndof);
+    block_diag_kernel<<<grid_for(c.g.nnode, 256), 256, 0, st>>>(c.g, c.blocks64.as<double>(), diag.as<double>());
+    TF_LAUNCH_CHECK("block_diag_kernel");
+    double* dmax = h->scal.as<double>() + 1;
+    amax_kernel<<<grid_for(c.ndof, 256, PCG_BLOCKS), 256, 0, st>>>(diag.as<double>(), c.ndof, h->partial.as<double>(),
+                                                                   h->count.as<unsigned>(), dmax);
+    TF_LAUNCH_CHECK("amax_kernel");
+    c.mask.alloc(c.g.nnode);
+    c.inv64.alloc(sizeof(double) * c.ndof);
+    if (!dbl) c.invw.alloc(sizeof(float) * c.ndof);
+    coarse_mask_inv_kernel<float><<<grid_for(c.g.nnode, 256), 256, 0, st>>>(c.g.nnode, diag.as<double>(), dmax, h->s.dead_ratio,
+                                                                            c.mask.as<uint8_t>(), c.inv64.as<double>(),
+                                                                            dbl ? nullptr : c.invw.as<float>());
+    TF_LAUNCH_CHECK("coarse_mask_inv_kernel");
+    if (!dbl) {
+      c.blocksw.alloc(sizeof(float) * 576 * c.nelem);
+      cast_kernel<float><<<grid_for(576 * c.nelem, 256), 256, 0, st>>>(c.blocks64.as<double>(), c.blocksw.as<float>(), 576 * c.nelem);
+      TF_LAUNCH_CHECK("cast_kernel");
+    }
+    TF_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  // lambda_max(D^-1 A) of every smoothed level, in the work precision
+  if (dbl) ensure_vbufs<double>(h, 1); else ensure_vbufs<float>(h, 1);
+  for (int l = 0; l + 1 < h->nlev; ++l)
+    hy.lv[l].lambda_max = dbl ? power_lambda<double>(h, hy, l, st) : power_lambda<float>(h, hy, l, st);
+  // dense coarsest factor of the live dofs
+  Level& cl = hy.lv[h->nlev - 1];
+  std::vector<uint8_t> cmask(cl.g.nnode);
+  TF_CUDA_CHECK(cudaMemcpyAsync(cmask.data(), cl.mask.p, cmask.size(), cudaMemcpyDeviceToHost, st));
+  TF_CUDA_CHECK(cudaStreamSynchronize(st));
+  std::vector<long long> live;
+  std::vector<int> live_of(cl.ndof, -1);
+  for (long long n = 0; n < cl.g.nnode; ++n)
+    for (int a = 0; a < 3; ++a)
+      if ((cmask[n] >> a) & 1u) {
+        live_of[3 * n + a] = static_cast<int>(live.size());
+        live.push_back(3 * n + a);
+      }
+  const long long nl = static_cast<long long>(live.size());
+  if (nl > DENSE_LIMIT)
+    throw Error(TF_INVALID, "coarsest grid has " + std::to_string(nl) + " live dofs; the dense coarsest factor allows at most " +
+                                std::to_string(DENSE_LIMIT) + " (raise max_levels or lower coarsest_dofs)");
+  hy.n_live = static_cast<int>(nl);
+  if (nl > 0) {
+    hy.live.alloc(sizeof(long long) * nl);
+    TF_CUDA_CHECK(cudaMemcpyAsync(hy.live.p, live.data(), sizeof(long long) * nl, cudaMemcpyHostToDevice, st));
+    DevBuf dlive_of(sizeof(int) * cl.ndof);
+    TF_CUDA_CHECK(cudaMemcpyAsync(dlive_of.p, live_of.data(), sizeof(int) * cl.ndof, cudaMemcpyHostToDevice, st));
+    DevBuf A(sizeof(double) * nl * nl);
+    TF_CUDA_CHECK(cudaMemsetAsync(A.p, 0, A.bytes, st));
+    coarsest_assemble_kernel<<<grid_for(nl, 128), 128, 0, st>>>(cl.g, cl.blocks64.as<double>(), dlive_of.as<int>(),
+                                                                hy.live.as<long long>(), static_cast<int>(nl), A.as<double>());
+    TF_LAUNCH_CHECK("coarsest_assemble_kernel");
+    dense_symmetrize(A.as<double>(), static_cast<int>(nl), st);
+    int* info = reinterpret_cast<int*>(h->scal.as<double>() + 8);
+    TF_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int), st));
+    dense_cholesky(A.as<double>(), static_cast<int>(nl), info, st);
+    int hinfo = 0;
+    TF_CUDA_CHECK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TF_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (hinfo != 0)
+      throw Error(TF_NUMERIC, "coarsest Galerkin matrix is not positive definite (pivot " + std::to_string(hinfo) +
+                                  "); the supports do not remove every rigid-body mode");
+    hy.X.alloc(sizeof(double) * nl * nl);
+    dense_trinv(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), st);
+    TF_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  hy.setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  hy.setup_reported = false;
+}
+
+Hierarchy& get_hierarchy(tf_handle* h, uint64_t key, cudaStream_t st) {
+  require(h->have_moduli, "update(moduli) must be called before solving");
+  require(h->bcs.count(key) > 0, "no boundary conditions registered for this key (tf_set_bc)");
+  auto it = h->hier.find(key);
+  if (it != h->hier.end()) return it->second;
+  Hierarchy& hy = h->hier[key];
+  try {
+    build_hierarchy(h, key, hy, st);
+  } catch (...) {
+    h->hier.erase(key);
+    throw;
+  }
+  return hy;
+}
+
+void ensure_coarse_work(tf_handle* h, Hierarchy& hy, int ncol) {
+  const size_t need = sizeof(double) * (size_t)std::max(hy.n_live, 1) * ncol;
+  if (h->ccap < need) {
+    h->cb.alloc(need);
+    h->cy.alloc(need);
+    h->ccap = need;
+  }
+}
+
+// ----------------------------------------------------------------- PCG ------
+
+template <typename T>
+void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int initial, cudaStream_t s) {
+  const long long n = 3 * h->geo[0].nnode;
+  VBufs<T>& vb = vbufs<T>(h);
+  dim3 gr(grid_for(n, RED_THREADS, PCG_BLOCKS), ncol);
+  pcg_prep_kernel<<<gr, RED_THREADS, 0, s>>>(h->vr.as<double>(), h->vz.as<double>(), n, st, initial ? 0 : 1);
+  TF_LAUNCH_CHECK("pcg_prep_kernel");
+  pcg_to_work_kernel<T><<<cols_grid(n, ncol), 256, 0, s>>>(h->vr.as<double>(), n, st, vb.b[0].template as<T>());
+  TF_LAUNCH_CHECK("pcg_to_work_kernel");
+  vcycle<T>(h, hy, vb, 0, ncol, st.active, s);
+  pcg_from_work_kernel<T><<<gr, RED_THREADS, 0, s>>>(vb.x[0].template as<T>(), h->vr.as<double>(), h->vz.as<double>(), n, st, initial);
+  TF_LAUNCH_CHECK("pcg_from_work_kernel");
+  pcg_direction_kernel<<<cols_grid(n, ncol), 256, 0, s>>>(h->vz.as<double>(), h->vp.as<double>(), n, st, initial);
+  TF_LAUNCH_CHECK("pcg_direction_kernel");
+}
+
+// FP64 fine operator with mask (the PCG operator, topology_multigrid.py:411)
+void fine_apply64(tf_handle* h, Hierarchy& hy, const double* u, const double* b, double* y, int mode, int ncol,
+                  const int* active, const int* gate, cudaStream_t s) {
+  LevelArgs<double> a{};
+  a.g = h->geo[0];
+  a.E = h->moduli64.as<double>();
+  a.mask = hy.lv[0].mask.as<uint8_t>();
+  a.u = u;
+  a.b = b;
+  a.y = y;
+  a.colstride = 3 * a.g.nnode;
+  a.ncol = ncol;
+  a.active = active;
+  a.gate = gate;
+  launch_level<double>(h, 0, a, mode, s);
+}
+
+struct PcgResult {
+  std::vector<int> iters;
+  std::vector<double> rel;
+  std::vector<double> history;
+  int steps = 0;
+};
+
+// Batched flexible PCG over `ncol` columns held in h->vb (rhs) / h->vx (solution).
+// `run` selects the columns; with `warm` the current h->vx is the start vector.
+template <typename T>
+PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run, bool warm, cudaStream_t s) {
+  const long long n = 3 * h->geo[0].nnode;
+  ensure_vbufs<T>(h, ncol);
+  ensure_coarse_work(h, hy, ncol);
+  PcgState st = pcg_state(h, ncol);
+  const double tol = h->s.tolerance;
+  const int limit = h->s.max_iterations;
+  std::vector<int> zeros(ncol, 0);
+  TF_CUDA_CHECK(cudaMemcpyAsync(st.active, run.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, s));
+  TF_CUDA_CHECK(cudaMemcpyAsync(st.cand, zeros.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, s));
+  TF_CUDA_CHECK(cudaMemcpyAsync(st.iters, zeros.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, s));
+  TF_CUDA_CHECK(cudaMemsetAsync(st.flags, 0, sizeof(int) * 8, s));
+  TF_CUDA_CHECK(cudaMemsetAsync(st.hist, 0, sizeof(unsigned long long) * h->hist_cap, s));
+  dim3 gr(grid_for(n, RED_THREADS, PCG_BLOCKS), ncol);
+  dim3 ge = cols_grid(n, ncol);
+  pcg_norm_kernel<<<gr, RED_THREADS, 0, s>>>(h->vb.as<double>(), n, st, st.bnorm, 1);
+  TF_LAUNCH_CHECK("pcg_norm_kernel");
+  if (warm) {
+    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vr.as<double>(), MODE_RESID, ncol, st.active, nullptr, s);
+  } else {
+    zero_cols_kernel<double><<<ge, 256, 0, s>>>(h->vx.as<double>(), n, st.active);
+    TF_LAUNCH_CHECK("zero_cols_kernel");
+    TF_CUDA_CHECK(cudaMemcpyAsync(h->vr.p, h->vb.p, sizeof(double) * n * ncol, cudaMemcpyDeviceToDevice, s));
+  }
+  precondition<T>(h, hy, ncol, st, 1, s);
+  int step = 0;
+  int n_active = 0;
+  for (int c = 0; c < ncol; ++c) n_active += run[c];
+  while (n_active > 0 && step < limit) {
+    fine_apply64(h, hy, h->vp.as<double>(), nullptr, h->vq.as<double>(), MODE_APPLY, ncol, st.active, nullptr, s);
+    pcg_alpha_kernel<<<gr, RED_THREADS, 0, s>>>(h->vp.as<double>(), h->vq.as<double>(), n, st);
+    TF_LAUNCH_CHECK("pcg_alpha_kernel");
+    ++step;
+    pcg_update_kernel<<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), h->vr.as<double>(), h->vp.as<double>(), h->vq.as<double>(),
+                                                 n, st, tol, step);
+    TF_LAUNCH_CHECK("pcg_update_kernel");
+    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vq.as<double>(), MODE_RESID, ncol, st.active, st.flags, s);
+    pcg_truecheck_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, tol, step);
+    TF_LAUNCH_CHECK("pcg_truecheck_kernel");
+    pcg_retire_kernel<<<ge, 256, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, step);
+    TF_LAUNCH_CHECK("pcg_retire_kernel");
+    pcg_flags_kernel<<<1, 256, 0, s>>>(st, step);
+    TF_LAUNCH_CHECK("pcg_flags_kernel");
+    TF_CUDA_CHECK(cudaMemcpyAsync(h->host_flags, st.flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    n_active = h->host_flags[0];
+    if (n_active == 0) break;
+    precondition<T>(h, hy, ncol, st, 0, s);
+  }
+  PcgResult res;
+  res.steps = step;
+  if (n_active > 0) {
+    // iteration limit: final true residual of the columns still running (topology_multigrid.py:450-453)
+    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vq.as<double>(), MODE_RESID, ncol, st.active, nullptr, s);
+    pcg_norm_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), n, st, st.rzo, 1);
+    TF_LAUNCH_CHECK("pcg_norm_kernel");
+  }
+  std::vector<int> act(ncol), it(ncol);
+  std::vector<double> rel(ncol), bn(ncol), fin(ncol);
+  std::vector<unsigned long long> hb(std::max(step, 1));
+  TF_CUDA_CHECK(cudaMemcpyAsync(act.data(), st.active, sizeof(int) * ncol, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_CHECK(cudaMemcpyAsync(it.data(), st.iters, sizeof(int) * ncol, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_CHECK(cudaMemcpyAsync(rel.data(), st.rel, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_CHECK(cudaMemcpyAsync(bn.data(), st.bnorm, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_CHECK(cudaMemcpyAsync(fin.data(), st.rzo, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+  if (step > 0)
+    TF_CUDA_CHECK(cudaMemcpyAsync(hb.data(), st.hist, sizeof(unsigned long long) * step, cudaMemcpyDeviceToHost, s));
+  TF_CUDA_CHECK(cudaStreamSynchronize(s));
+  res.iters.assign(ncol, 0);
+  res.rel.assign(ncol, 1.0);
+  for (int c = 0; c < ncol; ++c) {
+    if (!run[c]) continue;
+    if (act[c]) {
+      res.iters[c] = step;
+      res.rel[c] = fin[c] / bn[c];
+    } else {
+      res.iters[c] = it[c];
+      res.rel[c] = rel[c];
+    }
+  }
+  for (int q = 0; q < step; ++q) {
+    double v;
+    std::memcpy(&v, &hb[q], sizeof(double));
+    res.history.push_back(v);
+  }
+  return res;
+}
+
+// Precise FP64 re-run of the columns that missed the tolerance (topology_multigrid.py:376-406).
+PcgResult pcg_precise(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run, cudaStream_t s) {
+  return pcg<double>(h, hy, ncol, run, true, s);
+}
+
+template <typename F>
+int guard(tf_handle* h, F&& f) {
+  try {
+    f();
+    return TF_OK;
+  } catch (const Error& e) {
+    if (h) h->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    if (h) h->err = e.what();
+    return TF_INTERNAL;
+  }
+}
+
+void validate_settings(const tf_settings& s) {
+  require(s.precision >= TF_PRECISION_FLOAT64 && s.precision <= TF_PRECISION_FLOAT16, "invalid precision");
+  require(s.precision <= TF_PRECISION_FLOAT32, "bfloat16/float16 work precision is not available in this build");
+  require(s.smoother == TF_SMOOTHER_JACOBI || s.smoother == TF_SMOOTHER_CHEBYSHEV, "invalid smoother");
+  require(s.cycle == TF_CYCLE_V || s.cycle == TF_CYCLE_W, "invalid cycle");
+  require(s.coarse == TF_COARSE_GALERKIN, "only Galerkin coarse operators are available in this build");
+  require(s.sweeps >= 1 && s.chebyshev_degree >= 1, "sweeps and chebyshev_degree must be positive");
+  require(s.max_levels >= 2 && s.max_levels <= 16, "max_levels must be in [2, 16]");
+  require(s.power_iterations >= 1, "power_iterations must be positive");
+  require(s.max_iterations >= 1, "max_iterations must be positive");
+  require(s.retries >= 0 && s.batch >= 0, "retries and batch must be non-negative");
+  require(s.coarsest_dofs >= 1, "coarsest_dofs must be positive");
+  require(std::isfinite(s.damping) && s.damping > 0, "damping must be positive");
+  require(std::isfinite(s.chebyshev_ratio) && s.chebyshev_ratio > 1, "chebyshev_ratio must exceed 1");
+  require(std::isfinite(s.growth) && s.growth > 0, "growth must be positive");
+  require(std::isfinite(s.tolerance) && s.tolerance > 0, "tolerance must be positive");
+  require(std::isfinite(s.dead_ratio) && s.dead_ratio >= 0, "dead_ratio must be non-negative");
+  require(std::isfinite(s.zero_rhs) && s.zero_rhs >= 0, "zero_rhs must be non-negative");
+}
+
+}  // namespace
+
+// =============================================================== C ABI ======
+
+extern "C" int tf_default_settings(tf_settings* s) {
+  if (!s) return TF_INVALID;
+  *s = tf_settings{};
+  s->precision = TF_PRECISION_FLOAT32;
+  s->smoother = TF_SMOOTHER_CHEBYSHEV;
+  s->cycle = TF_CYCLE_V;
+  s->coarse = TF_COARSE_GALERKIN;
+  s->sweeps = 2;
+  s->chebyshev_degree = 3;
+  s->max_levels = 8;
+  s->power_iterations = 20;
+  s->max_iterations = 2000;
+  s->retries = 2;
+  s->batch = 0;
+  s->coarsest_dofs = 8000;
+  s->damping = 1.0;
+  s->chebyshev_ratio = 20.0;
+  s->growth = 2.0;
+  s->tolerance = 1e-8;
+  s->dead_ratio = 1e-12;
+  s->zero_rhs = 1e-12;
+  return TF_OK;
+}
+
+extern "C" int tf_create(const tf_grid* grid, const double* ke, const double* me, const tf_settings* settings, tf_handle** out) {
+  g_last_create_error.clear();
+  if (!out) { g_last_create_error = "out must not be NULL"; return TF_INVALID; }
+  *out = nullptr;
+  tf_handle* h = new tf_handle();
+  int rc = guard(h, [&] {
+    require(grid && ke, "grid and ke must not be NULL");
+    if (settings) h->s = *settings; else tf_default_settings(&h->s);
+    validate_settings(h->s);
+    for (int d = 0; d < 3; ++d) {
+      require(grid->shape[d] >= 1 && grid->shape[d] < (1 << 20), "grid shape must be positive");
+      require(std::isfinite(grid->spacing[d]) && grid->spacing[d] > 0, "grid spacing must be finite and positive");
+      h->shape[d] = grid->shape[d];
+      h->spacing[d] = grid->spacing[d];
+    }
+    for (int t = 0; t < 576; ++t) {
+      require(std::isfinite(ke[t]), "ke must be finite");
+      h->ke[t] = ke[t];
+      h->k64.k[t] = ke[t];
+      h->k32.k[t] = static_cast<float>(ke[t]);
+    }
+    (void)me;
+    // level count and padding (topology_multigrid.py:58-63)
+    int count = 2;
+    auto coarse_dofs = [&](int c) {
+      double p = 3.0;
+      for (int d = 0; d < 3; ++d) p *= std::ceil(double(h->shape[d]) / std::pow(2.0, c - 1)) + 1.0;
+      return p;
+    };
+    while (count < h->s.max_levels && coarse_dofs(count) > double(h->s.coarsest_dofs)) ++count;
+    const long long factor = 1LL << (count - 1);
+    for (int d = 0; d < 3; ++d) h->padded[d] = ((h->shape[d] + factor - 1) / factor) * factor;
+    h->nlev = count;
+    for (int l = 0; l < count; ++l)
+      h->geo.push_back(make_geo(h->padded[0] >> l, h->padded[1] >> l, h->padded[2] >> l));
+    h->un = make_geo(h->shape[0], h->shape[1], h->shape[2]);
+    // trilinear interpolation weights W[child][fine corner][coarse corner] (topology_multigrid.py:19-27)
+    static const int C[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int c = 0; c < 8; ++c) {
+      const int off[3] = {c >> 2, (c >> 1) & 1, c & 1};
+      for (int r = 0; r < 8; ++r)
+        for (int s2 = 0; s2 < 8; ++s2) {
+          double w = 1.0;
+          for (int d = 0; d < 3; ++d) {
+            const double pos = 0.5 * (off[d] + C[r][d]);
+            w *= C[s2][d] == 1 ? pos : 1.0 - pos;
+          }
+          h->W.W[c][r][s2] = w;
+        }
+    }
+    // Q_c = P_c^T K0 P_c for children whose 24 dofs are all live
+    std::vector<double> Q(8 * 576, 0.0);
+    for (int c = 0; c < 8; ++c)
+      for (int s1 = 0; s1 < 8; ++s1)
+        for (int x = 0; x < 3; ++x)
+          for (int t = 0; t < 8; ++t)
+            for (int y = 0; y < 3; ++y) {
+              double v = 0.0;
+              for (int r = 0; r < 8; ++r)
+                for (int q = 0; q < 8; ++q) v += h->W.W[c][r][s1] * ke[(3 * r + x) * 24 + 3 * q + y] * h->W.W[c][q][t];
+              Q[c * 576 + (3 * s1 + x) * 24 + 3 * t + y] = v;
+            }
+    h->Q.alloc(sizeof(double) * Q.size());
+    TF_CUDA_CHECK(cudaMemcpy(h->Q.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice));
+    h->K0dev.alloc(sizeof(double) * 576);
+    TF_CUDA_CHECK(cudaMemcpy(h->K0dev.p, ke, sizeof(double) * 576, cudaMemcpyHostToDevice));
+    double kd[24];
+    for (int t = 0; t < 24; ++t) kd[t] = ke[t * 25];
+    h->k0diag.alloc(sizeof(kd));
+    TF_CUDA_CHECK(cudaMemcpy(h->k0diag.p, kd, sizeof(kd), cudaMemcpyHostToDevice));
+    const long long ne = h->un.ex * (long long)h->un.ey * h->un.ez;
+    const long long np = (long long)h->geo[0].ex * h->geo[0].ey * h->geo[0].ez;
+    h->moduli_un.alloc(sizeof(double) * ne);
+    h->moduli64.alloc(sizeof(double) * np);
+    TF_CUDA_CHECK(cudaMemset(h->moduli64.p, 0, h->moduli64.bytes));
+    if (!work_is_double(h)) {
+      h->modulif.alloc(sizeof(float) * np);
+      TF_CUDA_CHECK(cudaMemset(h->modulif.p, 0, h->modulif.bytes));
+    }
+    ensure_scratch(h, 1);
+  });
+  if (rc != TF_OK) {
+    g_last_create_error = h->err;
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return TF_OK;
+}
+
+extern "C" int tf_levels(const tf_handle* h, int32_t* levels, int64_t padded[3]) {
+  if (!h) return TF_INVALID;
+  if (levels) *levels = h->nlev;
+  if (padded)
+    for (int d = 0; d < 3; ++d) padded[d] = h->padded[d];
+  return TF_OK;
+}
+
+namespace {
+__global__ void pad_moduli_kernel(Geo un, Geo pd, const double* __restrict__ src, double* __restrict__ dst64, float* __restrict__ dstf) {
+  const long long total = (long long)pd.ex * pd.ey * pd.ez;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int k = static_cast<int>(e % pd.ez);
+    const long long r = e / pd.ez;
+    const int j = static_cast<int>(r % pd.ey), i = static_cast<int>(r / pd.ey);
+    const double v = (i < un.ex && j < un.ey && k < un.ez) ? src[((long long)i * un.ey + j) * un.ez + k] : 0.0;
+    dst64[e] = v;
+    if (dstf) dstf[e] = static_cast<float>(v);
+  }
+}
+}  // namespace
+
+extern "C" int tf_update(tf_handle* h, const double* moduli_dev, void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(moduli_dev != nullptr, "moduli must not be NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long ne = (long long)h->un.ex * h->un.ey * h->un.ez;
+    TF_CUDA_CHECK(cudaMemcpyAsync(h->moduli_un.p, moduli_dev, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+    const Geo& pd = h->geo[0];
+    pad_moduli_kernel<<<grid_for((long long)pd.ex * pd.ey * pd.ez, 256), 256, 0, s>>>(
+        h->un, pd, h->moduli_un.as<double>(), h->moduli64.as<double>(), work_is_double(h) ? nullptr : h->modulif.as<float>());
+    TF_LAUNCH_CHECK("pad_moduli_kernel");
+    h->hier.clear();
+    h->have_moduli = true;
+  });
+}
+
+extern "C" int tf_set_bc(tf_handle* h, uint64_t key, const int64_t* fixed, int64_t count) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(count >= 0 && (count == 0 || fixed), "fixed must not be NULL");
+    const long long nd = 3 * h->un.nnode;
+    std::vector<int64_t> v(fixed, fixed + count);
+    for (int64_t d : v) require(d >= 0 && d < nd, "fixed dof index out of range");
+    auto it = h->bcs.find(key);
+    if (it != h->bcs.end() && it->second != v) h->hier.erase(key);
+    h->bcs[key] = std::move(v);
+  });
+}
+
+extern "C" int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
+                        void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    auto t0 = std::chrono::steady_clock::now();
+    require(nrhs >= 0, "nrhs must be non-negative");
+    require(nrhs == 0 || (f_dev && u_dev), "forces and solution must not be NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Hierarchy& hy = get_hierarchy(h, key, s);
+    const long long nun = 3 * h->un.nnode;
+    const long long n = 3 * h->geo[0].nnode;
+    // zero-RHS columns (topology_multigrid.py:350-351)
+    std::vector<double> norms(nrhs, 0.0);
+    if (nrhs > 0) {
+      ensure_scratch(h, nrhs);
+      DevBuf dn(sizeof(double) * nrhs);
+      colnorm_kernel<<<dim3(grid_for(nun, RED_THREADS, PCG_BLOCKS), nrhs), RED_THREADS, 0, s>>>(
+          f_dev, nun, dn.as<double>(), h->partial.as<double>(), h->count.as<unsigned>());
+      TF_LAUNCH_CHECK("colnorm_kernel");
+      TF_CUDA_CHECK(cudaMemcpyAsync(norms.data(), dn.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
+      TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    }
+    double mx = 0.0;
+    for (double v : norms) {
+      if (!std::isfinite(v)) throw Error(TF_INVALID, "forces must be finite");
+      mx = std::max(mx, v);
+    }
+    std::vector<int> live, dead;
+    for (int c = 0; c < nrhs; ++c) (norms[c] > h->s.zero_rhs * std::max(mx, 1e-300) ? live : dead).push_back(c);
+    std::vector<int> iters(nrhs, 0);
+    std::vector<double> rel(nrhs, 0.0);
+    std::vector<double> history;
+    int batches = 0, retried = 0, steps = 0;
+    if (!dead.empty()) {
+      DevBuf dcols(sizeof(int) * dead.size());
+      TF_CUDA_CHECK(cudaMemcpyAsync(dcols.p, dead.data(), sizeof(int) * dead.size(), cudaMemcpyHostToDevice, s));
+      zero_flat_cols_kernel<<<dim3(grid_for(nun, 256), (unsigned)dead.size()), 256, 0, s>>>(u_dev, nun, dcols.as<int>());
+      TF_LAUNCH_CHECK("zero_flat_cols_kernel");
+      TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    }
+    const int chunk = h->s.batch > 0 ? h->s.batch : std::max<int>(1, static_cast<int>(live.size()));
+    for (size_t start = 0; start < live.size(); start += chunk) {
+      const int nc = static_cast<int>(std::min<size_t>(chunk, live.size() - start));
+      std::vector<int> cols(live.begin() + start, live.begin() + start + nc);
+      ensure_pcg(h, nc);
+      TF_CUDA_CHECK(cudaMemcpyAsync(h->colmap.p, cols.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
+      pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(f_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
+                                                                h->vb.as<double>(), h->colmap.as<int>());
+      TF_LAUNCH_CHECK("pad_kernel");
+      std::vector<int> run(nc, 1);
+      PcgResult r = work_is_double(h) ? pcg<double>(h, hy, nc, run, false, s) : pcg<float>(h, hy, nc, run, false, s);
+      history.insert(history.end(), r.history.begin(), r.history.end());
+      steps += r.steps;
+      for (int attempt = 0; attempt < h->s.retries; ++attempt) {
+        std::vector<int> failed(nc, 0);
+        int nfail = 0;
+        for (int c = 0; c < nc; ++c)
+          if (!(r.rel[c] < h->s.tolerance)) { failed[c] = 1; ++nfail; }
+        if (!nfail) break;
+        // restart from the previous iterate where it improved on zero (topology_multigrid.py:393)
+        std::vector<int> reset(nc, 0);
+        for (int c = 0; c < nc; ++c) reset[c] = failed[c] && !(r.rel[c] < 1.0);
+        DevBuf dreset(sizeof(int) * nc);
+        TF_CUDA_CHECK(cudaMemcpyAsync(dreset.p, reset.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
+        zero_cols_kernel<double><<<cols_grid(n, nc), 256, 0, s>>>(h->vx.as<double>(), n, dreset.as<int>());
+        TF_LAUNCH_CHECK("zero_cols_kernel");
+        PcgResult again = pcg_precise(h, hy, nc, failed, s);
+        for (int c = 0; c < nc; ++c)
+          if (failed[c]) {
+            r.iters[c] += again.iters[c];
+            r.rel[c] = again.rel[c];
+          }
+        history.insert(history.end(), again.history.begin(), again.history.end());
+        steps += again.steps;
+        retried += nfail;
+      }
+      unpad_kernel<<<cols_grid(h->un.nnode, nc), 256, 0, s>>>(h->vx.as<double>(), h->un, h->geo[0], u_dev, nun, h->colmap.as<int>());
+      TF_LAUNCH_CHECK("unpad_kernel");
+      for (int c = 0; c < nc; ++c) {
+        iters[cols[c]] = r.iters[c];
+        rel[cols[c]] = r.rel[c];
+      }
+      ++batches;
+    }
+    TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool converged = true;
+    for (int c : live) converged &= rel[c] < h->s.tolerance;
+    if (report) {
+      if (report->iterations)
+        for (int c = 0; c < nrhs; ++c) report->iterations[c] = iters[c];
+      if (report->relative_residual)
+        for (int c = 0; c < nrhs; ++c) report->relative_residual[c] = rel[c];
+      report->history_len = 0;
+      if (report->history)
+        for (double v : history) {
+          if (report->history_len >= report->history_capacity) break;
+          report->history[report->history_len++] = v;
+        }
+      report->converged = converged ? 1 : 0;
+      report->batches = batches;
+      report->retried_columns = retried;
+      report->zero_rhs_columns = static_cast<int>(dead.size());
+      report->steps = steps;
+      report->levels = h->nlev;
+      report->coarsest_dofs = hy.n_live;
+      report->setup_s = hy.setup_reported ? 0.0 : hy.setup_s;
+      for (int l = 0; l < 16; ++l) report->lambda_max[l] = (l + 1 < h->nlev) ? hy.lv[l].lambda_max : 0.0;
+      report->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    hy.setup_reported = true;
+  });
+}
+
+namespace {
+void fill_level_report(tf_handle* h, Hierarchy& hy, tf_report* report) {
+  if (!report) return;
+  report->levels = h->nlev;
+  report->coarsest_dofs = hy.n_live;
+  report->setup_s = hy.setup_reported ? 0.0 : hy.setup_s;
+  for (int l = 0; l < 16; ++l) report->lambda_max[l] = (l + 1 < h->nlev) ? hy.lv[l].lambda_max : 0.0;
+}
+}  // namespace
+
+extern "C" int tf_prepare(tf_handle* h, uint64_t key, tf_report* report, void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    Hierarchy& hy = get_hierarchy(h, key, static_cast<cudaStream_t>(stream));
+    fill_level_report(h, hy, report);
+    hy.setup_reported = true;
+  });
+}
+
+extern "C" int tf_precondition(tf_handle* h, uint64_t key, const double* r_dev, int32_t nrhs, double* z_dev, void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(nrhs >= 0 && (nrhs == 0 || (r_dev && z_dev)), "invalid preconditioner arguments");
+    if (nrhs == 0) return;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Hierarchy& hy = get_hierarchy(h, key, s);
+    const long long nun = 3 * h->un.nnode;
+    ensure_pcg(h, nrhs);
+    ensure_coarse_work(h, hy, nrhs);
+    PcgState st = pcg_state(h, nrhs);
+    std::vector<int> ones(nrhs, 1);
+    TF_CUDA_CHECK(cudaMemcpyAsync(st.active, ones.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, s));
+    pad_kernel<<<cols_grid(h->geo[0].nnode, nrhs), 256, 0, s>>>(r_dev, nun, h->un, h->geo[0], nullptr, h->vr.as<double>(), nullptr);
+    TF_LAUNCH_CHECK("pad_kernel");
+    if (work_is_double(h)) {
+      ensure_vbufs<double>(h, nrhs);
+      precondition<double>(h, hy, nrhs, st, 1, s);
+    } else {
+      ensure_vbufs<float>(h, nrhs);
+      precondition<float>(h, hy, nrhs, st, 1, s);
+    }
+    unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vz.as<double>(), h->un, h->geo[0], z_dev, nun, nullptr);
+    TF_LAUNCH_CHECK("unpad_kernel");
+    TF_CUDA_CHECK(cudaStreamSynchronize(s));
+  });
+}
+
+extern "C" int tf_apply(tf_handle* h, uint64_t key, int32_t use_mask, const double* u_dev, int32_t nrhs, double* y_dev, void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(h->have_moduli, "update(moduli) must be called before applying the operator");
+    require(nrhs >= 0 && (nrhs == 0 || (u_dev && y_dev)), "invalid operator arguments");
+    if (nrhs == 0) return;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!use_mask) {
+      LevelArgs<double> a{};
+      a.g = h->un;
+      a.E = h->moduli_un.as<double>();
+      a.mask = nullptr;
+      a.u = u_dev;
+      a.y = y_dev;
+      a.colstride = 3 * h->un.nnode;
+      a.ncol = nrhs;
+      launch_level<double>(h, 0, a, MODE_APPLY, s);
+      return;
+    }
+    Hierarchy& hy = get_hierarchy(h, key, s);
+    const long long nun = 3 * h->un.nnode;
+    ensure_pcg(h, nrhs);
+    pad_kernel<<<cols_grid(h->geo[0].nnode, nrhs), 256, 0, s>>>(u_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
+                                                                h->vb.as<double>(), nullptr);
+    TF_LAUNCH_CHECK("pad_kernel");
+    fine_apply64(h, hy, h->vb.as<double>(), nullptr, h->vq.as<double>(), MODE_APPLY, nrhs, nullptr, nullptr, s);
+    unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vq.as<double>(), h->un, h->geo[0], y_dev, nun, nullptr);
+    TF_LAUNCH_CHECK("unpad_kernel");
+  });
+}
+
+extern "C" int tf_element_energy(tf_handle* h, const double* u_dev, int32_t nrhs, const double* comb_dev, int32_t ncomb,
+                                 const double* coef_dev, const double* scale_dev, double* out_dev, int32_t accumulate,
+                                 int32_t per_column, void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(nrhs >= 0 && (nrhs == 0 || (u_dev && out_dev)), "invalid energy arguments");
+    require(!comb_dev || ncomb >= 1, "ncomb must be positive with a combination matrix");
+    require(!(per_column && comb_dev), "per_column energies take no combination matrix");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long ne = (long long)h->un.ex * h->un.ey * h->un.ez;
+    energy_kernel<double><<<grid_for(ne, 128, 148 * 16), 128, 0, s>>>(h->k64, h->un, u_dev, 3 * h->un.nnode, nrhs, comb_dev,
+                                                                        comb_dev ? ncomb : nrhs, coef_dev, scale_dev, out_dev,
+                                                                        accumulate, per_column);
+    TF_LAUNCH_CHECK("energy_kernel");
+  });
+}
+
+extern "C" int tf_destroy(tf_handle* h) {
+  if (!h) return TF_OK;
+  cudaDeviceSynchronize();
+  delete h;
+  return TF_OK;
+}
+
+extern "C" const char* tf_last_error(const tf_handle* h) {
+  if (!h) return g_last_create_error.c_str();
+  return h->err.c_str();
+}

@@ -1,0 +1,367 @@
+"""Drop-in ``GeometricMultigrid`` backed by the sm_100a library.
+
+Same constructor, methods, settings keys and report keys as the reference's
+deep_frame/topology_multigrid.py:46-548, so ``HexElasticity(...,
+linear_solver="multigrid")`` style callers can swap it in.  All numerical
+work (operator, hierarchy, V-cycle, PCG, energies) runs in libtfb200.so; the
+torch tensors here only hold device memory and carry the current stream.
+There is no CPU path: without CUDA or without the built library every call
+raises.
+
+Host-facing calls (``solve``, ``product``) take and return NumPy arrays like
+the reference; ``solve_device`` / ``update_device`` keep everything in HBM.
+"""
+import ctypes
+from time import perf_counter
+
+import numpy as np
+
+from . import _lib
+
+# The reference's MULTIGRID defaults (topology_multigrid.py:8-10) with two
+# differences: the coarsest grid is factored densely on the device, so it is
+# kept at <= 8000 dofs, and all live RHS columns share one PCG launch (batch 0).
+MULTIGRID = {"coarse": "galerkin", "coarsest_dofs": 8000, "max_levels": 8, "smoother": "chebyshev", "sweeps": 2,
+             "damping": 1.0, "chebyshev_degree": 3, "chebyshev_ratio": 20.0, "growth": 2.0, "cycle": "V",
+             "power_iterations": 20, "precision": "float32", "tolerance": 1e-8, "max_iterations": 2000, "batch": 0,
+             "projection": True, "coarsest_projection": True, "dead_ratio": 1e-12, "zero_rhs": 1e-12, "retries": 2,
+             "device": "cuda", "eigen_tolerance": 1e-8, "eigen_iterations": 300, "eigen_guard": 2, "eigen_refresh": 10,
+             "eigen_drop": 1e-12, "eigen_seed": 0}
+PRECISIONS = ("float64", "float32", "bfloat16", "float16")
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Level:
+    """Shape bookkeeping of one multigrid level (reference topology_multigrid.py:40-44)."""
+
+    def __init__(self, shape, spacing):
+        self.shape, self.spacing = tuple(int(n) for n in shape), np.asarray(spacing, dtype=float)
+        self.nodes = tuple(n + 1 for n in self.shape)
+        self.lambda_max = None
+
+
+def _native_settings(settings):
+    s = _lib.default_settings()
+    if settings["precision"] not in PRECISIONS or settings["coarse"] not in ("galerkin", "rediscretize") \
+            or settings["smoother"] not in ("jacobi", "chebyshev") or settings["cycle"] not in ("V", "W"):
+        raise ValueError("Invalid multigrid settings")
+    s.precision = _lib.PRECISION[settings["precision"]]
+    s.smoother = _lib.SMOOTHER[settings["smoother"]]
+    s.cycle = _lib.CYCLE[settings["cycle"]]
+    s.coarse = _lib.COARSE[settings["coarse"]]
+    for name in ("sweeps", "chebyshev_degree", "max_levels", "power_iterations", "max_iterations", "retries", "batch",
+                 "coarsest_dofs"):
+        setattr(s, name, int(settings[name]))
+    for name in ("damping", "chebyshev_ratio", "growth", "tolerance", "dead_ratio", "zero_rhs"):
+        setattr(s, name, float(settings[name]))
+    return s
+
+
+class GeometricMultigrid:
+    def __init__(self, shape, spacing, ke, settings=None, me=None):
+        torch = _torch()
+        self.torch = torch
+        self.settings = {**MULTIGRID, **(settings or {})}
+        native = _native_settings(self.settings)
+        self.device = torch.device(self.settings["device"])
+        if self.device.type != "cuda" or not torch.cuda.is_available():
+            raise RuntimeError("GeometricMultigrid runs on the CUDA device only (no CPU fallback)")
+        self.lib = _lib.load()
+        self.shape = tuple(int(n) for n in shape)
+        self.spacing = np.asarray(spacing, dtype=float)
+        self.ke64 = np.ascontiguousarray(np.asarray(ke, dtype=float))
+        if self.ke64.shape != (24, 24):
+            raise ValueError("ke must be a 24x24 element stiffness")
+        self.me64 = None if me is None else np.ascontiguousarray(np.asarray(me, dtype=float))
+        grid = _lib.TfGrid()
+        for d in range(3):
+            grid.shape[d] = self.shape[d]
+            grid.spacing[d] = float(self.spacing[d])
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.tf_create(ctypes.byref(grid), self.ke64.ctypes.data_as(ctypes.c_void_p),
+                                          None if self.me64 is None else self.me64.ctypes.data_as(ctypes.c_void_p),
+                                          ctypes.byref(native), ctypes.byref(handle)), None, "tf_create")
+        self.handle = handle
+        levels, padded = ctypes.c_int32(), (ctypes.c_int64 * 3)()
+        _lib.check(self.lib.tf_levels(self.handle, ctypes.byref(levels), padded), self.handle, "tf_levels")
+        self.padded = tuple(int(p) for p in padded)
+        self.levels = [Level(np.asarray(self.padded) // 2 ** level, self.spacing * 2 ** level) for level in range(levels.value)]
+        self.center = np.asarray(self.shape) * self.spacing / 2
+        self.nodes = tuple(n + 1 for n in self.shape)
+        self.ndof = 3 * int(np.prod(self.nodes))
+        self.nelem = int(np.prod(self.shape))
+        self.moduli = None
+        self._moduli_host = None
+        self._keys, self._fixed = {}, {}
+        self.hierarchies, self.statistics = {}, []
+
+    # ------------------------------------------------------------ helpers --
+    def _stream(self):
+        return _lib.stream_of(self.device)
+
+    def _key(self, key, fixed):
+        fixed = np.ascontiguousarray(np.asarray(fixed, dtype=np.int64).ravel())
+        if key not in self._keys:
+            self._keys[key] = len(self._keys) + 1
+        ident = self._keys[key]
+        known = self._fixed.get(ident)
+        if known is None or not np.array_equal(known, fixed):
+            _lib.check(self.lib.tf_set_bc(self.handle, ident, fixed.ctypes.data_as(ctypes.c_void_p), len(fixed)),
+                       self.handle, "tf_set_bc")
+            self._fixed[ident] = fixed
+            self.hierarchies.pop(key, None)
+        return ident
+
+    def _columns(self, flat):
+        """NumPy or torch [ndof] / [ndof, R] -> contiguous device FP64 [R, ndof]."""
+        torch = self.torch
+        data = torch.as_tensor(flat, dtype=torch.float64, device=self.device)
+        data = data[:, None] if data.ndim == 1 else data
+        if data.shape[0] != self.ndof:
+            raise ValueError(f"expected {self.ndof} dofs, got {data.shape[0]}")
+        return data.T.contiguous()
+
+    def grid(self, flat, dtype=None):
+        """Flat [ndof, R] -> reference grid layout [R, 3, padded nodes] (topology_multigrid.py:80-88)."""
+        torch = self.torch
+        flat = torch.as_tensor(flat, device=self.device, dtype=dtype or torch.float64)
+        flat = flat[:, None] if flat.ndim == 1 else flat
+        count = flat.shape[1]
+        out = torch.zeros((count, 3) + self.levels[0].nodes, dtype=flat.dtype, device=self.device)
+        n = self.nodes
+        out[:, :, :n[0], :n[1], :n[2]] = flat.T.reshape((count,) + n + (3,)).permute(0, 4, 1, 2, 3)
+        return out
+
+    def flat(self, grid):
+        n = self.nodes
+        return grid[:, :, :n[0], :n[1], :n[2]].permute(0, 2, 3, 4, 1).reshape(grid.shape[0], -1).T
+
+    def element_field(self, values, dtype=None):
+        torch = self.torch
+        field = torch.zeros(self.padded, dtype=dtype or torch.float64, device=self.device)
+        field[:self.shape[0], :self.shape[1], :self.shape[2]] = torch.as_tensor(
+            np.asarray(values, dtype=float).reshape(self.shape), dtype=field.dtype, device=self.device)
+        return field
+
+    # -------------------------------------------------------------- state --
+    def update(self, moduli):
+        """Set element moduli [nelem] (host or device) and drop every hierarchy (topology_multigrid.py:97-100)."""
+        torch = self.torch
+        values = torch.as_tensor(moduli, dtype=torch.float64, device=self.device).reshape(-1).contiguous()
+        if values.numel() != self.nelem:
+            raise ValueError(f"expected {self.nelem} moduli, got {values.numel()}")
+        self.update_device(values)
+
+    def update_device(self, moduli):
+        if moduli.dtype != self.torch.float64 or not moduli.is_cuda or not moduli.is_contiguous() or moduli.numel() != self.nelem:
+            raise ValueError("moduli must be a contiguous CUDA float64 tensor with one value per element")
+        _lib.check(self.lib.tf_update(self.handle, _lib.ptr(moduli), self._stream()), self.handle, "tf_update")
+        self.moduli = moduli
+        self._moduli_host = None
+        self.hierarchies.clear()
+
+    def mask(self, fixed):
+        """(live mask, constrained) grids [3, padded nodes] (topology_multigrid.py:138-144)."""
+        torch = self.torch
+        if self.moduli is None:
+            raise ValueError("update(moduli) must be called first")
+        if self._moduli_host is None:
+            self._moduli_host = self.moduli.cpu().numpy().reshape(self.shape)
+        touched = np.zeros(tuple(p + 1 for p in self.padded), dtype=bool)
+        live = self._moduli_host > 0
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    touched[dx:dx + self.shape[0], dy:dy + self.shape[1], dz:dz + self.shape[2]] |= live
+        active = torch.as_tensor(np.broadcast_to(touched, (3,) + touched.shape).astype(float), device=self.device)
+        constrained = torch.zeros_like(active)
+        fixed = np.asarray(fixed, dtype=np.int64)
+        if len(fixed):
+            flags = np.zeros(self.ndof)
+            flags[fixed] = 1.0
+            constrained = self.grid(flags)[0] * active
+        return active * (1 - constrained), constrained
+
+    def hierarchy(self, key, fixed):
+        """Build (or reuse) the hierarchy of `key` and return its summary (topology_multigrid.py:145-208)."""
+        if key in self.hierarchies:
+            return self.hierarchies[key]
+        ident = self._key(key, fixed)
+        report = _lib.TfReport()
+        _lib.check(self.lib.tf_prepare(self.handle, ident, ctypes.byref(report), self._stream()), self.handle, "tf_prepare")
+        levels = [Level(level.shape, level.spacing) for level in self.levels]
+        for index, level in enumerate(levels[:-1]):
+            level.lambda_max = float(report.lambda_max[index])
+        hierarchy = {"key": key, "id": ident, "levels": levels, "fixed": np.asarray(fixed, dtype=np.int64),
+                     "coarsest": {"dofs": int(report.coarsest_dofs), "pins": 0}, "setup_s": float(report.setup_s),
+                     "kernel_check": [], "coefficients": np.zeros((6, 0))}
+        self.hierarchies[key] = hierarchy
+        return hierarchy
+
+    # ------------------------------------------------------------ solving --
+    def solve(self, key, fixed, forces, support=None):
+        """Reference-compatible solve: NumPy forces [ndof, R] in, (NumPy [ndof, R], report) out."""
+        torch = self.torch
+        started = perf_counter()
+        forces = np.asarray(forces, dtype=float)
+        columns = self._columns(forces.reshape(len(forces), -1))
+        out, report = self.solve_device(key, fixed, columns, support=support)
+        flat = out.T.cpu().numpy()
+        report["seconds"] = perf_counter() - started
+        return flat, report
+
+    def solve_device(self, key, fixed, forces, out=None, support=None):
+        """Device-resident solve: forces [R, ndof] contiguous CUDA float64; returns (u [R, ndof], report)."""
+        torch = self.torch
+        floating = support is not None and self.settings["projection"]
+        if floating:
+            raise NotImplementedError("floating (inertia-relief) supports are not available in this build")
+        started = perf_counter()
+        if self.moduli is None:
+            raise ValueError("update(moduli) must be called before solve")
+        if forces.dtype != torch.float64 or not forces.is_cuda or not forces.is_contiguous() or forces.shape[-1] != self.ndof:
+            raise ValueError("forces must be a contiguous CUDA float64 [R, ndof] tensor")
+        count = forces.shape[0]
+        ident = self._key((key, False), fixed)
+        out = torch.empty_like(forces) if out is None else out
+        iterations = np.zeros(count, dtype=np.int32)
+        relative = np.zeros(count, dtype=np.float64)
+        history = np.zeros(self.settings["max_iterations"] * (1 + self.settings["retries"]) + 8, dtype=np.float64)
+        report = _lib.TfReport()
+        report.iterations = iterations.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        report.relative_residual = relative.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        report.history = history.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        report.history_capacity = len(history)
+        _lib.check(self.lib.tf_solve(self.handle, ident, _lib.ptr(forces), count, _lib.ptr(out), ctypes.byref(report),
+                                     self._stream()), self.handle, "tf_solve")
+        levels = int(report.levels)
+        result = {"iterations": iterations.tolist(), "relative_residual": relative.tolist(),
+                  "converged": bool(report.converged), "history": [history[:report.history_len].tolist()],
+                  "batches": int(report.batches), "retried_columns": int(report.retried_columns),
+                  "zero_rhs_columns": int(report.zero_rhs_columns), "seconds": perf_counter() - started,
+                  "setup_s": float(report.setup_s), "floating": False, "levels": levels,
+                  "coarsest_dofs": int(report.coarsest_dofs), "kernel": 0, "rhs_kernel_component": None,
+                  "kernel_check": [], "lambda_max": [float(report.lambda_max[i]) for i in range(levels - 1)],
+                  "steps": int(report.steps)}
+        self.statistics.append(result)
+        return out, result
+
+    def precondition(self, hierarchy, residual):
+        """One V-cycle z = M^-1 r of `hierarchy` on a residual grid [R, 3, padded nodes]."""
+        columns = self.flat(residual).T.contiguous().to(self.torch.float64)
+        out = self.torch.empty_like(columns)
+        _lib.check(self.lib.tf_precondition(self.handle, hierarchy["id"], _lib.ptr(columns), columns.shape[0], _lib.ptr(out),
+                                            self._stream()), self.handle, "tf_precondition")
+        return self.grid(out.T)
+
+    # ----------------------------------------------------------- operators --
+    def apply_device(self, columns, key=None, fixed=None, out=None):
+        """y = K u on [R, ndof] device columns; with key/fixed the live mask of that hierarchy is applied."""
+        out = self.torch.empty_like(columns) if out is None else out
+        ident = 0 if key is None else self._key((key, False), fixed)
+        _lib.check(self.lib.tf_apply(self.handle, ident, 0 if key is None else 1, _lib.ptr(columns), columns.shape[0],
+                                     _lib.ptr(out), self._stream()), self.handle, "tf_apply")
+        return out
+
+    def operator(self, grid, moduli=None, mask=None):
+        """y = mask * K (mask * u) on a grid [R, 3, padded nodes] (topology_multigrid.py:105-109)."""
+        if moduli is not None:
+            raise NotImplementedError("operator(moduli=...) is not supported; call update() instead")
+        grid = grid if mask is None else grid * mask
+        columns = self.flat(grid).T.contiguous().to(self.torch.float64)
+        result = self.grid(self.apply_device(columns).T, dtype=grid.dtype)
+        return result if mask is None else result * mask
+
+    def product(self, flat):
+        """K u for host columns (topology_multigrid.py:455-457)."""
+        flat = np.asarray(flat, dtype=float)
+        columns = self._columns(flat.reshape(len(flat), -1))
+        return self.apply_device(columns).T.cpu().numpy()
+
+    def element_energy(self, grid):
+        """u_e^T K0 u_e per column and element, padded element grid [R, *padded] (topology_multigrid.py:458-459)."""
+        torch = self.torch
+        columns = self.flat(grid).T.contiguous().to(torch.float64)
+        energy = self.energy_device(columns)
+        out = torch.zeros((columns.shape[0],) + self.padded, dtype=torch.float64, device=self.device)
+        out[:, :self.shape[0], :self.shape[1], :self.shape[2]] = energy.reshape((-1,) + self.shape)
+        return out
+
+    def energy_device(self, columns, combination=None, coefficients=None, scale=None, out=None, accumulate=False):
+        """Element energies on device columns [R, ndof].
+
+        Without ``coefficients`` returns per-column energies [R, nelem].  With
+        ``coefficients`` returns the weighted sum  scale * sum_j c_j w_j^T K0 w_j
+        with w_j = columns[j] (``combination`` None) or w_j = sum_r combination[r, j] columns[r].
+        """
+        torch = self.torch
+        count = columns.shape[0]
+        per_column = coefficients is None
+        if per_column:
+            out = torch.empty((count, self.nelem), dtype=torch.float64, device=self.device) if out is None else out
+        else:
+            out = torch.zeros(self.nelem, dtype=torch.float64, device=self.device) if out is None else out
+        comb = None if combination is None else torch.as_tensor(combination, dtype=torch.float64, device=self.device).contiguous()
+        coef = None if coefficients is None else torch.as_tensor(coefficients, dtype=torch.float64, device=self.device).contiguous()
+        ncomb = 0 if comb is None else comb.shape[1]
+        _lib.check(self.lib.tf_element_energy(self.handle, _lib.ptr(columns), count, _lib.ptr(comb), ncomb, _lib.ptr(coef),
+                                              _lib.ptr(scale), _lib.ptr(out), 1 if accumulate else 0,
+                                              1 if per_column else 0, self._stream()), self.handle, "tf_element_energy")
+        return out
+
+    # ----------------------------------------------------------- lifecycle --
+    def diagnostics(self):
+        return {"settings": self.settings, "levels": [{"shape": list(level.shape), "spacing_mm": level.spacing.tolist()} for level in self.levels],
+                "padded_shape": list(self.padded), "solves": self.statistics[-64:]}
+
+    def close(self):
+        """Release the native handle; returns the list of cleanup errors (always empty or one entry)."""
+        errors = []
+        if getattr(self, "handle", None):
+            try:
+                self.lib.tf_destroy(self.handle)
+            except Exception as error:  # pragma: no cover - defensive
+                errors.append(str(error))
+            self.handle = None
+        return errors
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_elasticity(system, multigrid, physical_density, penalization=3.0, min_stiffness_ratio=1e-6):
+    """Compliance and sensitivities of every static case (topology_multigrid.py:553-581) on the device."""
+    torch = multigrid.torch
+    density = np.asarray(physical_density, dtype=float).ravel()
+    moduli = system.young * (min_stiffness_ratio + (1 - min_stiffness_ratio) * density ** penalization)
+    derivative = system.young * (1 - min_stiffness_ratio) * penalization * density ** (penalization - 1)
+    moduli[~system.active_elements] = 0
+    derivative[~system.active_elements] = 0
+    multigrid.update(moduli)
+    factor = 1.0 if system.symmetry is None else 2.0
+    results = {}
+    for members in system.groups.values():
+        part = members[0][1]
+        forces = np.column_stack([member["force"] for _, member in members])
+        columns = multigrid._columns(forces)
+        solutions, report = multigrid.solve_device(part["fixed"].tobytes(), part["fixed"], columns)
+        energies = multigrid.energy_device(solutions).cpu().numpy()
+        host = solutions.cpu().numpy()
+        for column, (case, member) in enumerate(members):
+            entry = results.setdefault(case["name"], {"compliance_n_mm": 0.0, "energy": np.zeros(system.nelem), "relative_residual": 0.0, "iterations": [], "fields": {}})
+            entry["compliance_n_mm"] += factor * float(member["force"] @ host[column])
+            entry["energy"] += factor * energies[column]
+            entry["relative_residual"] = max(entry["relative_residual"], report["relative_residual"][column])
+            entry["iterations"].append(report["iterations"][column])
+            entry["fields"][member["sign"]] = host[column]
+    for entry in results.values():
+        entry["derivative"] = -derivative * entry.pop("energy")
+    return results

@@ -1,0 +1,158 @@
+/*
+ * C ABI of the B200 (sm_100a) hex8 SIMP topology-optimisation hot path.
+ *
+ * Every entry point returns an int status (0 = ok, see TF_STATUS_*) and stores
+ * a message retrievable with tf_last_error().  Device pointers are raw CUDA
+ * pointers owned by the caller; `stream` is a cudaStream_t passed as void*
+ * (NULL = legacy default stream).  Dense right-hand-side / solution blocks are
+ * column-contiguous: column c of an [ndof x R] block starts at ptr + c * ndof,
+ * i.e. a Fortran-ordered NumPy [ndof, R] array, with dof = 3 * node + component
+ * and nodes in C order over (nx+1, ny+1, nz+1).
+ *
+ * The reference interface each function replaces is cited beside it
+ * (paths inside the reference project AAPPHH/Deep_Frame).
+ */
+#ifndef TF_B200_H
+#define TF_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TF_API __attribute__((visibility("default")))
+#else
+#define TF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TF_STATUS_OK = 0,
+  TF_STATUS_INVALID = 1,        /* bad argument: ValueError in the reference */
+  TF_STATUS_CUDA = 2,           /* CUDA runtime failure */
+  TF_STATUS_NOT_CONVERGED = 3,  /* PCG did not reach the tolerance */
+  TF_STATUS_NUMERIC = 4,        /* breakdown (non-SPD coarsest matrix, non-finite values) */
+  TF_STATUS_INTERNAL = 5
+};
+
+enum { TF_PRECISION_FLOAT64 = 0, TF_PRECISION_FLOAT32 = 1, TF_PRECISION_BFLOAT16 = 2, TF_PRECISION_FLOAT16 = 3 };
+enum { TF_SMOOTHER_JACOBI = 0, TF_SMOOTHER_CHEBYSHEV = 1 };
+enum { TF_CYCLE_V = 0, TF_CYCLE_W = 1 };
+enum { TF_COARSE_GALERKIN = 0, TF_COARSE_REDISCRETIZE = 1 };
+
+typedef struct tf_handle tf_handle;
+
+/* Structured grid of shape[0] x shape[1] x shape[2] hex8 elements. */
+typedef struct tf_grid {
+  int64_t shape[3];
+  double spacing[3];
+} tf_grid;
+
+/* Multigrid settings; same meaning as the reference's MULTIGRID dict
+ * (deep_frame/topology_multigrid.py:8-11). */
+typedef struct tf_settings {
+  int32_t precision;          /* work precision of the V-cycle (TF_PRECISION_*) */
+  int32_t smoother;           /* TF_SMOOTHER_* */
+  int32_t cycle;              /* TF_CYCLE_* */
+  int32_t coarse;             /* TF_COARSE_* */
+  int32_t sweeps;             /* Jacobi sweeps on the finest level (x growth^level below) */
+  int32_t chebyshev_degree;   /* Chebyshev degree on the finest level (x growth^level below) */
+  int32_t max_levels;
+  int32_t power_iterations;   /* lambda_max(D^-1 A) power iterations per level */
+  int32_t max_iterations;     /* PCG iteration limit */
+  int32_t retries;            /* FP64 re-runs of columns that missed the tolerance */
+  int32_t batch;              /* columns per PCG launch (0 = all live columns at once) */
+  int32_t reserved;
+  int64_t coarsest_dofs;      /* level count grows until the coarsest grid has <= this many dofs */
+  double damping;             /* Jacobi damping */
+  double chebyshev_ratio;     /* lambda_max / lambda_min of the Chebyshev interval */
+  double growth;              /* smoothing growth factor per level */
+  double tolerance;           /* relative residual of the recomputed true residual */
+  double dead_ratio;          /* coarse dofs with diag <= dead_ratio * max(diag) are dropped */
+  double zero_rhs;            /* columns with norm <= zero_rhs * max norm are skipped */
+} tf_settings;
+
+/* Solve report (deep_frame/topology_multigrid.py:367-373).  Arrays are caller-owned. */
+typedef struct tf_report {
+  int32_t* iterations;        /* [nrhs] or NULL */
+  double* relative_residual;  /* [nrhs] or NULL */
+  double* history;            /* [history_capacity] max relative residual per PCG step, or NULL */
+  int32_t history_capacity;
+  int32_t history_len;
+  int32_t converged;
+  int32_t batches;
+  int32_t retried_columns;
+  int32_t zero_rhs_columns;
+  int32_t levels;
+  int32_t steps;
+  int64_t coarsest_dofs;
+  double seconds;
+  double setup_s;
+  double lambda_max[16];
+} tf_report;
+
+/* Fill `s` with the library defaults (the reference's MULTIGRID values, with
+ * coarsest_dofs sized for a dense coarsest factor). */
+TF_API int tf_default_settings(tf_settings* s);
+
+/* GeometricMultigrid.__init__(shape, spacing, ke, settings, me)
+ * (deep_frame/topology_multigrid.py:47-79).  ke, me: 24x24 row-major FP64 host
+ * arrays (me may be NULL). */
+TF_API int tf_create(const tf_grid* grid, const double* ke, const double* me, const tf_settings* settings, tf_handle** out);
+
+/* Level count and padded element shape chosen at creation (topology_multigrid.py:58-63). */
+TF_API int tf_levels(const tf_handle* h, int32_t* levels, int64_t padded[3]);
+
+/* GeometricMultigrid.update(moduli) (topology_multigrid.py:97-100): element moduli
+ * [nelem] FP64 on the device, C order; drops every cached hierarchy. */
+TF_API int tf_update(tf_handle* h, const double* moduli_dev, void* stream);
+
+/* Register the Dirichlet dof set of hierarchy `key` (the `fixed` argument of
+ * GeometricMultigrid.solve / .hierarchy, topology_multigrid.py:145,336).  Host
+ * array of unpadded dof indices; the hierarchy itself is built lazily by tf_solve. */
+TF_API int tf_set_bc(tf_handle* h, uint64_t key, const int64_t* fixed, int64_t count);
+
+/* GeometricMultigrid.solve(key, fixed, forces) (topology_multigrid.py:336-375) for a
+ * Dirichlet-supported key: f_dev [nrhs][ndof] in, u_dev [nrhs][ndof] out (device FP64). */
+TF_API int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
+             void* stream);
+
+/* GeometricMultigrid.hierarchy(key, fixed) (topology_multigrid.py:145-208): build (or reuse)
+ * the hierarchy of `key` now and fill the level fields of `report` (levels, coarsest_dofs,
+ * setup_s, lambda_max); report may be NULL. */
+TF_API int tf_prepare(tf_handle* h, uint64_t key, tf_report* report, void* stream);
+
+/* GeometricMultigrid.precondition (topology_multigrid.py:318-324): z = M^-1 r with one
+ * V-cycle of the hierarchy of `key`, the residual scaled by max|r| per column.
+ * r_dev, z_dev: [nrhs][ndof] device FP64. */
+TF_API int tf_precondition(tf_handle* h, uint64_t key, const double* r_dev, int32_t nrhs, double* z_dev, void* stream);
+
+/* GeometricMultigrid.operator (topology_multigrid.py:105-109) / .product (:455-457):
+ * y = K(E) u for nrhs columns; with use_mask != 0 the live mask of `key` is applied
+ * to input and output (the reduced operator used by PCG). */
+TF_API int tf_apply(tf_handle* h, uint64_t key, int32_t use_mask, const double* u_dev, int32_t nrhs, double* y_dev,
+             void* stream);
+
+/* GeometricMultigrid.element_energy (topology_multigrid.py:458-459) and the
+ * sensitivity sums of HexElasticity._collect (topology_optimization.py:721-734) /
+ * InterfaceCovariance.energy (topology_problem.py:647-652):
+ *   per_column != 0:  out[c][e] = u_c,e^T K0 u_c,e                 (out is [nrhs][nelem])
+ *   otherwise:        out[e] (+)= scale[e] * sum_j coef[j] * w_j,e^T K0 w_j,e
+ * with w_j = u_j (comb == NULL, ncomb ignored) or w_j = sum_c comb[c * ncomb + j] u_c.
+ * comb, coef, scale are device arrays and may be NULL (coef, scale default to 1). */
+TF_API int tf_element_energy(tf_handle* h, const double* u_dev, int32_t nrhs, const double* comb_dev, int32_t ncomb,
+                      const double* coef_dev, const double* scale_dev, double* out_dev, int32_t accumulate,
+                      int32_t per_column, void* stream);
+
+/* Release the handle and every device buffer it owns (GeometricMultigrid.close,
+ * topology_multigrid.py:543-548).  Idempotent for NULL. */
+TF_API int tf_destroy(tf_handle* h);
+
+/* Message of the last failed call on `h` (or of the last failed tf_create when h is NULL). */
+TF_API const char* tf_last_error(const tf_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TF_B200_H */

@@ -1,0 +1,94 @@
+"""GMG-PCG solves vs a direct sparse solve of the oracle's assembled matrix.
+
+Mirrors tests/test_topology_multigrid.py:55-72 (PCG = spsolve to 1e-6) and
+:178-188 (zero RHS columns skip PCG) of the reference, over the settings the
+reference exposes (precision, smoother, cycle).
+"""
+import numpy as np
+import pytest
+from scipy.sparse.linalg import spsolve
+
+from oracle import hex8, operator as op
+
+pytestmark = pytest.mark.gpu
+
+
+def cantilever(shape, seed=0):
+    """x = 0 face clamped, unit -z load at the bottom-edge centre of the free end; rho ~ U[0.01, 1]."""
+    k0, _, _ = hex8.element_matrices((1, 1, 1), 0.3)
+    rho = np.random.default_rng(seed).uniform(0.01, 1.0, int(np.prod(shape)))
+    moduli = 1e-9 + (1 - 1e-9) * rho ** 3
+    points = hex8.node_points(shape, (1, 1, 1))
+    fixed_nodes = np.flatnonzero(points[:, 0] == 0)
+    fixed = (3 * fixed_nodes[:, None] + np.arange(3)).ravel()
+    ndof = 3 * len(points)
+    force = np.zeros(ndof)
+    tip = np.flatnonzero((points[:, 0] == shape[0]) & (points[:, 1] == shape[1] // 2) & (points[:, 2] == 0))[0]
+    force[3 * tip + 2] = -1.0
+    return k0, rho, moduli, fixed, force
+
+
+def direct(shape, k0, moduli, fixed, forces):
+    matrix = op.assemble(shape, k0, moduli).tocsc()
+    live = op.live_dofs(shape, moduli, fixed)
+    out = np.zeros_like(forces)
+    reduced = matrix[live][:, live].tocsc()
+    sol = spsolve(reduced, forces[live])
+    out[live] = sol.reshape(out[live].shape)
+    return out
+
+
+@pytest.mark.parametrize("settings", [
+    {"precision": "float64", "smoother": "jacobi", "sweeps": 2, "tolerance": 1e-10},
+    {"precision": "float32", "smoother": "chebyshev", "tolerance": 1e-10},
+    {"precision": "float32", "smoother": "jacobi", "cycle": "W", "tolerance": 1e-10},
+    {"precision": "float64", "smoother": "chebyshev", "cycle": "W", "tolerance": 1e-10},
+])
+def test_pcg_matches_direct_solution(cuda, settings):
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    shape = (16, 8, 8)
+    k0, _, moduli, fixed, force = cantilever(shape)
+    rng = np.random.default_rng(7)
+    forces = np.column_stack([force, rng.normal(size=force.size), rng.normal(size=force.size)])
+    mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 200, **settings})
+    mg.update(moduli)
+    solution, report = mg.solve("clamped", fixed, forces)
+    assert report["converged"], report
+    assert report["levels"] >= 3 and report["batches"] == 1
+    expected = direct(shape, k0, moduli, fixed, forces)
+    for c in range(forces.shape[1]):
+        assert np.linalg.norm(solution[:, c] - expected[:, c]) < 1e-6 * np.linalg.norm(expected[:, c])
+    # compliance to 1e-6 relative
+    assert force @ solution[:, 0] == pytest.approx(force @ expected[:, 0], rel=1e-8)
+    assert all(r < settings["tolerance"] for r in report["relative_residual"])
+    mg.close()
+
+
+def test_zero_load_columns_skip_pcg(cuda):
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    shape = (8, 4, 4)
+    k0, _, moduli, fixed, force = cantilever(shape, 1)
+    mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 200, "precision": "float64", "tolerance": 1e-12})
+    mg.update(moduli)
+    forces = np.column_stack([force, 1e-20 * force])
+    flat, report = mg.solve("zero", fixed, forces)
+    single, _ = mg.solve("zero", fixed, forces[:, :1])
+    assert report["converged"] and report["zero_rhs_columns"] == 1 and report["iterations"][1] == 0
+    assert not np.any(flat[:, 1]) and np.linalg.norm(flat[:, 0] - single[:, 0]) <= 1e-12 * np.linalg.norm(single[:, 0])
+    mg.close()
+
+
+def test_batched_columns_match_single_columns(cuda):
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    shape = (12, 6, 6)
+    k0, _, moduli, fixed, force = cantilever(shape, 2)
+    rng = np.random.default_rng(3)
+    forces = rng.normal(size=(force.size, 5))
+    forces[fixed] = 0
+    mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 200, "tolerance": 1e-10, "batch": 2})
+    mg.update(moduli)
+    flat, report = mg.solve("c", fixed, forces)
+    assert report["batches"] == 3 and report["converged"]
+    expected = direct(shape, k0, moduli, fixed, forces)
+    assert np.linalg.norm(flat - expected) < 1e-7 * np.linalg.norm(expected)
+    mg.close()
