@@ -1,0 +1,348 @@
+"""Benchmark: seconds per 42-RHS covariance hex8 solve to 1e-8 relative residual.
+
+One step = one design update of the covariance-load plate half model
+(96 x 96 x 16 voxels, 479 859 dofs, mirror symmetry on x = 0): new element
+moduli, both multigrid hierarchies rebuilt (symmetric and antisymmetric
+fixture groups), and the 42 load directions of each half solved by batched
+FP64 GMG-PCG to a recomputed true relative residual below 1e-8 (84 column
+solves).  ``value`` times this with every input resident in HBM; ``e2e`` times
+the same step through the reference-facing API (``GeometricMultigrid.update``
+and ``.solve`` with host NumPy moduli / forces in and host solutions out).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1 (torchrun, one rank per GPU) the 42 directions of each half are
+sharded across ranks; the flexibility columns are gathered with one NCCL
+all-reduce per solve.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "42-RHS hex8 solve s @1e-8 resid; SIMP iter/s: learned+mixed vs plain FP64"
+CONFIG = "plate_96x96x16"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--precision", default="float32")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), float(data["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(config, precision, device):
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    spec = problems.CONFIGS[config]
+    domain, density, cov = problems.plate(spec["shape"], 0)
+    system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": spec["tolerance"], "device": str(device)})
+    model = InterfaceCovariance(system, cov, domain["interfaces"])
+    return spec, system, model, density
+
+
+def ours(args):
+    import torch
+    import torch.distributed as dist
+    from deep_frame_b200 import _lib
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    spec, system, model, density = build_problem(args.config, args.precision, device)
+    mg = system._multigrid()
+    moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
+    moduli = torch.as_tensor(moduli_host, device=device)
+    groups = model.groups()
+    # shard the columns of every fixture group across ranks (no collective inside the solve)
+    shards = []
+    for key, ks, forces in groups:
+        cols = np.arange(len(ks))[rank::world]
+        shards.append((key, ks[cols], forces[torch.as_tensor(cols, device=device)].contiguous()))
+    reports = []
+
+    def step():
+        mg.update_device(moduli)
+        out = []
+        for key, ks, forces in shards:
+            part = system.groups[key][0][1]
+            u, report = mg.solve_device(key, part["fixed"], forces)
+            out.append((key, ks, forces, u))
+            reports.append(report)
+        if world > 1:
+            # gather the flexibility columns: every rank holds F[:, local] = P^T U_local
+            lib = _lib.load()
+            flex = torch.zeros((model.rank, model.rank), dtype=torch.float64, device=device)
+            for key, ks, forces, u in out:
+                allp = dict((k, f) for k2, kk, f in groups for k in [k2])[key]
+                full_ks = [g[1] for g in groups if g[0] == key][0]
+                m, mloc = len(full_ks), len(ks)
+                part = torch.empty((m, mloc), dtype=torch.float64, device=device)
+                scratch = torch.empty(int(lib.tf_gram_scratch_size(m, mloc)), dtype=torch.float64, device=device)
+                _lib.check(lib.tf_gram(_lib.ptr(allp), m, _lib.ptr(u), mloc, u.shape[1], _lib.ptr(part), _lib.ptr(scratch), mg._stream()))
+                idx = torch.as_tensor(full_ks, device=device)
+                loc = torch.as_tensor(ks, device=device)
+                flex[idx[:, None], loc[None, :]] += model.factor * part
+            dist.all_reduce(flex)
+        return out
+
+    for _ in range(args.warmup):
+        step()
+    reports.clear()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = int(_lib.load().tf_launch_count())
+    with Clocks(local) as clocks:
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            step()
+        stop.record()
+        torch.cuda.synchronize()
+    launches = int(_lib.load().tf_launch_count()) - launches0
+    if world > 1:
+        dist.barrier()
+    ms = start.elapsed_time(stop) / args.steps
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    # per-kernel-class breakdown of one more step (CUDA events on the launching stream)
+    lib = _lib.load()
+    lib.tf_timers(mg.handle, 1, None, None, 0)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    step()
+    s1.record()
+    torch.cuda.synchronize()
+    import ctypes
+    n = len(_lib.TIMER_CLASSES)
+    tms, tcnt = (ctypes.c_double * n)(), (ctypes.c_int64 * n)()
+    _lib.check(lib.tf_timers(mg.handle, 0, tms, tcnt, n), mg.handle, "tf_timers")
+    breakdown = {name: {"ms": round(tms[i], 3), "launches": int(tcnt[i])} for i, name in enumerate(_lib.TIMER_CLASSES)}
+    profiled_step_ms = s0.elapsed_time(s1)
+    iters = [int(np.max(r["iterations"])) for r in reports[-len(shards):]]
+    result = {"ms": ms, "launches_per_step": launches / args.steps, "breakdown": breakdown, "profiled_step_ms": profiled_step_ms,
+              "iterations_max": iters, "clocks": clocks.summary(), "world": world, "rank": rank,
+              "columns": [len(ks) for _, ks, _ in shards], "ndof": system.ndof, "levels": reports[-1]["levels"],
+              "coarsest_dofs": reports[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in reports)}
+    # roofline of the dominant kernel class: the finest-level operator (fine_work = V-cycle smoothing at the work precision)
+    dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
+    nodes = int(np.prod(np.asarray(mg.padded) + 1))
+    cols = sum(len(ks) for _, ks, _ in shards)
+    result["dominant"] = dominant
+    if breakdown[dominant]["launches"]:
+        per_launch_ms = breakdown[dominant]["ms"] / breakdown[dominant]["launches"]
+        result["dominant_per_launch_ms"] = per_launch_ms
+    # end-to-end through the host API (NumPy in / NumPy out), rank 0 at N = 1
+    if world == 1 and not args.no_e2e:
+        host_forces = [(key, forces.T.cpu().numpy().copy()) for key, _, forces in shards]
+        h2d = moduli_host.nbytes + sum(f.nbytes for _, f in host_forces)
+        d2h = sum(f.nbytes for _, f in host_forces)
+
+        def e2e_step():
+            mg.update(moduli_host)
+            outs = []
+            for key, f in host_forces:
+                part = system.groups[key][0][1]
+                outs.append(mg.solve(key, part["fixed"], f)[0])
+            return outs
+
+        e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        result["e2e"] = {"ms": e0.elapsed_time(e1) / args.steps, "wall_ms": (time.perf_counter() - t0) * 1e3 / args.steps,
+                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+    result["nodes"], result["cols"] = nodes, cols
+    if world > 1:
+        dist.destroy_process_group()
+    return result, system, model, density
+
+
+def cpu_sample(system, model, density, iterations_gpu, seconds_budget=20.0):
+    """The oracle's CPU GMG-PCG on one column of each half, a bounded number of PCG iterations."""
+    from oracle.gmg import MultigridOracle
+    moduli, _ = system.moduli(density, 3.0, 1e-9)
+    t_setup = 0.0
+    t_iter = []
+    for key, members in system.groups.items():
+        part = members[0][1]
+        t0 = time.perf_counter()
+        mg = MultigridOracle(system.shape, system.ke, moduli, part["fixed"], {"tolerance": 1e-8})
+        t_setup += time.perf_counter() - t0
+        force = members[0][1]["force"]
+        t0 = time.perf_counter()
+        iters = 3
+        mg.solve(force, max_iterations=iters)
+        t_iter.append((time.perf_counter() - t0) / iters)
+    cols = sum(len(m) for m in system.groups.values())
+    per_col_iter = float(np.mean(t_iter))
+    total_iters = float(np.mean(iterations_gpu)) if iterations_gpu else 40.0
+    value = t_setup + per_col_iter * cols * total_iters
+    return value, {"setup_s": t_setup, "per_column_iteration_s": per_col_iter, "columns": cols, "iterations": total_iters}
+
+
+def reference(args):
+    """--impl reference: the oracle's CPU restatement of the reference GMG-PCG path, on this box's host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from deep_frame_b200 import problems
+    from deep_frame_b200.elasticity import HexElasticity
+    from deep_frame_b200.covariance import InterfaceCovariance
+    spec = problems.CONFIGS[args.config]
+    domain, density, cov = problems.plate(spec["shape"], 0)
+    system = HexElasticity(domain)
+    InterfaceCovariance(system, cov, domain["interfaces"])
+    values = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        value, sample = cpu_sample(system, None, density, [])
+        if i >= args.warmup:
+            values.append(value)
+    v = float(np.mean(values))
+    cores = 1
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": system.ndof, "tolerance": 1e-8},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
+                             "sample": f"oracle GMG-PCG (NumPy/SciPy, 1 thread): full hierarchy set-up of both halves + 3 PCG iterations of one column per half, "
+                                       f"scaled to {sample['columns']} columns x {sample['iterations']:.0f} iterations"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return line
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference(args)
+        return
+    result, system, model, density = ours(args)
+    if result["rank"] != 0:
+        return
+    hbm, bf16, source = peaks()
+    ms = result["ms"]
+    # algorithmic bytes of one launch of the dominant kernel: every node reads its 3 input values and
+    # writes 3 outputs per column (+ the element moduli once per column launch)
+    dominant = result["dominant"]
+    word = 8 if dominant == "fine_fp64" or args.precision == "float64" else 4
+    nodes, cols = result["nodes"], result["cols"]
+    per_launch_cols = cols / max(1, len(result["columns"]))
+    traffic_alg = nodes * per_launch_cols * (6 * word) + nodes * per_launch_cols * word
+    roof = None
+    if "dominant_per_launch_ms" in result:
+        achieved = traffic_alg / (result["dominant_per_launch_ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "traffic": None, "kernel": dominant, "peak_source": source,
+                "per_launch_ms": round(result["dominant_per_launch_ms"], 4), "algorithmic_bytes_per_launch": int(traffic_alg)}
+    cpu = None
+    if not args.no_cpu and result["world"] == 1:
+        value, sample = cpu_sample(system, model, density, result["iterations_max"])
+        cpu = {"value": round(value, 2), "unit": "s", "cores": 1, "kind": "port",
+               "sample": f"oracle GMG-PCG (NumPy/SciPy, 1 thread): hierarchy set-up of both halves + 3 PCG iterations of one column per half, "
+                         f"scaled to {sample['columns']} columns x {sample['iterations']:.0f} iterations"}
+    line = {"metric": METRIC, "value": round(ms / 1e3, 6), "unit": "s", "n_gpus": result["world"], "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
+                       "outer": "fp64 PCG", "vcycle": args.precision, "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
+                       "pcg_iterations": result["iterations_max"], "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
+                       "parallelism": f"rhs-sharded x{result['world']}"},
+            "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),
+            "roofline": roof, "cpu_baseline": cpu, "breakdown_ms": result["breakdown"], "converged": result["converged"]}
+    if "e2e" in result:
+        e = result["e2e"]
+        line["e2e"] = {"value": round(e["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": e["h2d_bytes_per_step"],
+                       "d2h_bytes_per_step": e["d2h_bytes_per_step"]}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

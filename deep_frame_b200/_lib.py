@@ -17,7 +17,9 @@ COARSE = {"galerkin": 0, "rediscretize": 1}
 
 # every symbol include/tf_b200.h declares (checked by the CPU test suite)
 SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set_bc", "tf_prepare", "tf_precondition",
-           "tf_solve", "tf_apply", "tf_element_energy", "tf_destroy", "tf_last_error")
+           "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_timers", "tf_launch_count",
+           "tf_destroy", "tf_last_error")
+TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
 
 
 class TfSettings(ctypes.Structure):
@@ -75,13 +77,17 @@ def load():
             "tf_solve": [P, U64, P, I32, P, ctypes.POINTER(TfReport), P],
             "tf_apply": [P, U64, I32, P, I32, P, P],
             "tf_element_energy": [P, P, I32, P, I32, P, P, P, I32, I32, P],
+            "tf_gram": [P, I32, P, I32, I64, P, P, P],
+            "tf_gram_scratch_size": [I32, I32],
+            "tf_timers": [P, I32, ctypes.POINTER(D), ctypes.POINTER(I64), I32],
+            "tf_launch_count": [],
             "tf_destroy": [P],
             "tf_last_error": [P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_char_p if name == "tf_last_error" else ctypes.c_int
+            fn.restype = {"tf_last_error": ctypes.c_char_p, "tf_gram_scratch_size": ctypes.c_int64, "tf_launch_count": ctypes.c_int64}.get(name, ctypes.c_int)
         _lib = lib
         return lib
 

@@ -1,0 +1,151 @@
+"""Covariance load model on the device: 42-direction RHS, tr(K^-1 Sigma), lambda_max, KS.
+
+Host-side mirror of the reference's ``InterfaceCovariance``
+(deep_frame/topology_problem.py:572-684):
+* Sigma = D D^T from its eigenpairs, rank = eigenvalues above 1e-10 * max (:584-590);
+* unit-wrench minimum-norm nodal forces f = B^T (B B^T)^-1 e_j per interface,
+  mirrored on half models (:624-638);
+* one static case per direction, RHS_k = sum_j D_jk f_j, registered on the
+  support case and split into +/- parts by ``HexElasticity`` (:599-611);
+* ``measure``: F = sym(sum_parts factor P^T U), tr F, lambda_max and the KS
+  aggregate, and the sensitivities of tr and of the KS-weighted eigenvalues
+  (:657-684).
+Solves, F = P^T U, and the sensitivity sums run on the GPU (libtfb200.so);
+only the rank x rank eigen-decomposition of F runs on the host.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+DOFS = ["Fx", "Fy", "Fz", "Mx", "My", "Mz"]
+SETTINGS = {"prefix": "sigma_", "ks": 50.0, "ks_cutoff": 1e-9, "limits": {"mean_n_mm": None, "worst_n_mm": None}}
+
+
+class InterfaceCovariance:
+    def __init__(self, system, settings, interfaces):
+        self.system = system
+        self.settings = {**SETTINGS, **settings}
+        sigma = np.asarray(self.settings["sigma"], dtype=float)
+        labels = [tuple(label) for label in self.settings["labels"]]
+        missing = sorted({name for name, _ in labels} - set(interfaces))
+        if missing:
+            raise ValueError("Covariance interfaces missing from the domain: " + ", ".join(missing))
+        values, vectors = np.linalg.eigh((sigma + sigma.T) / 2)
+        values, vectors = values[::-1], vectors[:, ::-1]
+        if values[-1] < -1e-9 * values[0]:
+            raise ValueError("Load covariance is not positive semidefinite")
+        self.sigma, self.labels = sigma, labels
+        self.rank = int(np.sum(values > 1e-10 * values[0]))
+        self.directions = vectors[:, :self.rank] * np.sqrt(values[:self.rank])
+        self.factor = 1.0 if system.symmetry is None else 2.0
+        units = {name: self.wrenches(interfaces[name]) for name in dict.fromkeys(name for name, _ in labels)}
+        columns = [units[name][DOFS.index(dof)] for name, dof in labels]
+        self.cases, self.forces = [], []
+        for k in range(self.rank):
+            force, mirrored = np.zeros(system.ndof), np.zeros(system.ndof)
+            for weight, (direct, direct_values, mirror, mirror_values) in zip(self.directions[:, k], columns):
+                np.add.at(force, direct, weight * direct_values)
+                np.add.at(mirrored, mirror, weight * mirror_values)
+            case = system.add_case(self.settings["prefix"] + str(k), self.settings["support"], force, mirrored)
+            self.cases.append(case["name"])
+            self.forces.append({part["sign"]: part["force"] for part in case["parts"]})
+        self._groups = None
+
+    def wrenches(self, interface):
+        system = self.system
+        picked = [system._select_both(region, "covariance", "load") for region in interface["regions"]]
+        direct, mirror = (np.unique(np.concatenate([item[side] for item in picked])) for side in (0, 1))
+        flip = np.ones(3) if system.symmetry is None else system._flip()
+        arms = np.concatenate([system.points[direct], system.points[mirror] * flip]) - np.asarray(interface["reference_mm"], dtype=float)
+        if np.linalg.matrix_rank(arms - arms[0], tol=1e-8) < 2:
+            raise ValueError("An interface wrench needs at least three non-collinear nodes")
+        b = np.zeros((6, 3 * len(arms)))
+        for index, (x, y, z) in enumerate(arms):
+            b[:3, 3 * index:3 * index + 3] = np.eye(3)
+            b[3:, 3 * index:3 * index + 3] = [[0, -z, y], [z, 0, -x], [-y, x, 0]]
+        nodal = (b.T @ np.linalg.solve(b @ b.T, np.eye(6))).reshape(len(arms), 3, 6)
+        dofs = lambda nodes: (3 * nodes[:, None] + np.arange(3)).ravel()
+        return [(dofs(direct), nodal[:len(direct), :, j].ravel(), dofs(mirror), (nodal[len(direct):, :, j] * flip).ravel()) for j in range(6)]
+
+    # ------------------------------------------------------------- device --
+    def groups(self):
+        """Per fixture group: (key, case indices k, device force block [m, ndof])."""
+        if self._groups is None:
+            mg = self.system._multigrid()
+            torch = mg.torch
+            index = {name: k for k, name in enumerate(self.cases)}
+            groups = []
+            for key, members in self.system.groups.items():
+                ks = [index[case["name"]] for case, _ in members if case["name"] in index]
+                if not ks:
+                    continue
+                if len(ks) != len(members):
+                    raise ValueError("covariance cases share a fixture group with other load cases")
+                forces = torch.as_tensor(np.stack([part["force"] for _, part in members]), dtype=torch.float64, device=mg.device)
+                groups.append((key, np.asarray(ks), forces))
+            self._groups = groups
+        return self._groups
+
+    def measure_device(self, physical_density, penalization=3.0, min_stiffness_ratio=1e-6, gradients=True):
+        """Solve every direction on the GPU and return the load_mean / load_worst rows."""
+        system = self.system
+        mg = system._multigrid()
+        torch = mg.torch
+        lib = _lib.load()
+        moduli, derivative = system.moduli(physical_density, penalization, min_stiffness_ratio)
+        mg.update(moduli)
+        scale = torch.as_tensor(-derivative, dtype=torch.float64, device=mg.device)
+        return self.measure_from(self.solve_all(), scale, gradients)
+
+    def solve_all(self):
+        system = self.system
+        solved = []
+        for key, ks, forces in self.groups():
+            u, report = system.solve_group_device(key, forces)
+            solved.append((key, ks, forces, u, report))
+        return solved
+
+    def measure_from(self, solved, scale, gradients=True):
+        """Rows of the reference's measure (topology_problem.py:657-684) from device solutions."""
+        mg = self.system._multigrid()
+        torch = mg.torch
+        lib = _lib.load()
+        flex = np.zeros((self.rank, self.rank))
+        for key, ks, forces, u, _ in solved:
+            m = len(ks)
+            out = torch.empty((m, m), dtype=torch.float64, device=mg.device)
+            scratch = torch.empty(int(lib.tf_gram_scratch_size(m, m)), dtype=torch.float64, device=mg.device)
+            _lib.check(lib.tf_gram(_lib.ptr(forces), m, _lib.ptr(u), m, forces.shape[1], _lib.ptr(out), _lib.ptr(scratch),
+                                   mg._stream()), None, "tf_gram")
+            flex[np.ix_(ks, ks)] += self.factor * out.cpu().numpy()
+        flex = (flex + flex.T) / 2
+        s = self.settings["ks"]
+        limits = self.settings["limits"]
+        mean = float(np.trace(flex))
+        values, vectors = np.linalg.eigh(flex)
+        values, vectors = values[::-1], vectors[:, ::-1]
+        worst = float(values[0])
+        ks_scale = limits.get("worst_n_mm") or worst
+        weights = np.exp(s * (values - worst) / ks_scale)
+        ks_value = worst + ks_scale * np.log(weights.sum()) / s
+        weights /= weights.sum()
+        rows = [{"name": "load_mean", "value": mean, "limit": limits.get("mean_n_mm"), "unit": "N mm", "sense": "<=", "g": None, "gradient": None},
+                {"name": "load_worst", "value": worst, "limit": limits.get("worst_n_mm"), "unit": "N mm", "sense": "<=", "g": None, "gradient": None,
+                 "info": {"eigenvalues_n_mm": values[:6].tolist(), "ks_n_mm": float(ks_value), "ks": s, "rank": self.rank}}]
+        if gradients:
+            grad_mean = torch.zeros(self.system.nelem, dtype=torch.float64, device=mg.device)
+            grad_worst = torch.zeros_like(grad_mean)
+            keep = np.flatnonzero(weights > self.settings["ks_cutoff"])
+            for key, ks, forces, u, _ in solved:
+                m = len(ks)
+                mg.energy_device(u, coefficients=np.full(m, self.factor), scale=scale, out=grad_mean, accumulate=True)
+                comb = vectors[np.ix_(ks, keep)]
+                mg.energy_device(u, combination=comb, coefficients=weights[keep] * self.factor, scale=scale, out=grad_worst, accumulate=True)
+            limit_mean = limits.get("mean_n_mm") or 1.0
+            limit_worst = limits.get("worst_n_mm") or 1.0
+            rows[0].update(g=mean / limit_mean - 1, gradient=grad_mean / limit_mean)
+            rows[1].update(g=float(ks_value / limit_worst - 1), gradient=grad_worst / limit_worst)
+        self.flexibility = flex
+        return rows

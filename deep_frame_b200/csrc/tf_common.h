@@ -1,6 +1,7 @@
 // Shared host-side helpers of the sm_100a topology-optimisation library.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -27,8 +28,15 @@ inline void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess)
     throw Error(TF_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+// Number of kernels this library has launched in the process (reported by tf_launch_count).
+extern std::atomic<long long> g_launch_count;
+
 #define TF_CUDA_CHECK(x) ::tfb::cuda_check((x), #x)
-#define TF_LAUNCH_CHECK(name) ::tfb::cuda_check(cudaGetLastError(), name)
+#define TF_LAUNCH_CHECK(name) \
+  do {                                                  \
+    ::tfb::g_launch_count.fetch_add(1, std::memory_order_relaxed); \
+    ::tfb::cuda_check(cudaGetLastError(), name);        \
+  } while (0)
 
 inline void require(bool ok, const std::string& m) {
   if (!ok) throw Error(TF_INVALID, m);

@@ -75,6 +75,58 @@ inline dim3 cols_grid(long long n, int ncol, int block = 256, int cap = 1184) {
   return dim3(grid_for(n, block, cap), ncol);
 }
 
+// Optional CUDA-event timing of kernel classes on the launching stream.
+enum TimerClass : int {
+  TIMER_FINE64 = 0,    // FP64 finest-level operator of the PCG (apply and true residual)
+  TIMER_FINE_WORK = 1, // finest-level smoother / residual in the work precision
+  TIMER_COARSE = 2,    // Galerkin-level operators
+  TIMER_TRANSFER = 3,  // restriction and prolongation
+  TIMER_VECTOR = 4,    // PCG reductions and vector updates
+  TIMER_COARSEST = 5,  // dense coarsest solve
+  TIMER_SETUP = 6,     // hierarchy build (masks, Galerkin blocks, lambda_max, factor)
+  TIMER_ENERGY = 7,    // element energies
+  TIMER_CLASSES = 8
+};
+
+struct Timers {
+  bool enabled = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  std::vector<int> cls;
+  size_t used = 0;
+  ~Timers() {
+    for (auto& e : pool) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+  }
+  std::pair<cudaEvent_t, cudaEvent_t>* next(int c) {
+    if (used == pool.size()) {
+      cudaEvent_t a, b;
+      TF_CUDA_CHECK(cudaEventCreate(&a));
+      TF_CUDA_CHECK(cudaEventCreate(&b));
+      pool.push_back({a, b});
+      cls.push_back(c);
+    }
+    cls[used] = c;
+    return &pool[used++];
+  }
+};
+
+struct TimedRange {
+  Timers* t;
+  cudaStream_t s;
+  std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+  TimedRange(Timers& timers, int c, cudaStream_t stream) : t(&timers), s(stream) {
+    if (t->enabled) {
+      ev = t->next(c);
+      cudaEventRecord(ev->first, s);
+    }
+  }
+  ~TimedRange() {
+    if (ev) cudaEventRecord(ev->second, s);
+  }
+};
+
 }  // namespace
 
 struct tf_handle {
@@ -106,6 +158,7 @@ struct tf_handle {
   size_t ccap = 0;
   VBufs<float> wf;
   VBufs<double> wd;
+  Timers timers;
   std::string err;
   ~tf_handle() {
     if (host_flags) cudaFreeHost(host_flags);
@@ -218,7 +271,8 @@ template <> const K0Param<double>& k0param<double>(tf_handle* h) { return h->k64
 template <> const K0Param<float>& k0param<float>(tf_handle* h) { return h->k32; }
 
 template <typename T>
-void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st) {
+void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st, int timer = -1) {
+  TimedRange tr(h->timers, timer >= 0 ? timer : (l == 0 ? TIMER_FINE_WORK : TIMER_COARSE), st);
   if (l == 0) {
     dim3 grid(grid_for(a.g.nnode, 256, 4096), a.ncol);
     fine_level_kernel<T><<<grid, 256, 0, st>>>(k0param<T>(h), a, mode);
@@ -248,6 +302,7 @@ LevelArgs<T> level_args(tf_handle* h, Hierarchy& hy, int l, int ncol, const int*
 
 template <typename T>
 void coarsest_solve(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int ncol, const int* active, cudaStream_t st) {
+  TimedRange tr(h->timers, TIMER_COARSEST, st);
   const int l = h->nlev - 1;
   const long long nd = 3 * h->geo[l].nnode;
   const int n = hy.n_live;
@@ -338,11 +393,15 @@ void vcycle(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, int ncol, const in
     a.b = vb.b[l].template as<T>();
     a.y = vb.res[l].template as<T>();
     launch_level<T>(h, l, a, MODE_RESID, st);
+    {
+    TimedRange tr(h->timers, TIMER_TRANSFER, st);
     restrict_kernel<T><<<cols_grid(cg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.res[l].template as<T>(), 3 * fg.nnode,
                                                                   vb.b[l + 1].template as<T>(), 3 * cg.nnode,
                                                                   hy.lv[l + 1].mask.as<uint8_t>(), active);
     TF_LAUNCH_CHECK("restrict_kernel");
+    }
     vcycle<T>(h, hy, vb, l + 1, ncol, active, st);
+    TimedRange tr(h->timers, TIMER_TRANSFER, st);
     prolong_add_kernel<T><<<cols_grid(fg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.x[l + 1].template as<T>(), 3 * cg.nnode,
                                                                      vb.x[l].template as<T>(), 3 * fg.nnode,
                                                                      hy.lv[l].mask.as<uint8_t>(), active);
@@ -385,6 +444,11 @@ double power_lambda(tf_handle* h, Hierarchy& hy, int l, cudaStream_t st) {
 
 void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st) {
   auto t0 = std::chrono::steady_clock::now();
+  const bool timing = h->timers.enabled;
+  h->timers.enabled = false;   // the set-up is timed as one range below
+  struct Restore { Timers& t; bool v; ~Restore() { t.enabled = v; } } restore{h->timers, timing};
+  std::pair<cudaEvent_t, cudaEvent_t>* range = timing ? h->timers.next(TIMER_SETUP) : nullptr;
+  if (range) cudaEventRecord(range->first, st);
   const bool dbl = work_is_double(h);
   ensure_scratch(h, 1);
   hy.lv.clear();
@@ -502,6 +566,7 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     dense_trinv(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), st);
     TF_CUDA_CHECK(cudaStreamSynchronize(st));
   }
+  if (range) cudaEventRecord(range->second, st);
   hy.setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   hy.setup_reported = false;
 }
@@ -537,15 +602,21 @@ void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int
   const long long n = 3 * h->geo[0].nnode;
   VBufs<T>& vb = vbufs<T>(h);
   dim3 gr(grid_for(n, RED_THREADS, PCG_BLOCKS), ncol);
+  {
+  TimedRange tr_(h->timers, TIMER_VECTOR, s);
   pcg_prep_kernel<<<gr, RED_THREADS, 0, s>>>(h->vr.as<double>(), h->vz.as<double>(), n, st, initial ? 0 : 1);
   TF_LAUNCH_CHECK("pcg_prep_kernel");
   pcg_to_work_kernel<T><<<cols_grid(n, ncol), 256, 0, s>>>(h->vr.as<double>(), n, st, vb.b[0].template as<T>());
   TF_LAUNCH_CHECK("pcg_to_work_kernel");
+  }
   vcycle<T>(h, hy, vb, 0, ncol, st.active, s);
+  {
+  TimedRange tr_(h->timers, TIMER_VECTOR, s);
   pcg_from_work_kernel<T><<<gr, RED_THREADS, 0, s>>>(vb.x[0].template as<T>(), h->vr.as<double>(), h->vz.as<double>(), n, st, initial);
   TF_LAUNCH_CHECK("pcg_from_work_kernel");
   pcg_direction_kernel<<<cols_grid(n, ncol), 256, 0, s>>>(h->vz.as<double>(), h->vp.as<double>(), n, st, initial);
   TF_LAUNCH_CHECK("pcg_direction_kernel");
+  }
 }
 
 // FP64 fine operator with mask (the PCG operator, topology_multigrid.py:411)
@@ -562,7 +633,7 @@ void fine_apply64(tf_handle* h, Hierarchy& hy, const double* u, const double* b,
   a.ncol = ncol;
   a.active = active;
   a.gate = gate;
-  launch_level<double>(h, 0, a, mode, s);
+  launch_level<double>(h, 0, a, mode, s, TIMER_FINE64);
 }
 
 struct PcgResult {
@@ -605,19 +676,25 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
   for (int c = 0; c < ncol; ++c) n_active += run[c];
   while (n_active > 0 && step < limit) {
     fine_apply64(h, hy, h->vp.as<double>(), nullptr, h->vq.as<double>(), MODE_APPLY, ncol, st.active, nullptr, s);
-    pcg_alpha_kernel<<<gr, RED_THREADS, 0, s>>>(h->vp.as<double>(), h->vq.as<double>(), n, st);
+    {
+  TimedRange tr_(h->timers, TIMER_VECTOR, s);
+  pcg_alpha_kernel<<<gr, RED_THREADS, 0, s>>>(h->vp.as<double>(), h->vq.as<double>(), n, st);
     TF_LAUNCH_CHECK("pcg_alpha_kernel");
     ++step;
     pcg_update_kernel<<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), h->vr.as<double>(), h->vp.as<double>(), h->vq.as<double>(),
                                                  n, st, tol, step);
     TF_LAUNCH_CHECK("pcg_update_kernel");
+  }
     fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vq.as<double>(), MODE_RESID, ncol, st.active, st.flags, s);
-    pcg_truecheck_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, tol, step);
+    {
+  TimedRange tr_(h->timers, TIMER_VECTOR, s);
+  pcg_truecheck_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, tol, step);
     TF_LAUNCH_CHECK("pcg_truecheck_kernel");
     pcg_retire_kernel<<<ge, 256, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, step);
     TF_LAUNCH_CHECK("pcg_retire_kernel");
     pcg_flags_kernel<<<1, 256, 0, s>>>(st, step);
     TF_LAUNCH_CHECK("pcg_flags_kernel");
+  }
     TF_CUDA_CHECK(cudaMemcpyAsync(h->host_flags, st.flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
     n_active = h->host_flags[0];
@@ -1072,10 +1149,33 @@ extern "C" int tf_element_energy(tf_handle* h, const double* u_dev, int32_t nrhs
     require(!(per_column && comb_dev), "per_column energies take no combination matrix");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const long long ne = (long long)h->un.ex * h->un.ey * h->un.ez;
-    energy_kernel<double><<<grid_for(ne, 128, 148 * 16), 128, 0, s>>>(h->k64, h->un, u_dev, 3 * h->un.nnode, nrhs, comb_dev,
+    {
+  TimedRange tr_(h->timers, TIMER_ENERGY, s);
+  energy_kernel<double><<<grid_for(ne, 128, 148 * 16), 128, 0, s>>>(h->k64, h->un, u_dev, 3 * h->un.nnode, nrhs, comb_dev,
                                                                         comb_dev ? ncomb : nrhs, coef_dev, scale_dev, out_dev,
                                                                         accumulate, per_column);
     TF_LAUNCH_CHECK("energy_kernel");
+  }
+  });
+}
+
+extern "C" int tf_timers(tf_handle* h, int32_t enable, double* ms, int64_t* counts, int32_t nclasses) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(nclasses >= 0 && (nclasses == 0 || (ms && counts)), "invalid timer buffers");
+    if (nclasses > 0) {
+      for (int c = 0; c < nclasses; ++c) { ms[c] = 0.0; counts[c] = 0; }
+      for (size_t q = 0; q < h->timers.used; ++q) {
+        auto& e = h->timers.pool[q];
+        TF_CUDA_CHECK(cudaEventSynchronize(e.second));
+        float t = 0.f;
+        TF_CUDA_CHECK(cudaEventElapsedTime(&t, e.first, e.second));
+        const int c = h->timers.cls[q];
+        if (c < nclasses) { ms[c] += t; counts[c] += 1; }
+      }
+    }
+    h->timers.used = 0;
+    h->timers.enabled = enable != 0;
   });
 }
 

@@ -145,6 +145,26 @@ TF_API int tf_element_energy(tf_handle* h, const double* u_dev, int32_t nrhs, co
                       const double* coef_dev, const double* scale_dev, double* out_dev, int32_t accumulate,
                       int32_t per_column, void* stream);
 
+/* F = A B^T for column blocks A [ra][n] and B [rb][n] (device FP64, ra, rb <= 64): the
+ * flexibility P^T U of InterfaceCovariance.matrix (deep_frame/topology_problem.py:639-646).
+ * out_dev is [ra][rb]; scratch_dev holds tf_gram_scratch_size(ra, rb) doubles.  The
+ * reduction order is fixed, so results are bitwise reproducible. */
+TF_API int tf_gram(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
+                   double* scratch_dev, void* stream);
+TF_API int64_t tf_gram_scratch_size(int32_t ra, int32_t rb);
+
+/* CUDA-event timing of the kernel classes this handle launches, recorded on the launching
+ * stream: 0 FP64 finest operator of the PCG, 1 finest-level smoothing / residual in the work
+ * precision, 2 Galerkin-level operators, 3 restriction + prolongation, 4 PCG vector kernels,
+ * 5 dense coarsest solve, 6 hierarchy set-up, 7 element energies.  With nclasses > 0 the
+ * summed milliseconds and launch counts since the previous call are returned (after
+ * synchronising the recorded events) and the record is cleared; `enable` switches recording
+ * on or off for the calls that follow. */
+TF_API int tf_timers(tf_handle* h, int32_t enable, double* ms, int64_t* counts, int32_t nclasses);
+
+/* Kernels launched by this library in the calling process so far. */
+TF_API int64_t tf_launch_count(void);
+
 /* Release the handle and every device buffer it owns (GeometricMultigrid.close,
  * topology_multigrid.py:543-548).  Idempotent for NULL. */
 TF_API int tf_destroy(tf_handle* h);

@@ -1,0 +1,178 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own Python code.
+
+Run in a container that has the reference source tree:
+
+    python tests/golden/make_golden.py /root/reference
+
+The reference tree is copied to a scratch directory (its mount is read-only and
+pytest/pycache write files), imported, and run on the CPU: SciPy SuperLU for the
+direct solves, CPU torch for the reference's matrix-free operator and its
+density filter, and the reference's InterfaceCovariance for tr / lambda_max.
+Nothing under tests/ reads the reference at test time; only these .npz files.
+"""
+import shutil
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+OUT = Path(__file__).resolve().parent
+
+
+def load_reference(source):
+    scratch = Path(tempfile.mkdtemp(prefix="refcopy_"))
+    for name in ("deep_frame", "tests", "tools"):
+        shutil.copytree(Path(source) / name, scratch / name, ignore=shutil.ignore_patterns("__pycache__"))
+    sys.path.insert(0, str(scratch))
+    import deep_frame.topology_optimization as topt
+    import deep_frame.topology_multigrid as tmg
+    import deep_frame.topology_problem as tprob
+    return topt, tmg, tprob
+
+
+def box(lo, hi):
+    return {"kind": "box", "min_mm": list(map(float, lo)), "max_mm": list(map(float, hi))}
+
+
+def cantilever_domain(shape):
+    """The unit-voxel cantilever of the benchmark: x = 0 face clamped, unit -z load at node (Ex, Ey/2, 0)."""
+    ex, ey, ez = shape
+    t = 1e-6
+    allowed = np.ones(shape, dtype=bool)
+    return {"grid": {"shape": list(shape), "spacing_mm": [1.0, 1.0, 1.0], "origin_mm": [0.0, 0.0, 0.0], "order": "C", "axis_order": "xyz"},
+            "allowed": allowed, "preserve": np.zeros(shape, dtype=bool), "forbidden": ~allowed,
+            "material": {"young_modulus_mpa": 1.0, "poisson_ratio": 0.3, "density_g_cm3": 1.0},
+            "point_masses": [],
+            "load_cases": [{"name": "tip", "analysis": "static", "fixed_regions": [box([-t, -t, -t], [t, ey + t, ez + t])],
+                            "loads": [{"region": box([ex - t, ey // 2 - t, -t], [ex + t, ey // 2 + t, t]), "force_n": [0.0, 0.0, -1.0]}]}]}
+
+
+def hex8(topt):
+    out = {}
+    for name, spacing in (("unit", (1.0, 1.0, 1.0)), ("aniso", (2.0, 3.0, 4.0)), ("beam", (0.747, 0.753, 0.667))):
+        k, m, b = topt.hexahedron_matrices(spacing, 0.3)
+        out[f"{name}_spacing"] = np.asarray(spacing)
+        out[f"{name}_k0"], out[f"{name}_m0"], out[f"{name}_b"] = k, m, b
+    np.savez_compressed(OUT / "hex8.npz", **out)
+
+
+def operator(topt, tmg, tprob):
+    """Reference matrix-free operator (CPU torch) and assembled matrix products on the reference test domains."""
+    import torch
+    out = {}
+    from tests.test_topology_problem import tiny_domain
+    for name, domain in (("cantilever", tprob.cantilever_domain((8, 3, 5), 1.0)), ("tiny", tiny_domain())):
+        system = topt.HexElasticity(domain, linear_solver="cpu_superlu")
+        rng = np.random.default_rng(0)
+        density = np.clip(rng.uniform(0.3, 1.2, system.nelem), 0, 1)
+        moduli = system.young * (1e-6 + (1 - 1e-6) * density ** 3)
+        active = np.where(system.active_elements, moduli, 0)
+        mg = tmg.GeometricMultigrid(domain["grid"]["shape"], system.spacing, system.ke, {"device": "cpu", "coarsest_dofs": 200})
+        mg.update(active)
+        vectors = np.random.default_rng(1).normal(size=(system.ndof, 2))
+        vectors[np.setdiff1d(np.arange(system.ndof), system.active_dofs)] = 0
+        matrix = system.matrix(moduli).tocsr()
+        part = next(iter(system.groups.values()))[0][1]
+        masked = np.zeros_like(vectors)
+        masked[part["free"]] = vectors[part["free"]]
+        with torch.no_grad():
+            full = mg.flat(mg.operator(mg.grid(vectors))).cpu().numpy()
+            reduced = mg.flat(mg.operator(mg.grid(masked), mask=mg.mask(part["fixed"])[0])).cpu().numpy()
+        shape = tuple(domain["grid"]["shape"])
+        energy = mg.element_energy(mg.grid(vectors))[:, :shape[0], :shape[1], :shape[2]].reshape(2, -1).cpu().numpy()
+        out.update({f"{name}_shape": np.asarray(shape), f"{name}_spacing": system.spacing, f"{name}_ke": system.ke,
+                    f"{name}_moduli": active, f"{name}_vectors": vectors, f"{name}_assembled": matrix @ vectors,
+                    f"{name}_operator": full, f"{name}_fixed": part["fixed"], f"{name}_free": part["free"],
+                    f"{name}_reduced": reduced, f"{name}_reduced_expected": matrix[part["free"]][:, part["free"]] @ vectors[part["free"]],
+                    f"{name}_energy": energy})
+    np.savez_compressed(OUT / "operator.npz", **out)
+
+
+def direct(topt, shape, seed, name):
+    """Reference SuperLU compliance / sensitivities / displacement of the unit-voxel cantilever."""
+    domain = cantilever_domain(shape)
+    system = topt.HexElasticity(domain, linear_solver="cpu_superlu")
+    rho = np.random.default_rng(seed).uniform(0.01, 1.0, system.nelem)
+    result = system.solve(rho, 3.0, 1e-9, metrics=True)["tip"]
+    part = system.groups[next(iter(system.groups))][0][1]
+    fields = result.get("fields")
+    out = {"shape": np.asarray(shape), "seed": seed, "density": rho, "compliance": result["compliance_n_mm"],
+           "derivative": result["derivative"], "relative_residual": result["relative_residual"],
+           "max_displacement": result["max_displacement_mm"], "fixed": part["fixed"], "force": part["force"]}
+    if fields is None:
+        system2 = topt.HexElasticity(domain, linear_solver="cpu_superlu")
+        moduli = 1e-9 + (1 - 1e-9) * rho ** 3
+        matrix = system2.matrix(moduli).tocsc()
+        free = part["free"]
+        from scipy.sparse.linalg import splu
+        u = np.zeros(system2.ndof)
+        u[free] = splu(matrix[free][:, free].tocsc(), permc_spec="MMD_AT_PLUS_A", options={"SymmetricMode": True}).solve(part["force"][free])
+        fields = {1.0: u}
+    if int(np.prod(shape)) <= 4096:
+        out["displacement"] = next(iter(fields.values()))
+    np.savez_compressed(OUT / f"{name}.npz", **out)
+
+
+def density_filter(topt):
+    """Reference sparse cone filter: sums, filtered field and pullback (topology_optimization.py:1094-1178)."""
+    from tests.test_topology_optimization import beam_domain
+    out = {}
+    cases = {"beam": ((14, 11, 9), (0.747, 0.753, 0.667), 2.84, 4.0, 0.2), "unit": ((12, 10, 6), (1.0, 1.0, 1.0), 1.5, 0.0, 0.0)}
+    for name, (shape, spacing, radius, beta, forbid) in cases.items():
+        domain = beam_domain(shape, spacing)
+        allowed = np.random.default_rng(3).uniform(size=shape) >= forbid
+        allowed[0] = allowed[-1] = True
+        preserve = np.zeros(shape, dtype=bool)
+        preserve[0] = True
+        domain.update(allowed=allowed, forbidden=~allowed, preserve=preserve & allowed)
+        mapping = topt.DensityMap(domain, topt._settings({"filter_radius_mm": radius, "projection_beta": beta, "density_filter": "sparse"}))
+        rng = np.random.default_rng(5)
+        design, sensitivity = rng.uniform(size=allowed.size), rng.normal(size=allowed.size)
+        physical, projection = mapping.physical(design)
+        out.update({f"{name}_shape": np.asarray(shape), f"{name}_spacing": np.asarray(spacing), f"{name}_radius": radius,
+                    f"{name}_beta": beta, f"{name}_allowed": allowed.ravel(), f"{name}_preserve": (preserve & allowed).ravel(),
+                    f"{name}_design": design, f"{name}_sensitivity": sensitivity, f"{name}_sums": mapping.sums,
+                    f"{name}_filtered": mapping.filtered(design), f"{name}_physical": physical, f"{name}_projection": projection,
+                    f"{name}_pullback": mapping.pullback(sensitivity, projection)})
+    np.savez_compressed(OUT / "filter.npz", **out)
+
+
+def covariance(topt, tprob):
+    """Reference InterfaceCovariance on the covariance cantilever half model: tr, lambda_max and their gradients."""
+    shape = (16, 3, 6)
+    domain, problem = tprob.covariance_cantilever(shape, limits={"mean_n_mm": 1.0, "worst_n_mm": 1.0})
+    problem["covariance"]["ks"] = 50.0
+    tp = tprob.TopologyProblem(domain, problem)
+    density = np.random.default_rng(3).uniform(0.3, 1.0, int(np.prod(shape)))
+    rows = {row["name"]: row for part in tp.physics(density)[:2] for row in part}
+    cov = tp.covariance
+    system = tp.system
+    # the per-case force pairs and the registered parts (sign, fixed) the reference solves
+    forces = {f"force_{k}_{'p' if sign > 0 else 'm'}": v for k, f in enumerate(cov.forces) for sign, v in f.items()}
+    parts = {}
+    for key, members in system.groups.items():
+        sign = members[0][1]["sign"]
+        parts[f"fixed_{'p' if sign > 0 else 'm'}"] = members[0][1]["fixed"]
+    out = {"shape": np.asarray(shape), "density": density, "sigma": np.asarray(cov.sigma), "directions": cov.directions,
+           "factor": cov.factor, "rank": cov.rank, "load_mean": rows["load_mean"]["value"], "load_worst": rows["load_worst"]["value"],
+           "ks": rows["load_worst"]["info"]["ks_n_mm"], "grad_mean": rows["load_mean"]["gradient"],
+           "grad_worst": rows["load_worst"]["gradient"], "ke": system.ke, "penalization": 3.0, "min_stiffness_ratio": 1e-6,
+           "young": system.young, **forces, **parts}
+    np.savez_compressed(OUT / "covariance.npz", **out)
+    tp.close()
+
+
+def main(source):
+    topt, tmg, tprob = load_reference(source)
+    hex8(topt)
+    operator(topt, tmg, tprob)
+    direct(topt, (16, 8, 8), 0, "cantilever_small")
+    density_filter(topt)
+    covariance(topt, tprob)
+    if "--skip-config1" not in sys.argv:
+        direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--") else "/root/reference")
