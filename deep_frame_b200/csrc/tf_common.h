@@ -69,6 +69,11 @@ struct DevBuf {
     TF_CUDA_CHECK(cudaMalloc(&p, b));
     bytes = b;
   }
+  // keep the current allocation when it already has exactly `b` bytes
+  void ensure(size_t b) {
+    if (p && bytes == b) return;
+    alloc(b);
+  }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;

@@ -99,7 +99,9 @@ __device__ __forceinline__ void fine_node(const K0Param<T>& K, const Geo& g, con
 // ---------------------------------------------------------------------------
 // Coarse-level (Galerkin block) operator at one node for CB columns at once:
 // out[c] = sum_e B_e[c_n(e) rows, :] (mask*u_c)_e.  Each block value loaded is
-// reused for CB columns.
+// reused for CB columns.  Blocks are stored entry-major ([576][nelem]), so the
+// threads of a warp (consecutive nodes along z) read consecutive elements and
+// every block load is one coalesced transaction.
 // ---------------------------------------------------------------------------
 template <typename T, int CB>
 __device__ __forceinline__ void block_node(const Geo& g, const T* __restrict__ B, const uint8_t* __restrict__ mask,
@@ -113,7 +115,7 @@ __device__ __forceinline__ void block_node(const Geo& g, const T* __restrict__ B
   for (int e = 0; e < 8; ++e) {
     const int ei = i - 1 + (e >> 2), ej = j - 1 + ((e >> 1) & 1), ek = k - 1 + (e & 1);
     evalid[e] = (unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez;
-    ebase[e] = evalid[e] ? (((long long)ei * g.ey + ej) * g.ez + ek) * 576 : 0;
+    ebase[e] = evalid[e] ? (((long long)ei * g.ey + ej) * g.ez + ek) : 0;
   }
 #pragma unroll
   for (int di = -1; di <= 1; ++di) {
@@ -138,13 +140,14 @@ __device__ __forceinline__ void block_node(const Geo& g, const T* __restrict__ B
           if (!evalid[e]) continue;
           const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
           const int cm = corner_id(cx, cy, cz);
-          const T* bp = B + ebase[e] + (3 * cn) * 24 + 3 * cm;
+          const long long est = (long long)g.ex * g.ey * g.ez;
+          const T* bp = B + ebase[e] + (long long)((3 * cn) * 24 + 3 * cm) * est;
           T b[9];
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            b[3 * a + 0] = bp[a * 24 + 0];
-            b[3 * a + 1] = bp[a * 24 + 1];
-            b[3 * a + 2] = bp[a * 24 + 2];
+            b[3 * a + 0] = bp[(a * 24 + 0) * est];
+            b[3 * a + 1] = bp[(a * 24 + 1) * est];
+            b[3 * a + 2] = bp[(a * 24 + 2) * est];
           }
 #pragma unroll
           for (int c = 0; c < CB; ++c) {
@@ -169,7 +172,7 @@ enum ApplyMode : int {
 template <typename T>
 struct LevelArgs {
   Geo g;
-  const T* E;            // fine: element moduli [ex][ey][ez]; coarse: blocks [nelem][24][24]
+  const T* E;            // fine: element moduli [ex][ey][ez]; coarse: blocks entry-major [576][nelem]
   const uint8_t* mask;   // per-node 3-bit live mask
   const T* inv;          // inverse diagonal [ndof] (Jacobi / Chebyshev)
   const T* u;            // operator input, [R][ndof]

@@ -283,6 +283,25 @@ __global__ void __launch_bounds__(128) galerkin_kernel(const __grid_constant__ G
   }
 }
 
+// [nelem][576] FP64 blocks -> entry-major [576][nelem] copy in T (tiled through shared memory).
+template <typename T>
+__global__ void blocks_soa_kernel(const double* __restrict__ aos, T* __restrict__ soa, long long nelem) {
+  __shared__ double tile[32][65];
+  const long long e0 = (long long)blockIdx.x * 32;
+  const int r0 = blockIdx.y * 64;
+  for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+    const int el = t / 64, r = t % 64;
+    const long long e = e0 + el;
+    tile[el][r] = (e < nelem && r0 + r < 576) ? aos[e * 576 + r0 + r] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+    const int r = t / 32, el = t % 32;
+    const long long e = e0 + el;
+    if (e < nelem && r0 + r < 576) soa[(long long)(r0 + r) * nelem + e] = static_cast<T>(tile[el][r]);
+  }
+}
+
 template <typename T>
 __global__ void cast_kernel(const double* __restrict__ src, T* __restrict__ dst, long long n) {
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)

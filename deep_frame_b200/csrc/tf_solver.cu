@@ -37,8 +37,9 @@ struct Level {
   Geo g{};
   long long ndof = 0, nelem = 0;
   DevBuf mask;      // uint8 [nnode]
-  DevBuf blocks64;  // Galerkin blocks [nelem][576] (levels >= 1)
-  DevBuf blocksw;   // FP32 copy of the blocks (FP32 work precision only)
+  DevBuf blocks64;  // Galerkin blocks [nelem][576] (levels >= 1), used by the set-up
+  DevBuf blocks64s; // entry-major FP64 copy [576][nelem] for the operator
+  DevBuf blocksw;   // entry-major FP32 copy (FP32 work precision only)
   DevBuf inv64;     // inverse diagonal [ndof]
   DevBuf invw;      // FP32 copy (FP32 work precision only)
   double lambda_max = 1.0;
@@ -49,8 +50,10 @@ struct Hierarchy {
   int n_live = 0;
   DevBuf live;      // int64 [n_live]: live dofs of the coarsest level
   DevBuf X;         // FP64 [n_live][n_live] inverse Cholesky factor
+  DevBuf A, live_of, bits;  // set-up scratch kept for the next rebuild
   double setup_s = 0.0;
   bool setup_reported = false;
+  bool valid = false;
 };
 
 template <typename T>
@@ -158,6 +161,7 @@ struct tf_handle {
   size_t ccap = 0;
   VBufs<float> wf;
   VBufs<double> wd;
+  DevBuf tmp_diag;
   Timers timers;
   std::string err;
   ~tf_handle() {
@@ -259,7 +263,7 @@ template <typename T>
 const T* level_E(tf_handle* h, Hierarchy& hy, int l, bool precise) {
   const bool dbl = std::is_same<T, double>::value;
   if (l == 0) return static_cast<const T*>(dbl ? h->moduli64.p : h->modulif.p);
-  return static_cast<const T*>(dbl ? hy.lv[l].blocks64.p : hy.lv[l].blocksw.p);
+  return static_cast<const T*>(dbl ? hy.lv[l].blocks64s.p : hy.lv[l].blocksw.p);
 }
 template <typename T>
 const T* level_inv(Hierarchy& hy, int l) {
@@ -451,8 +455,10 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
   if (range) cudaEventRecord(range->first, st);
   const bool dbl = work_is_double(h);
   ensure_scratch(h, 1);
-  hy.lv.clear();
-  hy.lv.resize(h->nlev);
+  if ((int)hy.lv.size() != h->nlev) {
+    hy.lv.clear();
+    hy.lv.resize(h->nlev);
+  }
   const std::vector<int64_t>& fixed = h->bcs.at(key);
   // level 0
   Level& f = hy.lv[0];
@@ -471,21 +477,22 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
       const long long pn = (i * f.g.ny + j) * f.g.nz + k;
       bits[pn] |= static_cast<uint8_t>(1u << comp);
     }
-    DevBuf dbits(bits.size());
+    DevBuf& dbits = hy.bits;
+    dbits.ensure(bits.size());
     TF_CUDA_CHECK(cudaMemcpyAsync(dbits.p, bits.data(), bits.size(), cudaMemcpyHostToDevice, st));
-    f.mask.alloc(f.g.nnode);
+    f.mask.ensure(f.g.nnode);
     fine_mask_kernel<<<grid_for(f.g.nnode, 256), 256, 0, st>>>(f.g, h->moduli64.as<double>(), dbits.as<uint8_t>(), f.mask.as<uint8_t>());
     TF_LAUNCH_CHECK("fine_mask_kernel");
-    DevBuf diag(sizeof(double) * f.ndof);
+    DevBuf& diag = h->tmp_diag;
+    diag.ensure(sizeof(double) * f.ndof);
     fine_diag_kernel<<<grid_for(f.g.nnode, 256), 256, 0, st>>>(f.g, h->moduli64.as<double>(), f.mask.as<uint8_t>(),
                                                                h->k0diag.as<double>(), diag.as<double>());
     TF_LAUNCH_CHECK("fine_diag_kernel");
-    f.inv64.alloc(sizeof(double) * f.ndof);
-    if (!dbl) f.invw.alloc(sizeof(float) * f.ndof);
+    f.inv64.ensure(sizeof(double) * f.ndof);
+    if (!dbl) f.invw.ensure(sizeof(float) * f.ndof);
     fine_inv_kernel<float><<<grid_for(f.g.nnode, 256), 256, 0, st>>>(f.g.nnode, diag.as<double>(), f.mask.as<uint8_t>(),
                                                                      f.inv64.as<double>(), dbl ? nullptr : f.invw.as<float>());
     TF_LAUNCH_CHECK("fine_inv_kernel");
-    TF_CUDA_CHECK(cudaStreamSynchronize(st));  // dbits / diag go out of scope
   }
   for (int l = 1; l < h->nlev; ++l) {
     Level& c = hy.lv[l];
@@ -493,32 +500,35 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     c.g = h->geo[l];
     c.ndof = 3 * c.g.nnode;
     c.nelem = (long long)c.g.ex * c.g.ey * c.g.ez;
-    c.blocks64.alloc(sizeof(double) * 576 * c.nelem);
+    c.blocks64.ensure(sizeof(double) * 576 * c.nelem);
     galerkin_kernel<<<grid_for(c.nelem, 1, 148 * 16), 128, 0, st>>>(h->W, c.g, p.g, l == 1 ? 1 : 0, h->moduli64.as<double>(),
                                                                      hy.lv[0].mask.as<uint8_t>(), h->K0dev.as<double>(),
                                                                      h->Q.as<double>(), l == 1 ? nullptr : p.blocks64.as<double>(),
                                                                      c.blocks64.as<double>());
     TF_LAUNCH_CHECK("galerkin_kernel");
-    DevBuf diag(sizeof(double) * c.ndof);
+    DevBuf& diag = h->tmp_diag;
     block_diag_kernel<<<grid_for(c.g.nnode, 256), 256, 0, st>>>(c.g, c.blocks64.as<double>(), diag.as<double>());
     TF_LAUNCH_CHECK("block_diag_kernel");
     double* dmax = h->scal.as<double>() + 1;
     amax_kernel<<<grid_for(c.ndof, 256, PCG_BLOCKS), 256, 0, st>>>(diag.as<double>(), c.ndof, h->partial.as<double>(),
                                                                    h->count.as<unsigned>(), dmax);
     TF_LAUNCH_CHECK("amax_kernel");
-    c.mask.alloc(c.g.nnode);
-    c.inv64.alloc(sizeof(double) * c.ndof);
-    if (!dbl) c.invw.alloc(sizeof(float) * c.ndof);
+    c.mask.ensure(c.g.nnode);
+    c.inv64.ensure(sizeof(double) * c.ndof);
+    if (!dbl) c.invw.ensure(sizeof(float) * c.ndof);
     coarse_mask_inv_kernel<float><<<grid_for(c.g.nnode, 256), 256, 0, st>>>(c.g.nnode, diag.as<double>(), dmax, h->s.dead_ratio,
                                                                             c.mask.as<uint8_t>(), c.inv64.as<double>(),
                                                                             dbl ? nullptr : c.invw.as<float>());
     TF_LAUNCH_CHECK("coarse_mask_inv_kernel");
+    const dim3 tgrid((unsigned)((c.nelem + 31) / 32), 9);
+    c.blocks64s.ensure(sizeof(double) * 576 * c.nelem);
+    blocks_soa_kernel<double><<<tgrid, 256, 0, st>>>(c.blocks64.as<double>(), c.blocks64s.as<double>(), c.nelem);
+    TF_LAUNCH_CHECK("blocks_soa_kernel");
     if (!dbl) {
-      c.blocksw.alloc(sizeof(float) * 576 * c.nelem);
-      cast_kernel<float><<<grid_for(576 * c.nelem, 256), 256, 0, st>>>(c.blocks64.as<double>(), c.blocksw.as<float>(), 576 * c.nelem);
-      TF_LAUNCH_CHECK("cast_kernel");
+      c.blocksw.ensure(sizeof(float) * 576 * c.nelem);
+      blocks_soa_kernel<float><<<tgrid, 256, 0, st>>>(c.blocks64.as<double>(), c.blocksw.as<float>(), c.nelem);
+      TF_LAUNCH_CHECK("blocks_soa_kernel");
     }
-    TF_CUDA_CHECK(cudaStreamSynchronize(st));
   }
   // lambda_max(D^-1 A) of every smoothed level, in the work precision
   if (dbl) ensure_vbufs<double>(h, 1); else ensure_vbufs<float>(h, 1);
@@ -543,11 +553,13 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
                                 std::to_string(DENSE_LIMIT) + " (raise max_levels or lower coarsest_dofs)");
   hy.n_live = static_cast<int>(nl);
   if (nl > 0) {
-    hy.live.alloc(sizeof(long long) * nl);
+    hy.live.ensure(sizeof(long long) * nl);
     TF_CUDA_CHECK(cudaMemcpyAsync(hy.live.p, live.data(), sizeof(long long) * nl, cudaMemcpyHostToDevice, st));
-    DevBuf dlive_of(sizeof(int) * cl.ndof);
+    DevBuf& dlive_of = hy.live_of;
+    dlive_of.ensure(sizeof(int) * cl.ndof);
     TF_CUDA_CHECK(cudaMemcpyAsync(dlive_of.p, live_of.data(), sizeof(int) * cl.ndof, cudaMemcpyHostToDevice, st));
-    DevBuf A(sizeof(double) * nl * nl);
+    DevBuf& A = hy.A;
+    A.ensure(sizeof(double) * nl * nl);
     TF_CUDA_CHECK(cudaMemsetAsync(A.p, 0, A.bytes, st));
     coarsest_assemble_kernel<<<grid_for(nl, 128), 128, 0, st>>>(cl.g, cl.blocks64.as<double>(), dlive_of.as<int>(),
                                                                 hy.live.as<long long>(), static_cast<int>(nl), A.as<double>());
@@ -562,7 +574,7 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     if (hinfo != 0)
       throw Error(TF_NUMERIC, "coarsest Galerkin matrix is not positive definite (pivot " + std::to_string(hinfo) +
                                   "); the supports do not remove every rigid-body mode");
-    hy.X.alloc(sizeof(double) * nl * nl);
+    hy.X.ensure(sizeof(double) * nl * nl);
     dense_trinv(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), st);
     TF_CUDA_CHECK(cudaStreamSynchronize(st));
   }
@@ -574,15 +586,15 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
 Hierarchy& get_hierarchy(tf_handle* h, uint64_t key, cudaStream_t st) {
   require(h->have_moduli, "update(moduli) must be called before solving");
   require(h->bcs.count(key) > 0, "no boundary conditions registered for this key (tf_set_bc)");
-  auto it = h->hier.find(key);
-  if (it != h->hier.end()) return it->second;
   Hierarchy& hy = h->hier[key];
+  if (hy.valid) return hy;
   try {
     build_hierarchy(h, key, hy, st);
   } catch (...) {
     h->hier.erase(key);
     throw;
   }
+  hy.valid = true;
   return hy;
 }
 
@@ -930,7 +942,7 @@ extern "C" int tf_update(tf_handle* h, const double* moduli_dev, void* stream) {
     pad_moduli_kernel<<<grid_for((long long)pd.ex * pd.ey * pd.ez, 256), 256, 0, s>>>(
         h->un, pd, h->moduli_un.as<double>(), h->moduli64.as<double>(), work_is_double(h) ? nullptr : h->modulif.as<float>());
     TF_LAUNCH_CHECK("pad_moduli_kernel");
-    h->hier.clear();
+    for (auto& kv : h->hier) kv.second.valid = false;   // rebuilt lazily, reusing their buffers
     h->have_moduli = true;
   });
 }
@@ -943,7 +955,10 @@ extern "C" int tf_set_bc(tf_handle* h, uint64_t key, const int64_t* fixed, int64
     std::vector<int64_t> v(fixed, fixed + count);
     for (int64_t d : v) require(d >= 0 && d < nd, "fixed dof index out of range");
     auto it = h->bcs.find(key);
-    if (it != h->bcs.end() && it->second != v) h->hier.erase(key);
+    if (it != h->bcs.end() && it->second != v) {
+      auto hit = h->hier.find(key);
+      if (hit != h->hier.end()) hit->second.valid = false;
+    }
     h->bcs[key] = std::move(v);
   });
 }
