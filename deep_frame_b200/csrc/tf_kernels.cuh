@@ -211,42 +211,211 @@ __device__ __forceinline__ void epilogue(const LevelArgs<T>& a, int mode, long l
   }
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory tiled level operators.  A CTA owns a tile of TX x TY x tz
+// output nodes (tz <= TZMAX chosen per grid so that the z extent is covered
+// with little waste) and stages the tile's input nodes with a one-node halo,
+// already masked and zero-padded outside the grid, in a fixed-pitch shared
+// array: every neighbour offset of the 27-point stencil is then a
+// compile-time immediate and the inner loop has no bounds or mask tests.
+// The element moduli (finest level) are staged the same way, with zeros for
+// elements outside the grid.
+// ---------------------------------------------------------------------------
+constexpr int TX = 4, TY = 8, TZMAX = 9;
+constexpr int HX = TX + 2, HY = TY + 2, HZ = TZMAX + 2;   // halo tile pitch (nodes)
+constexpr int EX = TX + 1, EY = TY + 1, EZ = TZMAX + 1;   // element tile pitch
+constexpr int HALO = HX * HY * HZ;
+
+struct TileMap {
+  int tiles_x, tiles_y, tiles_z, tz;
+};
+
+__host__ inline TileMap tile_map(const Geo& g) {
+  TileMap m;
+  const int nzt = (g.nz + TZMAX - 1) / TZMAX;
+  m.tz = (g.nz + nzt - 1) / nzt;
+  m.tiles_x = (g.nx + TX - 1) / TX;
+  m.tiles_y = (g.ny + TY - 1) / TY;
+  m.tiles_z = (g.nz + m.tz - 1) / m.tz;
+  return m;
+}
+
+// Stage the masked input tile of one column (3 values per node) into s[HALO][3].
 template <typename T>
-__global__ void __launch_bounds__(256) fine_level_kernel(const __grid_constant__ K0Param<T> K, const LevelArgs<T> a, int mode) {
-  const int col = blockIdx.y;
-  if (a.gate && !*a.gate) return;
-  if (a.active && !a.active[col]) return;
-  const long long off = (long long)col * a.colstride;
-  const T* u = a.u + off;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < a.g.nnode; n += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    node_coords(n, a.g, i, j, k);
-    T av[3];
-    fine_node<T>(K, a.g, a.E, a.mask, u, i, j, k, av);
-    const unsigned m = a.mask ? a.mask[n] : 7u;
-    epilogue(a, mode, off, n, m, av);
+__device__ __forceinline__ void stage_tile(T* __restrict__ s, const Geo& g, const T* __restrict__ u, const uint8_t* __restrict__ mask,
+                                           int x0, int y0, int z0, int tz) {
+  const int hz = tz + 2;
+  const int count = HX * HY * hz;
+  for (int t = threadIdx.x; t < count; t += blockDim.x) {
+    const int cz = t % hz, r = t / hz, cy = r % HY, cx = r / HY;
+    const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
+    T v0 = T(0), v1 = T(0), v2 = T(0);
+    if ((unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz)
+      load_masked(u, mask, ((long long)gx * g.ny + gy) * g.nz + gz, v0, v1, v2);
+    T* d = s + 3 * ((cx * HY + cy) * HZ + cz);
+    d[0] = v0; d[1] = v1; d[2] = v2;
   }
 }
 
+// Finest level: out = sum_e E_e K0[c_n(e), :] u_e from the staged tiles.
+template <typename T>
+__device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __restrict__ su, const T* __restrict__ sE,
+                                               int lx, int ly, int lz, T out[3]) {
+  T acc[8][3];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) { acc[e][0] = T(0); acc[e][1] = T(0); acc[e][2] = T(0); }
+  const T* base = su + 3 * (((lx + 1) * HY + (ly + 1)) * HZ + (lz + 1));
+#pragma unroll
+  for (int di = -1; di <= 1; ++di) {
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+#pragma unroll
+      for (int dk = -1; dk <= 1; ++dk) {
+        const T* p = base + 3 * ((di * HY + dj) * HZ + dk);
+        const T u0 = p[0], u1 = p[1], u2 = p[2];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+          const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
+          if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
+          const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+          const int cm = corner_id(cx, cy, cz);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const int row = (3 * cn + a) * 24 + 3 * cm;
+            acc[e][a] += K.k[row] * u0 + K.k[row + 1] * u1 + K.k[row + 2] * u2;
+          }
+        }
+      }
+    }
+  }
+  const T* eb = sE + (lx * EY + ly) * EZ + lz;
+  out[0] = out[1] = out[2] = T(0);
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const T w = eb[((e >> 2) * EY + ((e >> 1) & 1)) * EZ + (e & 1)];
+    out[0] += w * acc[e][0];
+    out[1] += w * acc[e][1];
+    out[2] += w * acc[e][2];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY * TZMAX) fine_level_kernel(const __grid_constant__ K0Param<T> K, const LevelArgs<T> a,
+                                                                    int mode, TileMap tm) {
+  __shared__ T su[HALO * 3];
+  __shared__ T sE[EX * EY * EZ];
+  const int col = blockIdx.y;
+  if (a.gate && !*a.gate) return;
+  if (a.active && !a.active[col]) return;
+  const Geo& g = a.g;
+  const int b = blockIdx.x;
+  const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
+  const int tz = tm.tz;
+  const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
+  const long long off = (long long)col * a.colstride;
+  stage_tile(su, g, a.u + off, a.mask, x0, y0, z0, tz);
+  const int ez = tz + 1;
+  for (int t = threadIdx.x; t < EX * EY * ez; t += blockDim.x) {
+    const int cz = t % ez, rr = t / ez, cy = rr % EY, cx = rr / EY;
+    const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
+    T v = T(0);
+    if ((unsigned)gx < (unsigned)g.ex && (unsigned)gy < (unsigned)g.ey && (unsigned)gz < (unsigned)g.ez)
+      v = a.E[((long long)gx * g.ey + gy) * g.ez + gz];
+    sE[(cx * EY + cy) * EZ + cz] = v;
+  }
+  __syncthreads();
+  const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
+  const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  T av[3];
+  fine_tile_node<T>(K, su, sE, lx, ly, lz, av);
+  const long long n = ((long long)i * g.ny + j) * g.nz + k;
+  const unsigned m = a.mask ? a.mask[n] : 7u;
+  epilogue(a, mode, off, n, m, av);
+}
+
+// Galerkin levels: CB columns per CTA share every block value loaded.
 template <typename T, int CB>
-__global__ void __launch_bounds__(128) block_level_kernel(const LevelArgs<T> a, int mode) {
+__global__ void __launch_bounds__(TX * TY * TZMAX) block_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);   // [CB][HALO][3]
   const int c0 = blockIdx.y * CB;
   if (a.gate && !*a.gate) return;
   const int nc = min(CB, a.ncol - c0);
   bool any = false;
   for (int c = 0; c < nc; ++c) any |= (!a.active || a.active[c0 + c]);
   if (!any) return;
+  const Geo& g = a.g;
+  const int b = blockIdx.x;
+  const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
+  const int tz = tm.tz;
+  const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
   const long long off = (long long)c0 * a.colstride;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < a.g.nnode; n += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    node_coords(n, a.g, i, j, k);
-    T av[CB][3];
-    block_node<T, CB>(a.g, a.E, a.mask, a.u + off, a.colstride, nc, i, j, k, av);
-    const unsigned m = a.mask ? a.mask[n] : 7u;
 #pragma unroll
-    for (int c = 0; c < CB; ++c) {
-      if (c < nc && (!a.active || a.active[c0 + c])) epilogue(a, mode, off + c * a.colstride, n, m, av[c]);
+  for (int c = 0; c < CB; ++c) {
+    if (c < nc) stage_tile(su + c * HALO * 3, g, a.u + off + c * a.colstride, a.mask, x0, y0, z0, tz);
+  }
+  __syncthreads();
+  const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
+  const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const long long est = (long long)g.ex * g.ey * g.ez;
+  long long ebase[8];
+  bool evalid[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int ei = i - 1 + (e >> 2), ej = j - 1 + ((e >> 1) & 1), ek = k - 1 + (e & 1);
+    evalid[e] = (unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez;
+    ebase[e] = evalid[e] ? (((long long)ei * g.ey + ej) * g.ez + ek) : 0;
+  }
+  T out[CB][3];
+#pragma unroll
+  for (int c = 0; c < CB; ++c) { out[c][0] = T(0); out[c][1] = T(0); out[c][2] = T(0); }
+  const int cbase = 3 * (((lx + 1) * HY + (ly + 1)) * HZ + (lz + 1));
+#pragma unroll
+  for (int di = -1; di <= 1; ++di) {
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+#pragma unroll
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int noff = cbase + 3 * ((di * HY + dj) * HZ + dk);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+          const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
+          if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
+          const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+          const int cm = corner_id(cx, cy, cz);
+          T bv[9];
+          if (evalid[e]) {
+            const T* bp = a.E + ebase[e] + (long long)((3 * cn) * 24 + 3 * cm) * est;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              bv[3 * q + 0] = bp[(q * 24 + 0) * est];
+              bv[3 * q + 1] = bp[(q * 24 + 1) * est];
+              bv[3 * q + 2] = bp[(q * 24 + 2) * est];
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) bv[q] = T(0);
+          }
+#pragma unroll
+          for (int c = 0; c < CB; ++c) {
+            const T* p = su + c * HALO * 3 + noff;
+            const T u0 = p[0], u1 = p[1], u2 = p[2];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) out[c][q] += bv[3 * q] * u0 + bv[3 * q + 1] * u1 + bv[3 * q + 2] * u2;
+          }
+        }
+      }
     }
+  }
+  const long long n = ((long long)i * g.ny + j) * g.nz + k;
+  const unsigned m = a.mask ? a.mask[n] : 7u;
+#pragma unroll
+  for (int c = 0; c < CB; ++c) {
+    if (c < nc && (!a.active || a.active[c0 + c])) epilogue(a, mode, off + c * a.colstride, n, m, out[c]);
   }
 }
 

@@ -30,7 +30,8 @@ namespace {
 
 thread_local std::string g_last_create_error;
 
-constexpr int CB = 4;                    // columns per thread in the Galerkin-level operator
+constexpr int CB32 = 4;                  // columns per CTA of the FP32 Galerkin-level operator
+constexpr int CB64 = 2;                  // columns per CTA of the FP64 Galerkin-level operator
 constexpr long long DENSE_LIMIT = 24000;  // largest dense coarsest factor (4.6 GB in FP64)
 
 struct Level {
@@ -277,13 +278,18 @@ template <> const K0Param<float>& k0param<float>(tf_handle* h) { return h->k32; 
 template <typename T>
 void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st, int timer = -1) {
   TimedRange tr(h->timers, timer >= 0 ? timer : (l == 0 ? TIMER_FINE_WORK : TIMER_COARSE), st);
+  const TileMap tm = tile_map(a.g);
+  const int threads = TX * TY * tm.tz;
+  const unsigned tiles = (unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z);
   if (l == 0) {
-    dim3 grid(grid_for(a.g.nnode, 256, 4096), a.ncol);
-    fine_level_kernel<T><<<grid, 256, 0, st>>>(k0param<T>(h), a, mode);
+    dim3 grid(tiles, a.ncol);
+    fine_level_kernel<T><<<grid, threads, 0, st>>>(k0param<T>(h), a, mode, tm);
     TF_LAUNCH_CHECK("fine_level_kernel");
   } else {
-    dim3 grid(grid_for(a.g.nnode, 128, 4096), (a.ncol + CB - 1) / CB);
-    block_level_kernel<T, CB><<<grid, 128, 0, st>>>(a, mode);
+    constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
+    dim3 grid(tiles, (a.ncol + cb - 1) / cb);
+    const size_t smem = sizeof(T) * 3 * HALO * cb;
+    block_level_kernel<T, cb><<<grid, threads, smem, st>>>(a, mode, tm);
     TF_LAUNCH_CHECK("block_level_kernel");
   }
 }

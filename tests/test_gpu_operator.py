@@ -21,7 +21,8 @@ def _moduli(shape, seed, dead=0.0):
 
 
 @pytest.mark.parametrize("shape,spacing,dead", [((8, 3, 5), (1.0, 1.0, 1.0), 0.0), ((4, 8, 4), (1.0, 1.0, 1.0), 0.0),
-                                                 ((7, 6, 5), (0.747, 0.753, 0.667), 0.2), ((12, 10, 17), (1.0, 1.0, 1.0), 0.1)])
+                                                 ((7, 6, 5), (0.747, 0.753, 0.667), 0.2), ((12, 10, 17), (1.0, 1.0, 1.0), 0.1),
+                                                 ((9, 7, 1), (1.0, 1.0, 1.0), 0.0), ((5, 3, 30), (1.0, 2.0, 0.5), 0.05)])
 def test_operator_matches_assembled_matrix(cuda, shape, spacing, dead):
     from deep_frame_b200.topology_multigrid import GeometricMultigrid
     k0, _, _ = hex8.element_matrices(spacing, 0.3)
