@@ -17,7 +17,7 @@ COARSE = {"galerkin": 0, "rediscretize": 1}
 
 # every symbol include/tf_b200.h declares (checked by the CPU test suite)
 SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set_bc", "tf_prepare", "tf_precondition",
-           "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_timers", "tf_launch_count",
+           "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
 
@@ -79,6 +79,7 @@ def load():
             "tf_element_energy": [P, P, I32, P, I32, P, P, P, I32, I32, P],
             "tf_gram": [P, I32, P, I32, I64, P, P, P],
             "tf_gram_scratch_size": [I32, I32],
+            "tf_gram_static": [P, I32, P, I32, I64, P, P],
             "tf_timers": [P, I32, ctypes.POINTER(D), ctypes.POINTER(I64), I32],
             "tf_launch_count": [],
             "tf_destroy": [P],

@@ -8,6 +8,8 @@
 #include "tf_b200.h"
 #include "tf_common.h"
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 using namespace tfb;
 
@@ -87,4 +89,75 @@ extern "C" int64_t tf_launch_count(void) { return g_launch_count.load(); }
 
 extern "C" int64_t tf_gram_scratch_size(int32_t ra, int32_t rb) {
   return (int64_t)GRAM_BLOCKS * ra * rb;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of tf_gram.
+//
+// Some callers cannot allocate device memory at the moment they need F: a
+// host application that hands this library a fixed device-memory budget and
+// owns every allocation itself, or an optimiser loop that runs inside such a
+// host's callbacks, where neither cudaMalloc nor a caching allocator may be
+// touched.  tf_gram_static takes no scratch argument: its per-CTA partials live
+// in the file-scope array below, sized for at most TF_GRAM_STATIC_MAX_PAIRS
+// (ra * rb) pairs.  The array is part of the library image, so every GPU that
+// loads the library holds it (4.85 MB) until the process exits.
+//
+// Host code cannot pass the array's name to a kernel: on the host it is only a
+// stand-in symbol, not a device address.  The first call on each device looks
+// up the device address with cudaGetSymbolAddress (with that device current)
+// and caches it; make that first call before any stream capture.  All calls
+// share the one array, which keeps the last call's partials: the partial
+// kernel writes every slot the reduction then reads, so nothing needs clearing,
+// but calls that overlap on the GPU (different streams, no ordering) race on
+// the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int TF_GRAM_STATIC_MAX_PAIRS = 2048;   // e.g. 42 x 42 = 1764 fits
+constexpr int TF_GRAM_STATIC_MAX_DEVICES = 64;
+static __device__ __align__(256) double g_gram_static_scratch[GRAM_BLOCKS * TF_GRAM_STATIC_MAX_PAIRS];
+std::mutex g_gram_static_mutex;
+double* g_gram_static_ptr[TF_GRAM_STATIC_MAX_DEVICES] = {};
+}  // namespace
+
+extern "C" int tf_gram_static(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
+                              void* stream) {
+  if (ra < 1 || rb < 1 || ra > GRAM_MAX || rb > GRAM_MAX || n < 1 || !a_dev || !b_dev || !out_dev) {
+    record_unhandled_error("tf_gram_static: need 1 <= ra, rb <= 64, n >= 1 and non-NULL pointers");
+    return TF_INVALID;
+  }
+  if ((long long)ra * rb > TF_GRAM_STATIC_MAX_PAIRS) {
+    record_unhandled_error("tf_gram_static: ra * rb = " + std::to_string((long long)ra * rb) +
+                           " exceeds the static scratch limit of " + std::to_string(TF_GRAM_STATIC_MAX_PAIRS) +
+                           " pairs; use tf_gram with a caller-provided scratch buffer");
+    return TF_INVALID;
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= TF_GRAM_STATIC_MAX_DEVICES) {
+    record_unhandled_error("tf_gram_static: no usable current CUDA device");
+    return TF_CUDA;
+  }
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_gram_static_mutex);
+    if (!g_gram_static_ptr[device]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_gram_static_scratch);
+      if (e != cudaSuccess || !p) {
+        record_unhandled_error(std::string("tf_gram_static: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+        return TF_CUDA;
+      }
+      g_gram_static_ptr[device] = static_cast<double*>(p);
+    }
+    scratch = g_gram_static_ptr[device];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int blocks = static_cast<int>(std::min<long long>(GRAM_BLOCKS, (n + KC - 1) / KC));
+  gram_partial_kernel<<<blocks, 256, 0, s>>>(a_dev, ra, b_dev, rb, n, scratch);
+  g_launch_count.fetch_add(1, std::memory_order_relaxed);
+  if (cudaGetLastError() != cudaSuccess) return TF_CUDA;
+  gram_reduce_kernel<<<(ra * rb + 255) / 256, 256, 0, s>>>(scratch, ra * rb, blocks, out_dev);
+  g_launch_count.fetch_add(1, std::memory_order_relaxed);
+  if (cudaGetLastError() != cudaSuccess) return TF_CUDA;
+  return TF_OK;
 }

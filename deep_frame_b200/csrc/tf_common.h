@@ -38,6 +38,9 @@ extern std::atomic<long long> g_launch_count;
     ::tfb::cuda_check(cudaGetLastError(), name);        \
   } while (0)
 
+// Store the message tf_last_error(NULL) returns (entry points without a handle).
+void record_unhandled_error(const std::string& message);
+
 inline void require(bool ok, const std::string& m) {
   if (!ok) throw Error(TF_INVALID, m);
 }

@@ -801,6 +801,11 @@ void validate_settings(const tf_settings& s) {
 
 // =============================================================== C ABI ======
 
+namespace tfb {
+// Message for tf_last_error(NULL) from entry points that take no handle.
+void record_unhandled_error(const std::string& message) { g_last_create_error = message; }
+}  // namespace tfb
+
 extern "C" int tf_default_settings(tf_settings* s) {
   if (!s) return TF_INVALID;
   *s = tf_settings{};

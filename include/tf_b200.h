@@ -153,6 +153,18 @@ TF_API int tf_gram(const double* a_dev, int32_t ra, const double* b_dev, int32_t
                    double* scratch_dev, void* stream);
 TF_API int64_t tf_gram_scratch_size(int32_t ra, int32_t rb);
 
+/* tf_gram without the scratch argument, for callers that cannot allocate device memory
+ * when they need F (a host application that owns every device allocation through a
+ * fixed budget, or code running inside its callbacks).  No counterpart in the reference.
+ * The partials live in a static 4.85 MB device array inside the library (held by every
+ * GPU that loads it), which limits ra * rb to 2048 pairs; larger requests return
+ * TF_STATUS_INVALID with a message in tf_last_error(NULL).  The first call on a device
+ * resolves the array's device address and should come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be ordered by the
+ * caller.  Allocates nothing. */
+TF_API int tf_gram_static(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
+                          void* stream);
+
 /* CUDA-event timing of the kernel classes this handle launches, recorded on the launching
  * stream: 0 FP64 finest operator of the PCG, 1 finest-level smoothing / residual in the work
  * precision, 2 Galerkin-level operators, 3 restriction + prolongation, 4 PCG vector kernels,
@@ -169,7 +181,8 @@ TF_API int64_t tf_launch_count(void);
  * topology_multigrid.py:543-548).  Idempotent for NULL. */
 TF_API int tf_destroy(tf_handle* h);
 
-/* Message of the last failed call on `h` (or of the last failed tf_create when h is NULL). */
+/* Message of the last failed call on `h` (or, with h NULL, of the last failed tf_create or
+ * tf_gram_static on this thread). */
 TF_API const char* tf_last_error(const tf_handle* h);
 
 #ifdef __cplusplus
