@@ -19,6 +19,8 @@ COARSE = {"galerkin": 0, "rediscretize": 1}
 SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set_bc", "tf_prepare", "tf_precondition",
            "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
+SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_destroy",
+            "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
 
 
@@ -43,6 +45,10 @@ class TfReport(ctypes.Structure):
                 ("retried_columns", ctypes.c_int32), ("zero_rhs_columns", ctypes.c_int32), ("levels", ctypes.c_int32),
                 ("steps", ctypes.c_int32), ("coarsest_dofs", ctypes.c_int64), ("seconds", ctypes.c_double),
                 ("setup_s", ctypes.c_double), ("lambda_max", ctypes.c_double * 16)]
+
+
+class TfMmaSettings(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_double) for name in ("move", "asyinit", "asydecr", "asyincr", "asymin", "asymax", "raa0", "albefa", "epsimin")]
 
 
 class TfError(RuntimeError):
@@ -84,11 +90,23 @@ def load():
             "tf_launch_count": [],
             "tf_destroy": [P],
             "tf_last_error": [P],
+            "tf_filter_create": [ctypes.POINTER(I64), ctypes.POINTER(D), D, P, P, ctypes.POINTER(P)],
+            "tf_filter_apply": [P, P, P, P, I32, P],
+            "tf_filter_sums": [P, P, P],
+            "tf_filter_project": [P, P, D, D, I32, P, P, P],
+            "tf_filter_destroy": [P],
+            "tf_filter_last_error": [P],
+            "tf_mma_create": [I32, I64, ctypes.POINTER(P)],
+            "tf_mma_step": [P, I32, P, P, P, P, P, P, P, P, P, P, D, P, P, P, ctypes.POINTER(TfMmaSettings), P, P, P, P,
+                            ctypes.POINTER(I32), P],
+            "tf_mma_destroy": [P],
+            "tf_mma_last_error": [P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
             fn.argtypes = args
-            fn.restype = {"tf_last_error": ctypes.c_char_p, "tf_gram_scratch_size": ctypes.c_int64, "tf_launch_count": ctypes.c_int64}.get(name, ctypes.c_int)
+            fn.restype = {"tf_last_error": ctypes.c_char_p, "tf_filter_last_error": ctypes.c_char_p, "tf_mma_last_error": ctypes.c_char_p,
+                          "tf_gram_scratch_size": ctypes.c_int64, "tf_launch_count": ctypes.c_int64}.get(name, ctypes.c_int)
         _lib = lib
         return lib
 

@@ -165,6 +165,52 @@ TF_API int64_t tf_gram_scratch_size(int32_t ra, int32_t rb);
 TF_API int tf_gram_static(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
                           void* stream);
 
+/* ------------------------------------------------------------------------------------
+ * Cone density filter (ConeFilter / cone_filter / DensityMap.filtered, .pullback,
+ * .project: deep_frame/topology_optimization.py:1082-1178).  Cells are C-ordered over
+ * shape; allowed / preserve are host byte masks (preserve may be NULL).  The filter
+ * radius may span at most 4 cells per axis.
+ * ------------------------------------------------------------------------------------ */
+typedef struct tf_filter tf_filter;
+TF_API int tf_filter_create(const int64_t shape[3], const double spacing[3], double radius, const uint8_t* allowed,
+                            const uint8_t* preserve, tf_filter** out);
+/* adjoint == 0: out = allowed * (W (allowed * in * in2)) / sums          (DensityMap.filtered)
+ * adjoint != 0: out = free * (W (allowed * in * in2 / sums))             (DensityMap.pullback)
+ * in2 is an optional per-cell multiplier (the projection derivative of the pullback). */
+TF_API int tf_filter_apply(tf_filter* f, const double* in_dev, const double* in2_dev, double* out_dev, int32_t adjoint, void* stream);
+/* Row sums W (allowed) on allowed cells, 1 on forbidden cells (DensityMap.sums). */
+TF_API int tf_filter_sums(const tf_filter* f, double* sums_dev, void* stream);
+/* Threshold projection with derivative; robust != 0 selects the eroded/dilated form. */
+TF_API int tf_filter_project(tf_filter* f, const double* filtered_dev, double beta, double eta, int32_t robust,
+                             double* physical_dev, double* derivative_dev, void* stream);
+TF_API int tf_filter_destroy(tf_filter* f);
+TF_API const char* tf_filter_last_error(const tf_filter* f);
+
+/* ------------------------------------------------------------------------------------
+ * Method of moving asymptotes (mmapy.mmasub as called from
+ * deep_frame/topology_optimizers.py:61-63): asymptotes, move limits, convex
+ * approximation and the primal-dual interior-point subproblem, n variables on the
+ * device, 1 <= m <= TF_MMA_MAX_M constraints.
+ * ------------------------------------------------------------------------------------ */
+#define TF_MMA_MAX_M 8
+typedef struct tf_mma tf_mma;
+typedef struct tf_mma_settings {
+  double move, asyinit, asydecr, asyincr, asymin, asymax, raa0, albefa, epsimin;
+} tf_mma_settings;
+TF_API int tf_mma_create(int32_t m, int64_t n, tf_mma** out);
+/* Device arrays: xval, xmin, xmax, xold1, xold2, df0dx [n]; dfdx [m][n]; low, upp [n]
+ * (in: previous asymptotes, out: new); xnew [n].  Host arrays: fval, a, c, d [m];
+ * y_out, lam_out [m] and z_out, newton_iterations may be NULL.  settings NULL = defaults
+ * (move 0.5, asyinit 0.5, asydecr 0.7, asyincr 1.2, asymin 0.01, asymax 10, raa0 1e-5,
+ * albefa 0.1, epsimin 1e-7). */
+TF_API int tf_mma_step(tf_mma* h, int32_t iteration, const double* xval, const double* xmin, const double* xmax,
+                       const double* xold1, const double* xold2, const double* df0dx, const double* fval, const double* dfdx,
+                       double* low, double* upp, double a0, const double* a, const double* c, const double* d,
+                       const tf_mma_settings* settings, double* xnew, double* y_out, double* z_out, double* lam_out,
+                       int32_t* newton_iterations, void* stream);
+TF_API int tf_mma_destroy(tf_mma* h);
+TF_API const char* tf_mma_last_error(const tf_mma* h);
+
 /* CUDA-event timing of the kernel classes this handle launches, recorded on the launching
  * stream: 0 FP64 finest operator of the PCG, 1 finest-level smoothing / residual in the work
  * precision, 2 Galerkin-level operators, 3 restriction + prolongation, 4 PCG vector kernels,
@@ -181,8 +227,8 @@ TF_API int64_t tf_launch_count(void);
  * topology_multigrid.py:543-548).  Idempotent for NULL. */
 TF_API int tf_destroy(tf_handle* h);
 
-/* Message of the last failed call on `h` (or, with h NULL, of the last failed tf_create or
- * tf_gram_static on this thread). */
+/* Message of the last failed call on `h` (or, with h NULL, of the last failed tf_create,
+ * tf_filter_create, tf_mma_create or tf_gram_static on this thread). */
 TF_API const char* tf_last_error(const tf_handle* h);
 
 #ifdef __cplusplus
