@@ -20,7 +20,7 @@ SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set
            "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
 SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_destroy",
-            "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error")
+            "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error", "tf_simp")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
 
 
@@ -101,6 +101,7 @@ def load():
                             ctypes.POINTER(I32), P],
             "tf_mma_destroy": [P],
             "tf_mma_last_error": [P],
+            "tf_simp": [P, I64, D, D, D, P, P, P, P, P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

@@ -107,7 +107,7 @@ class InterfaceCovariance:
             solved.append((key, ks, forces, u, report))
         return solved
 
-    def measure_from(self, solved, scale, gradients=True):
+    def measure_from(self, solved, scale, gradients=True, worst_gradient=True):
         """Rows of the reference's measure (topology_problem.py:657-684) from device solutions."""
         mg = self.system._multigrid()
         torch = mg.torch
@@ -141,11 +141,12 @@ class InterfaceCovariance:
             for key, ks, forces, u, _ in solved:
                 m = len(ks)
                 mg.energy_device(u, coefficients=np.full(m, self.factor), scale=scale, out=grad_mean, accumulate=True)
-                comb = vectors[np.ix_(ks, keep)]
-                mg.energy_device(u, combination=comb, coefficients=weights[keep] * self.factor, scale=scale, out=grad_worst, accumulate=True)
+                if worst_gradient:
+                    comb = vectors[np.ix_(ks, keep)]
+                    mg.energy_device(u, combination=comb, coefficients=weights[keep] * self.factor, scale=scale, out=grad_worst, accumulate=True)
             limit_mean = limits.get("mean_n_mm") or 1.0
             limit_worst = limits.get("worst_n_mm") or 1.0
             rows[0].update(g=mean / limit_mean - 1, gradient=grad_mean / limit_mean)
-            rows[1].update(g=float(ks_value / limit_worst - 1), gradient=grad_worst / limit_worst)
+            rows[1].update(g=float(ks_value / limit_worst - 1), gradient=grad_worst / limit_worst if worst_gradient else None)
         self.flexibility = flex
         return rows

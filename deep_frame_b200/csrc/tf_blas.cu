@@ -85,6 +85,48 @@ namespace tfb {
 std::atomic<long long> g_launch_count{0};
 }
 
+namespace {
+// SIMP interpolation E = E0 (eps + (1 - eps) rho^p), dE/drho = E0 (1 - eps) p rho^(p-1), zero on
+// inactive cells (topology_optimization.py:657-661); one CTA also sums rho over the
+// active cells (the volume row of topology_problem.py:345) in a fixed order.
+__global__ void __launch_bounds__(1024) simp_kernel(const double* __restrict__ rho, long long n, double p, double eps, double young,
+                                                    const uint8_t* __restrict__ active, double* __restrict__ moduli,
+                                                    double* __restrict__ derivative, double* __restrict__ volume) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (long long c = threadIdx.x; c < n; c += blockDim.x) {
+    const double r = rho[c];
+    const bool on = active ? active[c] != 0 : true;
+    moduli[c] = on ? young * (eps + (1.0 - eps) * pow(r, p)) : 0.0;
+    if (derivative) derivative[c] = on ? young * (1.0 - eps) * p * pow(r, p - 1.0) : 0.0;
+    if (on) acc += r;
+  }
+  if (!volume) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    *volume = t;
+  }
+}
+}  // namespace
+
+extern "C" int tf_simp(const double* rho_dev, int64_t n, double penalization, double min_stiffness_ratio, double young,
+                       const uint8_t* active_dev, double* moduli_dev, double* derivative_dev, double* volume_dev, void* stream) {
+  if (!rho_dev || !moduli_dev || n < 1 || !(penalization >= 1.0) || !(min_stiffness_ratio > 0.0 && min_stiffness_ratio < 1.0) ||
+      !(young > 0.0)) {
+    record_unhandled_error("tf_simp: invalid arguments");
+    return TF_INVALID;
+  }
+  simp_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(rho_dev, n, penalization, min_stiffness_ratio, young, active_dev,
+                                                                  moduli_dev, derivative_dev, volume_dev);
+  g_launch_count.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError() == cudaSuccess ? TF_OK : TF_CUDA;
+}
+
 extern "C" int64_t tf_launch_count(void) { return g_launch_count.load(); }
 
 extern "C" int64_t tf_gram_scratch_size(int32_t ra, int32_t rb) {

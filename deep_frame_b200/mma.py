@@ -79,7 +79,7 @@ def mmasub(m, n, iter, xval, xmin, xmax, xold1, xold2, f0val, df0dx, fval, dfdx,
     solver = _solvers.get(key)
     if solver is None:
         solver = _solvers[key] = MMA(m, n, device)
-    dev = lambda v: torch.as_tensor(np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=float).ravel(), (n,))), device=device)
+    dev = lambda v: torch.as_tensor(np.array(np.broadcast_to(np.asarray(v, dtype=float).ravel(), (n,))), device=device)
     lo, up = dev(low), dev(upp)
     xnew, y, z, lam = solver.step(iter, dev(xval), dev(xmin), dev(xmax), dev(xold1), dev(xold2), dev(df0dx), fval,
                                   torch.as_tensor(np.ascontiguousarray(np.asarray(dfdx, dtype=float).reshape(m, n)), device=device),

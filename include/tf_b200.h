@@ -165,6 +165,13 @@ TF_API int64_t tf_gram_scratch_size(int32_t ra, int32_t rb);
 TF_API int tf_gram_static(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
                           void* stream);
 
+/* SIMP interpolation (HexElasticity.solve, deep_frame/topology_optimization.py:657-661):
+ * moduli = young (eps + (1 - eps) rho^p), derivative = young (1 - eps) p rho^(p-1), both zero
+ * where active[c] == 0 (active may be NULL); volume (device scalar, may be NULL) receives
+ * sum of rho over the active cells (the volume row of topology_problem.py:345). */
+TF_API int tf_simp(const double* rho_dev, int64_t n, double penalization, double min_stiffness_ratio, double young,
+                   const uint8_t* active_dev, double* moduli_dev, double* derivative_dev, double* volume_dev, void* stream);
+
 /* ------------------------------------------------------------------------------------
  * Cone density filter (ConeFilter / cone_filter / DensityMap.filtered, .pullback,
  * .project: deep_frame/topology_optimization.py:1082-1178).  Cells are C-ordered over
