@@ -257,22 +257,30 @@ __device__ __forceinline__ void stage_tile(T* __restrict__ s, const Geo& g, cons
   }
 }
 
-// Finest level: out = sum_e E_e K0[c_n(e), :] u_e from the staged tiles.
+// Finest-level tile: component-planar shared rows of pitch FP (in words) chosen so
+// that a warp (8 z-lanes x 4 y-rows) reads 32 distinct banks; the thread block is
+// (tz, TY, TX) so no index needs a runtime division.
+constexpr int FTZ = 8;                       // z nodes per fine tile
+constexpr int FP32_PITCH = 24, FP64_PITCH = 24;   // row pitch in elements: conflict-free warps for tz = 8
+template <typename T> struct FinePitch { static constexpr int P = sizeof(T) == 4 ? FP32_PITCH : FP64_PITCH; };
+
 template <typename T>
 __device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __restrict__ su, const T* __restrict__ sE,
                                                int lx, int ly, int lz, T out[3]) {
+  constexpr int P = FinePitch<T>::P;
+  constexpr int PLANE = HX * HY * P;   // one component plane
   T acc[8][3];
 #pragma unroll
   for (int e = 0; e < 8; ++e) { acc[e][0] = T(0); acc[e][1] = T(0); acc[e][2] = T(0); }
-  const T* base = su + 3 * (((lx + 1) * HY + (ly + 1)) * HZ + (lz + 1));
+  const T* base = su + ((lx + 1) * HY + (ly + 1)) * P + (lz + 1);
 #pragma unroll
   for (int di = -1; di <= 1; ++di) {
 #pragma unroll
     for (int dj = -1; dj <= 1; ++dj) {
 #pragma unroll
       for (int dk = -1; dk <= 1; ++dk) {
-        const T* p = base + 3 * ((di * HY + dj) * HZ + dk);
-        const T u0 = p[0], u1 = p[1], u2 = p[2];
+        const T* p = base + (di * HY + dj) * P + dk;
+        const T u0 = p[0], u1 = p[PLANE], u2 = p[2 * PLANE];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
@@ -283,7 +291,9 @@ __device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __r
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
             const int row = (3 * cn + a) * 24 + 3 * cm;
-            acc[e][a] += K.k[row] * u0 + K.k[row + 1] * u1 + K.k[row + 2] * u2;
+            T t = fma(K.k[row], u0, acc[e][a]);
+            t = fma(K.k[row + 1], u1, t);
+            acc[e][a] = fma(K.k[row + 2], u2, t);
           }
         }
       }
@@ -294,16 +304,18 @@ __device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __r
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     const T w = eb[((e >> 2) * EY + ((e >> 1) & 1)) * EZ + (e & 1)];
-    out[0] += w * acc[e][0];
-    out[1] += w * acc[e][1];
-    out[2] += w * acc[e][2];
+    out[0] = fma(w, acc[e][0], out[0]);
+    out[1] = fma(w, acc[e][1], out[1]);
+    out[2] = fma(w, acc[e][2], out[2]);
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TX * TY * TZMAX) fine_level_kernel(const __grid_constant__ K0Param<T> K, const LevelArgs<T> a,
-                                                                    int mode, TileMap tm) {
-  __shared__ T su[HALO * 3];
+__global__ void __launch_bounds__(TX * TY * FTZ) fine_level_kernel(const __grid_constant__ K0Param<T> K, const LevelArgs<T> a,
+                                                                  int mode, TileMap tm) {
+  constexpr int P = FinePitch<T>::P;
+  constexpr int PLANE = HX * HY * P;
+  __shared__ T su[3 * PLANE];
   __shared__ T sE[EX * EY * EZ];
   const int col = blockIdx.y;
   if (a.gate && !*a.gate) return;
@@ -311,21 +323,41 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) fine_level_kernel(const __gri
   const Geo& g = a.g;
   const int b = blockIdx.x;
   const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
-  const int tz = tm.tz;
+  const int tz = FTZ;
   const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
   const long long off = (long long)col * a.colstride;
-  stage_tile(su, g, a.u + off, a.mask, x0, y0, z0, tz);
-  const int ez = tz + 1;
-  for (int t = threadIdx.x; t < EX * EY * ez; t += blockDim.x) {
-    const int cz = t % ez, rr = t / ez, cy = rr % EY, cx = rr / EY;
-    const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
-    T v = T(0);
-    if ((unsigned)gx < (unsigned)g.ex && (unsigned)gy < (unsigned)g.ey && (unsigned)gz < (unsigned)g.ez)
-      v = a.E[((long long)gx * g.ey + gy) * g.ez + gz];
-    sE[(cx * EY + cy) * EZ + cz] = v;
+  const T* u = a.u + off;
+  const int lz = threadIdx.x, ly = threadIdx.y, lx = threadIdx.z;
+  // stage the masked node halo: (TX+2) x (TY+2) x (FTZ+2)
+  for (int cx = lx; cx < HX; cx += TX) {
+    const int gx = x0 - 1 + cx;
+    for (int cy = ly; cy < HY; cy += TY) {
+      const int gy = y0 - 1 + cy;
+      for (int cz = lz; cz < FTZ + 2; cz += FTZ) {
+        const int gz = z0 - 1 + cz;
+        T v0 = T(0), v1 = T(0), v2 = T(0);
+        if ((unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz)
+          load_masked(u, a.mask, ((long long)gx * g.ny + gy) * g.nz + gz, v0, v1, v2);
+        T* d = su + (cx * HY + cy) * P + cz;
+        d[0] = v0; d[PLANE] = v1; d[2 * PLANE] = v2;
+      }
+    }
+  }
+  // stage the element moduli: (TX+1) x (TY+1) x (FTZ+1), zero outside the grid
+  for (int cx = lx; cx < EX; cx += TX) {
+    const int gx = x0 - 1 + cx;
+    for (int cy = ly; cy < EY; cy += TY) {
+      const int gy = y0 - 1 + cy;
+      for (int cz = lz; cz < FTZ + 1; cz += FTZ) {
+        const int gz = z0 - 1 + cz;
+        T v = T(0);
+        if ((unsigned)gx < (unsigned)g.ex && (unsigned)gy < (unsigned)g.ey && (unsigned)gz < (unsigned)g.ez)
+          v = a.E[((long long)gx * g.ey + gy) * g.ez + gz];
+        sE[(cx * EY + cy) * EZ + cz] = v;
+      }
+    }
   }
   __syncthreads();
-  const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
   const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   T av[3];
@@ -405,7 +437,7 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) block_level_kernel(const Leve
             const T* p = su + c * HALO * 3 + noff;
             const T u0 = p[0], u1 = p[1], u2 = p[2];
 #pragma unroll
-            for (int q = 0; q < 3; ++q) out[c][q] += bv[3 * q] * u0 + bv[3 * q + 1] * u1 + bv[3 * q + 2] * u2;
+            for (int q = 0; q < 3; ++q) out[c][q] = fma(bv[3 * q + 2], u2, fma(bv[3 * q + 1], u1, fma(bv[3 * q], u0, out[c][q])));
           }
         }
       }

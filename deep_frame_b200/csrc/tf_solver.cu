@@ -278,14 +278,19 @@ template <> const K0Param<float>& k0param<float>(tf_handle* h) { return h->k32; 
 template <typename T>
 void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st, int timer = -1) {
   TimedRange tr(h->timers, timer >= 0 ? timer : (l == 0 ? TIMER_FINE_WORK : TIMER_COARSE), st);
-  const TileMap tm = tile_map(a.g);
-  const int threads = TX * TY * tm.tz;
-  const unsigned tiles = (unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z);
   if (l == 0) {
-    dim3 grid(tiles, a.ncol);
-    fine_level_kernel<T><<<grid, threads, 0, st>>>(k0param<T>(h), a, mode, tm);
+    TileMap tm;
+    tm.tz = FTZ;
+    tm.tiles_x = (a.g.nx + TX - 1) / TX;
+    tm.tiles_y = (a.g.ny + TY - 1) / TY;
+    tm.tiles_z = (a.g.nz + FTZ - 1) / FTZ;
+    dim3 grid((unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z), a.ncol);
+    fine_level_kernel<T><<<grid, dim3(FTZ, TY, TX), 0, st>>>(k0param<T>(h), a, mode, tm);
     TF_LAUNCH_CHECK("fine_level_kernel");
   } else {
+    const TileMap tm = tile_map(a.g);
+    const int threads = TX * TY * tm.tz;
+    const unsigned tiles = (unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z);
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
     dim3 grid(tiles, (a.ncol + cb - 1) / cb);
     const size_t smem = sizeof(T) * 3 * HALO * cb;
