@@ -21,6 +21,20 @@ struct Geo {
 
 template <typename T> struct K0Param { T k[576]; };
 
+// Element stiffness of the finest level in constant memory.  A handle claims one
+// of K0_SLOTS slots (per distinct K0); the operator kernels are instantiated per
+// slot so every coefficient is a compile-time constant-bank operand of its FMA.
+constexpr int K0_SLOTS = 2;
+__constant__ float c_k0f[K0_SLOTS][576];
+__constant__ double c_k0d[K0_SLOTS][576];
+template <typename T, int SLOT> struct K0Const;
+template <int SLOT> struct K0Const<float, SLOT> {
+  __device__ __forceinline__ float operator[](int i) const { return c_k0f[SLOT][i]; }
+};
+template <int SLOT> struct K0Const<double, SLOT> {
+  __device__ __forceinline__ double operator[](int i) const { return c_k0d[SLOT][i]; }
+};
+
 // corner numbering of the reference element (deep_frame/topology_optimization.py:246-249)
 __host__ __device__ constexpr int corner_id(int x, int y, int z) {
   return z * 4 + (y ? (x ? 2 : 3) : (x ? 1 : 0));
@@ -264,8 +278,8 @@ constexpr int FTZ = 8;                       // z nodes per fine tile
 constexpr int FP32_PITCH = 24, FP64_PITCH = 24;   // row pitch in elements: conflict-free warps for tz = 8
 template <typename T> struct FinePitch { static constexpr int P = sizeof(T) == 4 ? FP32_PITCH : FP64_PITCH; };
 
-template <typename T>
-__device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __restrict__ su, const T* __restrict__ sE,
+template <typename T, typename KC>
+__device__ __forceinline__ void fine_tile_node(const KC& K, const T* __restrict__ su, const T* __restrict__ sE,
                                                int lx, int ly, int lz, T out[3]) {
   constexpr int P = FinePitch<T>::P;
   constexpr int PLANE = HX * HY * P;   // one component plane
@@ -291,9 +305,9 @@ __device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __r
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
             const int row = (3 * cn + a) * 24 + 3 * cm;
-            T t = fma(K.k[row], u0, acc[e][a]);
-            t = fma(K.k[row + 1], u1, t);
-            acc[e][a] = fma(K.k[row + 2], u2, t);
+            T t = fma(K[row], u0, acc[e][a]);
+            t = fma(K[row + 1], u1, t);
+            acc[e][a] = fma(K[row + 2], u2, t);
           }
         }
       }
@@ -310,9 +324,9 @@ __device__ __forceinline__ void fine_tile_node(const K0Param<T>& K, const T* __r
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(TX * TY * FTZ) fine_level_kernel(const __grid_constant__ K0Param<T> K, const LevelArgs<T> a,
-                                                                  int mode, TileMap tm) {
+template <typename T, int SLOT>
+__global__ void __launch_bounds__(TX * TY * FTZ) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+  const K0Const<T, SLOT> K;
   constexpr int P = FinePitch<T>::P;
   constexpr int PLANE = HX * HY * P;
   __shared__ T su[3 * PLANE];

@@ -16,6 +16,7 @@
 #include <type_traits>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -163,6 +164,7 @@ struct tf_handle {
   VBufs<float> wf;
   VBufs<double> wd;
   DevBuf tmp_diag;
+  int k0_slot = -1;   // constant-memory slot of ke (set on the first finest-level launch)
   Timers timers;
   std::string err;
   ~tf_handle() {
@@ -275,6 +277,40 @@ template <typename T> const K0Param<T>& k0param(tf_handle* h);
 template <> const K0Param<double>& k0param<double>(tf_handle* h) { return h->k64; }
 template <> const K0Param<float>& k0param<float>(tf_handle* h) { return h->k32; }
 
+// Constant-memory slots of the element stiffness: one per distinct K0 in the
+// process, uploaded once per device.  Guarded by a mutex; the upload is
+// synchronous, before the first launch that reads the slot.
+std::mutex g_k0_mutex;
+double g_k0_slots[K0_SLOTS][576];
+int g_k0_used = 0;
+unsigned long long g_k0_uploaded[K0_SLOTS] = {};   // bit per device ordinal
+
+int k0_slot(tf_handle* h) {
+  if (h->k0_slot >= 0) return h->k0_slot;
+  int device = 0;
+  TF_CUDA_CHECK(cudaGetDevice(&device));
+  require(device < 64, "device ordinal out of range for the constant-memory slots");
+  std::lock_guard<std::mutex> lock(g_k0_mutex);
+  int slot = -1;
+  for (int s = 0; s < g_k0_used; ++s)
+    if (std::memcmp(g_k0_slots[s], h->ke, sizeof(h->ke)) == 0) slot = s;
+  if (slot < 0) {
+    if (g_k0_used == K0_SLOTS)
+      throw Error(TF_INVALID, "more distinct element stiffness matrices in one process than constant-memory slots (2)");
+    slot = g_k0_used++;
+    std::memcpy(g_k0_slots[slot], h->ke, sizeof(h->ke));
+  }
+  if (!(g_k0_uploaded[slot] >> device & 1ull)) {
+    float f[576];
+    for (int t = 0; t < 576; ++t) f[t] = static_cast<float>(h->ke[t]);
+    TF_CUDA_CHECK(cudaMemcpyToSymbol(c_k0d, h->ke, sizeof(h->ke), sizeof(h->ke) * slot));
+    TF_CUDA_CHECK(cudaMemcpyToSymbol(c_k0f, f, sizeof(f), sizeof(f) * slot));
+    g_k0_uploaded[slot] |= 1ull << device;
+  }
+  h->k0_slot = slot;
+  return slot;
+}
+
 template <typename T>
 void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st, int timer = -1) {
   TimedRange tr(h->timers, timer >= 0 ? timer : (l == 0 ? TIMER_FINE_WORK : TIMER_COARSE), st);
@@ -285,7 +321,9 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     tm.tiles_y = (a.g.ny + TY - 1) / TY;
     tm.tiles_z = (a.g.nz + FTZ - 1) / FTZ;
     dim3 grid((unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z), a.ncol);
-    fine_level_kernel<T><<<grid, dim3(FTZ, TY, TX), 0, st>>>(k0param<T>(h), a, mode, tm);
+    const int slot = k0_slot(h);
+    if (slot == 0) fine_level_kernel<T, 0><<<grid, dim3(FTZ, TY, TX), 0, st>>>(a, mode, tm);
+    else fine_level_kernel<T, 1><<<grid, dim3(FTZ, TY, TX), 0, st>>>(a, mode, tm);
     TF_LAUNCH_CHECK("fine_level_kernel");
   } else {
     const TileMap tm = tile_map(a.g);
