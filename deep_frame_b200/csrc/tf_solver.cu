@@ -164,7 +164,9 @@ struct tf_handle {
   VBufs<float> wf;
   VBufs<double> wd;
   DevBuf tmp_diag;
-  int k0_slot = -1;   // constant-memory slot of ke (set on the first finest-level launch)
+  int k0_slot = -1;   // constant-memory slot of ke, its device and the slot version it saw
+  int k0_device = -1;
+  unsigned long long k0_version = 0;
   Timers timers;
   std::string err;
   ~tf_handle() {
@@ -277,37 +279,52 @@ template <typename T> const K0Param<T>& k0param(tf_handle* h);
 template <> const K0Param<double>& k0param<double>(tf_handle* h) { return h->k64; }
 template <> const K0Param<float>& k0param<float>(tf_handle* h) { return h->k32; }
 
-// Constant-memory slots of the element stiffness: one per distinct K0 in the
-// process, uploaded once per device.  Guarded by a mutex; the upload is
-// synchronous, before the first launch that reads the slot.
+// Constant-memory slots of the element stiffness, per device.  A handle whose
+// K0 is not resident takes the least recently used slot: the device is drained
+// first (no kernel in flight can still read the slot), then the FP64 and FP32
+// copies are uploaded.  A per-slot version lets a handle skip the comparison
+// while its slot is untouched.
+constexpr int MAX_DEVICES = 64;
+struct K0Slots {
+  double content[K0_SLOTS][576];
+  unsigned long long version[K0_SLOTS] = {};
+  unsigned long long last_use[K0_SLOTS] = {};
+  bool valid[K0_SLOTS] = {};
+};
 std::mutex g_k0_mutex;
-double g_k0_slots[K0_SLOTS][576];
-int g_k0_used = 0;
-unsigned long long g_k0_uploaded[K0_SLOTS] = {};   // bit per device ordinal
+K0Slots g_k0[MAX_DEVICES];
+unsigned long long g_k0_clock = 0, g_k0_versions = 0;
 
 int k0_slot(tf_handle* h) {
-  if (h->k0_slot >= 0) return h->k0_slot;
   int device = 0;
   TF_CUDA_CHECK(cudaGetDevice(&device));
-  require(device < 64, "device ordinal out of range for the constant-memory slots");
+  require(device >= 0 && device < MAX_DEVICES, "device ordinal out of range for the constant-memory slots");
   std::lock_guard<std::mutex> lock(g_k0_mutex);
-  int slot = -1;
-  for (int s = 0; s < g_k0_used; ++s)
-    if (std::memcmp(g_k0_slots[s], h->ke, sizeof(h->ke)) == 0) slot = s;
-  if (slot < 0) {
-    if (g_k0_used == K0_SLOTS)
-      throw Error(TF_INVALID, "more distinct element stiffness matrices in one process than constant-memory slots (2)");
-    slot = g_k0_used++;
-    std::memcpy(g_k0_slots[slot], h->ke, sizeof(h->ke));
+  K0Slots& t = g_k0[device];
+  if (h->k0_slot >= 0 && h->k0_device == device && t.version[h->k0_slot] == h->k0_version) {
+    t.last_use[h->k0_slot] = ++g_k0_clock;
+    return h->k0_slot;
   }
-  if (!(g_k0_uploaded[slot] >> device & 1ull)) {
+  int slot = -1;
+  for (int s = 0; s < K0_SLOTS; ++s)
+    if (t.valid[s] && std::memcmp(t.content[s], h->ke, sizeof(h->ke)) == 0) slot = s;
+  if (slot < 0) {
+    slot = 0;
+    for (int s = 1; s < K0_SLOTS; ++s)
+      if (!t.valid[s] || (t.valid[slot] && t.last_use[s] < t.last_use[slot])) slot = s;
+    if (t.valid[slot]) TF_CUDA_CHECK(cudaDeviceSynchronize());
     float f[576];
-    for (int t = 0; t < 576; ++t) f[t] = static_cast<float>(h->ke[t]);
+    for (int q = 0; q < 576; ++q) f[q] = static_cast<float>(h->ke[q]);
     TF_CUDA_CHECK(cudaMemcpyToSymbol(c_k0d, h->ke, sizeof(h->ke), sizeof(h->ke) * slot));
     TF_CUDA_CHECK(cudaMemcpyToSymbol(c_k0f, f, sizeof(f), sizeof(f) * slot));
-    g_k0_uploaded[slot] |= 1ull << device;
+    std::memcpy(t.content[slot], h->ke, sizeof(h->ke));
+    t.valid[slot] = true;
+    t.version[slot] = ++g_k0_versions;
   }
+  t.last_use[slot] = ++g_k0_clock;
   h->k0_slot = slot;
+  h->k0_device = device;
+  h->k0_version = t.version[slot];
   return slot;
 }
 
