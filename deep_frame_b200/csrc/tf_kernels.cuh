@@ -19,6 +19,11 @@ struct Geo {
   long long nnode;  // nx * ny * nz
 };
 
+// corner numbering of the reference element (deep_frame/topology_optimization.py:246-249)
+__host__ __device__ constexpr int corner_id(int x, int y, int z) {
+  return z * 4 + (y ? (x ? 2 : 3) : (x ? 1 : 0));
+}
+
 template <typename T> struct K0Param { T k[576]; };
 
 // Element stiffness of the finest level in constant memory.  A handle claims one
@@ -27,18 +32,41 @@ template <typename T> struct K0Param { T k[576]; };
 constexpr int K0_SLOTS = 2;
 __constant__ float c_k0f[K0_SLOTS][576];
 __constant__ double c_k0d[K0_SLOTS][576];
-template <typename T, int SLOT> struct K0Const;
-template <int SLOT> struct K0Const<float, SLOT> {
-  __device__ __forceinline__ float operator[](int i) const { return c_k0f[SLOT][i]; }
+// For a box element with an axis-aligned orthotropic (or isotropic) material,
+// K0 is invariant under the 8 reflections of the element: with R the corner
+// bits of the row corner c,  K0[3c+a][3d+b] = s_a s_b K0[a][3(d xor R)+b]
+// (s = -1 on reflected axes).  Only the 72 coefficients of corner 0's rows are
+// distinct, and every index and sign is a compile-time constant.
+__constant__ float c_kcf[K0_SLOTS][72];
+__constant__ double c_kcd[K0_SLOTS][72];
+
+__host__ __device__ constexpr int corner_x(int c) { return (c == 1 || c == 2 || c == 5 || c == 6) ? 1 : 0; }
+__host__ __device__ constexpr int corner_y(int c) { return (c == 2 || c == 3 || c == 6 || c == 7) ? 1 : 0; }
+__host__ __device__ constexpr int corner_z(int c) { return c >> 2; }
+
+template <typename T, int SLOT, bool REFLECT> struct K0Const;
+template <int SLOT> struct K0Const<float, SLOT, false> {
+  __device__ __forceinline__ float operator()(int cn, int a, int cm, int b) const { return c_k0f[SLOT][(3 * cn + a) * 24 + 3 * cm + b]; }
 };
-template <int SLOT> struct K0Const<double, SLOT> {
-  __device__ __forceinline__ double operator[](int i) const { return c_k0d[SLOT][i]; }
+template <int SLOT> struct K0Const<double, SLOT, false> {
+  __device__ __forceinline__ double operator()(int cn, int a, int cm, int b) const { return c_k0d[SLOT][(3 * cn + a) * 24 + 3 * cm + b]; }
+};
+template <typename T, int SLOT>
+__device__ __forceinline__ T reflected_k0(const T (&table)[K0_SLOTS][72], int cn, int a, int cm, int b) {
+  const int rx = corner_x(cn), ry = corner_y(cn), rz = corner_z(cn);
+  const int d = corner_id(corner_x(cm) ^ rx, corner_y(cm) ^ ry, corner_z(cm) ^ rz);
+  const int ra = a == 0 ? rx : (a == 1 ? ry : rz);
+  const int rb = b == 0 ? rx : (b == 1 ? ry : rz);
+  const T v = table[SLOT][(a * 8 + d) * 3 + b];
+  return (ra ^ rb) ? -v : v;
+}
+template <int SLOT> struct K0Const<float, SLOT, true> {
+  __device__ __forceinline__ float operator()(int cn, int a, int cm, int b) const { return reflected_k0<float, SLOT>(c_kcf, cn, a, cm, b); }
+};
+template <int SLOT> struct K0Const<double, SLOT, true> {
+  __device__ __forceinline__ double operator()(int cn, int a, int cm, int b) const { return reflected_k0<double, SLOT>(c_kcd, cn, a, cm, b); }
 };
 
-// corner numbering of the reference element (deep_frame/topology_optimization.py:246-249)
-__host__ __device__ constexpr int corner_id(int x, int y, int z) {
-  return z * 4 + (y ? (x ? 2 : 3) : (x ? 1 : 0));
-}
 
 __device__ __forceinline__ void node_coords(long long n, const Geo& g, int& i, int& j, int& k) {
   k = static_cast<int>(n % g.nz);
@@ -304,10 +332,9 @@ __device__ __forceinline__ void fine_tile_node(const KC& K, const T* __restrict_
           const int cm = corner_id(cx, cy, cz);
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            const int row = (3 * cn + a) * 24 + 3 * cm;
-            T t = fma(K[row], u0, acc[e][a]);
-            t = fma(K[row + 1], u1, t);
-            acc[e][a] = fma(K[row + 2], u2, t);
+            T t = fma(K(cn, a, cm, 0), u0, acc[e][a]);
+            t = fma(K(cn, a, cm, 1), u1, t);
+            acc[e][a] = fma(K(cn, a, cm, 2), u2, t);
           }
         }
       }
@@ -324,9 +351,9 @@ __device__ __forceinline__ void fine_tile_node(const KC& K, const T* __restrict_
   }
 }
 
-template <typename T, int SLOT>
+template <typename T, int SLOT, bool REFLECT>
 __global__ void __launch_bounds__(TX * TY * FTZ) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
-  const K0Const<T, SLOT> K;
+  const K0Const<T, SLOT, REFLECT> K;
   constexpr int P = FinePitch<T>::P;
   constexpr int PLANE = HX * HY * P;
   __shared__ T su[3 * PLANE];

@@ -164,6 +164,7 @@ struct tf_handle {
   VBufs<float> wf;
   VBufs<double> wd;
   DevBuf tmp_diag;
+  bool k0_reflect = false;   // ke has the 8-fold reflection symmetry (72 distinct coefficients)
   int k0_slot = -1;   // constant-memory slot of ke, its device and the slot version it saw
   int k0_device = -1;
   unsigned long long k0_version = 0;
@@ -317,6 +318,16 @@ int k0_slot(tf_handle* h) {
     for (int q = 0; q < 576; ++q) f[q] = static_cast<float>(h->ke[q]);
     TF_CUDA_CHECK(cudaMemcpyToSymbol(c_k0d, h->ke, sizeof(h->ke), sizeof(h->ke) * slot));
     TF_CUDA_CHECK(cudaMemcpyToSymbol(c_k0f, f, sizeof(f), sizeof(f) * slot));
+    double kc[72];
+    float kcf[72];
+    for (int a = 0; a < 3; ++a)
+      for (int d = 0; d < 8; ++d)
+        for (int b = 0; b < 3; ++b) {
+          kc[(a * 8 + d) * 3 + b] = h->ke[a * 24 + 3 * d + b];
+          kcf[(a * 8 + d) * 3 + b] = static_cast<float>(kc[(a * 8 + d) * 3 + b]);
+        }
+    TF_CUDA_CHECK(cudaMemcpyToSymbol(c_kcd, kc, sizeof(kc), sizeof(kc) * slot));
+    TF_CUDA_CHECK(cudaMemcpyToSymbol(c_kcf, kcf, sizeof(kcf), sizeof(kcf) * slot));
     std::memcpy(t.content[slot], h->ke, sizeof(h->ke));
     t.valid[slot] = true;
     t.version[slot] = ++g_k0_versions;
@@ -339,8 +350,14 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     tm.tiles_z = (a.g.nz + FTZ - 1) / FTZ;
     dim3 grid((unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z), a.ncol);
     const int slot = k0_slot(h);
-    if (slot == 0) fine_level_kernel<T, 0><<<grid, dim3(FTZ, TY, TX), 0, st>>>(a, mode, tm);
-    else fine_level_kernel<T, 1><<<grid, dim3(FTZ, TY, TX), 0, st>>>(a, mode, tm);
+    const dim3 block(FTZ, TY, TX);
+    if (h->k0_reflect) {
+      if (slot == 0) fine_level_kernel<T, 0, true><<<grid, block, 0, st>>>(a, mode, tm);
+      else fine_level_kernel<T, 1, true><<<grid, block, 0, st>>>(a, mode, tm);
+    } else {
+      if (slot == 0) fine_level_kernel<T, 0, false><<<grid, block, 0, st>>>(a, mode, tm);
+      else fine_level_kernel<T, 1, false><<<grid, block, 0, st>>>(a, mode, tm);
+    }
     TF_LAUNCH_CHECK("fine_level_kernel");
   } else {
     const TileMap tm = tile_map(a.g);
@@ -912,6 +929,22 @@ extern "C" int tf_create(const tf_grid* grid, const double* ke, const double* me
       h->k32.k[t] = static_cast<float>(ke[t]);
     }
     (void)me;
+    {
+      // reflection symmetry of ke (box element, axis-aligned orthotropic material)
+      double kmax = 0.0, err = 0.0;
+      for (int t = 0; t < 576; ++t) kmax = std::max(kmax, std::fabs(ke[t]));
+      for (int c = 0; c < 8; ++c)
+        for (int a = 0; a < 3; ++a)
+          for (int d = 0; d < 8; ++d)
+            for (int b = 0; b < 3; ++b) {
+              const int rx = corner_x(c), ry = corner_y(c), rz = corner_z(c);
+              const int rd = corner_id(corner_x(d) ^ rx, corner_y(d) ^ ry, corner_z(d) ^ rz);
+              const int ra = a == 0 ? rx : (a == 1 ? ry : rz), rb = b == 0 ? rx : (b == 1 ? ry : rz);
+              const double v = ((ra ^ rb) ? -1.0 : 1.0) * ke[a * 24 + 3 * rd + b];
+              err = std::max(err, std::fabs(ke[(3 * c + a) * 24 + 3 * d + b] - v));
+            }
+      h->k0_reflect = err <= 1e-13 * kmax;
+    }
     // level count and padding (topology_multigrid.py:58-63)
     int count = 2;
     auto coarse_dofs = [&](int c) {
