@@ -299,113 +299,135 @@ __device__ __forceinline__ void stage_tile(T* __restrict__ s, const Geo& g, cons
   }
 }
 
-// Finest-level tile: component-planar shared rows of pitch FP (in words) chosen so
-// that a warp (8 z-lanes x 4 y-rows) reads 32 distinct banks; the thread block is
-// (tz, TY, TX) so no index needs a runtime division.
-constexpr int FTZ = 8;                       // z nodes per fine tile
-constexpr int FP32_PITCH = 24, FP64_PITCH = 24;   // row pitch in elements: conflict-free warps for tz = 8
-template <typename T> struct FinePitch { static constexpr int P = sizeof(T) == 4 ? FP32_PITCH : FP64_PITCH; };
+// Finest-level tile.  The thread block is (TZ, TY, FTXT) and every thread owns
+// NPT nodes adjacent in x, so a CTA covers (FTXT * NPT) x TY x TZ output nodes.
+// Inputs are staged component-planar with a row pitch chosen so that a warp
+// reads distinct banks; no index needs a runtime division.
+constexpr int FTXT = 4;   // threads along x
+template <typename T, int TZ> struct FineTile {
+  static constexpr int P = sizeof(T) == 4 ? (TZ == 8 ? 24 : 41) : (TZ == 8 ? 24 : 25);   // row pitch (elements)
+};
 
-template <typename T, typename KC>
-__device__ __forceinline__ void fine_tile_node(const KC& K, const T* __restrict__ su, const T* __restrict__ sE,
-                                               int lx, int ly, int lz, T out[3]) {
-  constexpr int P = FinePitch<T>::P;
-  constexpr int PLANE = HX * HY * P;   // one component plane
-  T acc[8][3];
+template <typename T, int NPT, typename KC>
+__device__ __forceinline__ void fine_tile_nodes(const KC& K, const T* __restrict__ su, const T* __restrict__ sE, int plane, int hy, int p,
+                                                int ey, int ez, int lx, int ly, int lz, T out[NPT][3]) {
+  T acc[NPT][8][3];
 #pragma unroll
-  for (int e = 0; e < 8; ++e) { acc[e][0] = T(0); acc[e][1] = T(0); acc[e][2] = T(0); }
-  const T* base = su + ((lx + 1) * HY + (ly + 1)) * P + (lz + 1);
+  for (int q = 0; q < NPT; ++q)
 #pragma unroll
-  for (int di = -1; di <= 1; ++di) {
+    for (int e = 0; e < 8; ++e) { acc[q][e][0] = T(0); acc[q][e][1] = T(0); acc[q][e][2] = T(0); }
+  const int x0 = lx * NPT;   // first node of this thread in the tile
+  const T* base = su + ((x0 + 1) * hy + (ly + 1)) * p + (lz + 1);
+#pragma unroll
+  for (int px = -1; px <= NPT; ++px) {
 #pragma unroll
     for (int dj = -1; dj <= 1; ++dj) {
 #pragma unroll
       for (int dk = -1; dk <= 1; ++dk) {
-        const T* p = base + (di * HY + dj) * P + dk;
-        const T u0 = p[0], u1 = p[PLANE], u2 = p[2 * PLANE];
+        const T* ptr = base + (px * hy + dj) * p + dk;
+        const T u0 = ptr[0], u1 = ptr[plane], u2 = ptr[2 * plane];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
-          const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
-          if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
-          const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
-          const int cm = corner_id(cx, cy, cz);
+        for (int q = 0; q < NPT; ++q) {
+          const int di = px - q;
+          if (di < -1 || di > 1) continue;
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            T t = fma(K(cn, a, cm, 0), u0, acc[e][a]);
-            t = fma(K(cn, a, cm, 1), u1, t);
-            acc[e][a] = fma(K(cn, a, cm, 2), u2, t);
+          for (int e = 0; e < 8; ++e) {
+            const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+            const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
+            if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
+            const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+            const int cm = corner_id(cx, cy, cz);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              T t = fma(K(cn, a, cm, 0), u0, acc[q][e][a]);
+              t = fma(K(cn, a, cm, 1), u1, t);
+              acc[q][e][a] = fma(K(cn, a, cm, 2), u2, t);
+            }
           }
         }
       }
     }
   }
-  const T* eb = sE + (lx * EY + ly) * EZ + lz;
-  out[0] = out[1] = out[2] = T(0);
 #pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    const T w = eb[((e >> 2) * EY + ((e >> 1) & 1)) * EZ + (e & 1)];
-    out[0] = fma(w, acc[e][0], out[0]);
-    out[1] = fma(w, acc[e][1], out[1]);
-    out[2] = fma(w, acc[e][2], out[2]);
+  for (int q = 0; q < NPT; ++q) {
+    const T* eb = sE + ((x0 + q) * ey + ly) * ez + lz;
+    out[q][0] = out[q][1] = out[q][2] = T(0);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const T w = eb[((e >> 2) * ey + ((e >> 1) & 1)) * ez + (e & 1)];
+      out[q][0] = fma(w, acc[q][e][0], out[q][0]);
+      out[q][1] = fma(w, acc[q][e][1], out[q][1]);
+      out[q][2] = fma(w, acc[q][e][2], out[q][2]);
+    }
   }
 }
 
-template <typename T, int SLOT, bool REFLECT>
-__global__ void __launch_bounds__(TX * TY * FTZ) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+template <typename T, int SLOT, bool REFLECT, int TZ, int NPT>
+__global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+  constexpr int TXN = FTXT * NPT;                 // tile nodes along x
+  constexpr int SHX = TXN + 2, SHY = TY + 2;      // staged halo extents
+  constexpr int P = FineTile<T, TZ>::P;
+  constexpr int PLANE = SHX * SHY * P;
+  constexpr int SEX = TXN + 1, SEY = TY + 1, SEZ = TZ + 1;
+  extern __shared__ __align__(16) unsigned char fine_smem[];
+  T* su = reinterpret_cast<T*>(fine_smem);
+  T* sE = su + 3 * PLANE;
   const K0Const<T, SLOT, REFLECT> K;
-  constexpr int P = FinePitch<T>::P;
-  constexpr int PLANE = HX * HY * P;
-  __shared__ T su[3 * PLANE];
-  __shared__ T sE[EX * EY * EZ];
   const int col = blockIdx.y;
   if (a.gate && !*a.gate) return;
   if (a.active && !a.active[col]) return;
   const Geo& g = a.g;
   const int b = blockIdx.x;
   const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
-  const int tz = FTZ;
-  const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
+  const int x0 = bx * TXN, y0 = by * TY, z0 = bz * TZ;
   const long long off = (long long)col * a.colstride;
   const T* u = a.u + off;
   const int lz = threadIdx.x, ly = threadIdx.y, lx = threadIdx.z;
-  // stage the masked node halo: (TX+2) x (TY+2) x (FTZ+2)
-  for (int cx = lx; cx < HX; cx += TX) {
+  for (int cx = lx; cx < SHX; cx += FTXT) {
     const int gx = x0 - 1 + cx;
-    for (int cy = ly; cy < HY; cy += TY) {
+    for (int cy = ly; cy < SHY; cy += TY) {
       const int gy = y0 - 1 + cy;
-      for (int cz = lz; cz < FTZ + 2; cz += FTZ) {
+      for (int cz = lz; cz < TZ + 2; cz += TZ) {
         const int gz = z0 - 1 + cz;
         T v0 = T(0), v1 = T(0), v2 = T(0);
         if ((unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz)
           load_masked(u, a.mask, ((long long)gx * g.ny + gy) * g.nz + gz, v0, v1, v2);
-        T* d = su + (cx * HY + cy) * P + cz;
+        T* d = su + (cx * SHY + cy) * P + cz;
         d[0] = v0; d[PLANE] = v1; d[2 * PLANE] = v2;
       }
     }
   }
-  // stage the element moduli: (TX+1) x (TY+1) x (FTZ+1), zero outside the grid
-  for (int cx = lx; cx < EX; cx += TX) {
+  for (int cx = lx; cx < SEX; cx += FTXT) {
     const int gx = x0 - 1 + cx;
-    for (int cy = ly; cy < EY; cy += TY) {
+    for (int cy = ly; cy < SEY; cy += TY) {
       const int gy = y0 - 1 + cy;
-      for (int cz = lz; cz < FTZ + 1; cz += FTZ) {
+      for (int cz = lz; cz < SEZ; cz += TZ) {
         const int gz = z0 - 1 + cz;
         T v = T(0);
         if ((unsigned)gx < (unsigned)g.ex && (unsigned)gy < (unsigned)g.ey && (unsigned)gz < (unsigned)g.ez)
           v = a.E[((long long)gx * g.ey + gy) * g.ez + gz];
-        sE[(cx * EY + cy) * EZ + cz] = v;
+        sE[(cx * SEY + cy) * SEZ + cz] = v;
       }
     }
   }
   __syncthreads();
-  const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
-  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
-  T av[3];
-  fine_tile_node<T>(K, su, sE, lx, ly, lz, av);
-  const long long n = ((long long)i * g.ny + j) * g.nz + k;
-  const unsigned m = a.mask ? a.mask[n] : 7u;
-  epilogue(a, mode, off, n, m, av);
+  const int j = y0 + ly, k = z0 + lz;
+  if (j >= g.ny || k >= g.nz) return;
+  T av[NPT][3];
+  fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) {
+    const int i = x0 + lx * NPT + q;
+    if (i >= g.nx) continue;
+    const long long n = ((long long)i * g.ny + j) * g.nz + k;
+    const unsigned m = a.mask ? a.mask[n] : 7u;
+    epilogue(a, mode, off, n, m, av[q]);
+  }
+}
+
+template <typename T, int TZ, int NPT>
+constexpr size_t fine_smem_bytes() {
+  return sizeof(T) * (3 * (FTXT * NPT + 2) * (TY + 2) * FineTile<T, TZ>::P + (FTXT * NPT + 1) * (TY + 1) * (TZ + 1));
 }
 
 // Galerkin levels: CB columns per CTA share every block value loaded.

@@ -339,26 +339,51 @@ int k0_slot(tf_handle* h) {
   return slot;
 }
 
+// One finest-level launch: z tiles of 8 or 9 nodes (whichever wastes fewer
+// threads on this grid), two x-adjacent nodes per thread in FP32.
+template <typename T, int SLOT, bool REFLECT, int TZ>
+void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
+  constexpr int NPT = sizeof(T) == 4 ? 2 : 1;
+  constexpr size_t smem = fine_smem_bytes<T, TZ, NPT>();
+  static bool configured = false;   // per variant and process; the attribute is per function
+  if (!configured) {
+    TF_CUDA_CHECK(cudaFuncSetAttribute(fine_level_kernel<T, SLOT, REFLECT, TZ, NPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  TileMap tm;
+  tm.tz = TZ;
+  tm.tiles_x = (a.g.nx + FTXT * NPT - 1) / (FTXT * NPT);
+  tm.tiles_y = (a.g.ny + TY - 1) / TY;
+  tm.tiles_z = (a.g.nz + TZ - 1) / TZ;
+  dim3 grid((unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z), a.ncol);
+  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm);
+  TF_LAUNCH_CHECK("fine_level_kernel");
+}
+
+template <typename T>
+void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st) {
+  const int slot = k0_slot(h);
+  const int nz = a.g.nz;
+  const bool nine = h->k0_reflect && ((nz + 8) / 9) * 9 < ((nz + 7) / 8) * 8;
+  if (h->k0_reflect) {
+    if (nine) {
+      if (slot == 0) launch_fine_variant<T, 0, true, 9>(a, mode, st);
+      else launch_fine_variant<T, 1, true, 9>(a, mode, st);
+    } else {
+      if (slot == 0) launch_fine_variant<T, 0, true, 8>(a, mode, st);
+      else launch_fine_variant<T, 1, true, 8>(a, mode, st);
+    }
+  } else {
+    if (slot == 0) launch_fine_variant<T, 0, false, 8>(a, mode, st);
+    else launch_fine_variant<T, 1, false, 8>(a, mode, st);
+  }
+}
+
 template <typename T>
 void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st, int timer = -1) {
   TimedRange tr(h->timers, timer >= 0 ? timer : (l == 0 ? TIMER_FINE_WORK : TIMER_COARSE), st);
   if (l == 0) {
-    TileMap tm;
-    tm.tz = FTZ;
-    tm.tiles_x = (a.g.nx + TX - 1) / TX;
-    tm.tiles_y = (a.g.ny + TY - 1) / TY;
-    tm.tiles_z = (a.g.nz + FTZ - 1) / FTZ;
-    dim3 grid((unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z), a.ncol);
-    const int slot = k0_slot(h);
-    const dim3 block(FTZ, TY, TX);
-    if (h->k0_reflect) {
-      if (slot == 0) fine_level_kernel<T, 0, true><<<grid, block, 0, st>>>(a, mode, tm);
-      else fine_level_kernel<T, 1, true><<<grid, block, 0, st>>>(a, mode, tm);
-    } else {
-      if (slot == 0) fine_level_kernel<T, 0, false><<<grid, block, 0, st>>>(a, mode, tm);
-      else fine_level_kernel<T, 1, false><<<grid, block, 0, st>>>(a, mode, tm);
-    }
-    TF_LAUNCH_CHECK("fine_level_kernel");
+    launch_fine<T>(h, a, mode, st);
   } else {
     const TileMap tm = tile_map(a.g);
     const int threads = TX * TY * tm.tz;
