@@ -362,38 +362,50 @@ __device__ __forceinline__ void fine_tile_nodes(const KC& K, const T* __restrict
   }
 }
 
+// One CTA handles one tile for `cpb` consecutive columns: the element moduli,
+// the halo's global indices and live bits are staged once; while column c is
+// computed from shared memory, column c+1's halo is already loading into
+// registers, so the global-load latency overlaps the FMAs.
 template <typename T, int SLOT, bool REFLECT, int TZ, int NPT>
-__global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+__global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm, int cpb) {
+  constexpr int FMAXH = NPT == 1 ? 3 : 4;   // halo nodes staged per thread and column
   constexpr int TXN = FTXT * NPT;                 // tile nodes along x
   constexpr int SHX = TXN + 2, SHY = TY + 2;      // staged halo extents
   constexpr int P = FineTile<T, TZ>::P;
   constexpr int PLANE = SHX * SHY * P;
   constexpr int SEX = TXN + 1, SEY = TY + 1, SEZ = TZ + 1;
+  constexpr int NT = FTXT * TY * TZ;
+  constexpr int HALO_N = SHX * SHY * (TZ + 2);
+  static_assert(HALO_N <= FMAXH * NT, "halo exceeds the per-thread staging slots");
   extern __shared__ __align__(16) unsigned char fine_smem[];
   T* su = reinterpret_cast<T*>(fine_smem);
   T* sE = su + 3 * PLANE;
   const K0Const<T, SLOT, REFLECT> K;
-  const int col = blockIdx.y;
   if (a.gate && !*a.gate) return;
-  if (a.active && !a.active[col]) return;
+  const int c_begin = blockIdx.y * cpb;
+  const int c_end = min(a.ncol, c_begin + cpb);
   const Geo& g = a.g;
   const int b = blockIdx.x;
   const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
   const int x0 = bx * TXN, y0 = by * TY, z0 = bz * TZ;
-  const long long off = (long long)col * a.colstride;
-  const T* u = a.u + off;
   const int lz = threadIdx.x, ly = threadIdx.y, lx = threadIdx.z;
-  for (int cx = lx; cx < SHX; cx += FTXT) {
-    const int gx = x0 - 1 + cx;
-    for (int cy = ly; cy < SHY; cy += TY) {
-      const int gy = y0 - 1 + cy;
-      for (int cz = lz; cz < TZ + 2; cz += TZ) {
-        const int gz = z0 - 1 + cz;
-        T v0 = T(0), v1 = T(0), v2 = T(0);
-        if ((unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz)
-          load_masked(u, a.mask, ((long long)gx * g.ny + gy) * g.nz + gz, v0, v1, v2);
-        T* d = su + (cx * SHY + cy) * P + cz;
-        d[0] = v0; d[PLANE] = v1; d[2 * PLANE] = v2;
+  const int tid = (lx * TY + ly) * TZ + lz;
+  // halo slots of this thread: shared offset, global node index (-1 outside) and live bits
+  int soff[FMAXH], gnode[FMAXH];
+  unsigned live[FMAXH];
+#pragma unroll
+  for (int h = 0; h < FMAXH; ++h) {
+    const int t = tid + h * NT;
+    soff[h] = -1;
+    gnode[h] = -1;
+    live[h] = 0;
+    if (t < HALO_N) {
+      const int cz = t % (TZ + 2), rr = t / (TZ + 2), cy = rr % SHY, cx = rr / SHY;
+      soff[h] = (cx * SHY + cy) * P + cz;
+      const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
+      if ((unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz) {
+        gnode[h] = (gx * g.ny + gy) * g.nz + gz;
+        live[h] = a.mask ? a.mask[gnode[h]] : 7u;
       }
     }
   }
@@ -410,18 +422,61 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
       }
     }
   }
+  T pre[FMAXH][3];
+  auto fetch = [&](int c) {
+    const T* u = a.u + (long long)c * a.colstride;
+#pragma unroll
+    for (int h = 0; h < FMAXH; ++h) {
+      pre[h][0] = pre[h][1] = pre[h][2] = T(0);
+      if (gnode[h] >= 0) {
+        const T* p = u + 3 * (long long)gnode[h];
+        if (live[h] & 1u) pre[h][0] = p[0];
+        if (live[h] & 2u) pre[h][1] = p[1];
+        if (live[h] & 4u) pre[h][2] = p[2];
+      }
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int h = 0; h < FMAXH; ++h) {
+      if (soff[h] >= 0) {
+        su[soff[h]] = pre[h][0];
+        su[soff[h] + PLANE] = pre[h][1];
+        su[soff[h] + 2 * PLANE] = pre[h][2];
+      }
+    }
+  };
+  // skip to the first active column of the chunk
+  int c = c_begin;
+  while (c < c_end && a.active && !a.active[c]) ++c;
+  if (c >= c_end) return;
+  fetch(c);
+  store();
   __syncthreads();
   const int j = y0 + ly, k = z0 + lz;
-  if (j >= g.ny || k >= g.nz) return;
-  T av[NPT][3];
-  fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+  const bool owner = j < g.ny && k < g.nz;
+  while (c < c_end) {
+    int next = c + 1;
+    while (next < c_end && a.active && !a.active[next]) ++next;
+    if (next < c_end) fetch(next);
+    if (owner) {
+      T av[NPT][3];
+      fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+      const long long off = (long long)c * a.colstride;
 #pragma unroll
-  for (int q = 0; q < NPT; ++q) {
-    const int i = x0 + lx * NPT + q;
-    if (i >= g.nx) continue;
-    const long long n = ((long long)i * g.ny + j) * g.nz + k;
-    const unsigned m = a.mask ? a.mask[n] : 7u;
-    epilogue(a, mode, off, n, m, av[q]);
+      for (int q = 0; q < NPT; ++q) {
+        const int i = x0 + lx * NPT + q;
+        if (i >= g.nx) continue;
+        const long long n = ((long long)i * g.ny + j) * g.nz + k;
+        const unsigned m = a.mask ? a.mask[n] : 7u;
+        epilogue(a, mode, off, n, m, av[q]);
+      }
+    }
+    if (next >= c_end) break;
+    __syncthreads();
+    store();
+    __syncthreads();
+    c = next;
   }
 }
 

@@ -343,7 +343,7 @@ int k0_slot(tf_handle* h) {
 // threads on this grid), two x-adjacent nodes per thread in FP32.
 template <typename T, int SLOT, bool REFLECT, int TZ>
 void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
-  constexpr int NPT = sizeof(T) == 4 ? 2 : 1;
+  constexpr int NPT = (sizeof(T) == 4 && REFLECT) ? 2 : 1;
   constexpr size_t smem = fine_smem_bytes<T, TZ, NPT>();
   static bool configured = false;   // per variant and process; the attribute is per function
   if (!configured) {
@@ -355,8 +355,12 @@ void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   tm.tiles_x = (a.g.nx + FTXT * NPT - 1) / (FTXT * NPT);
   tm.tiles_y = (a.g.ny + TY - 1) / TY;
   tm.tiles_z = (a.g.nz + TZ - 1) / TZ;
-  dim3 grid((unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z), a.ncol);
-  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm);
+  const int tiles = tm.tiles_x * tm.tiles_y * tm.tiles_z;
+  // columns per CTA: enough CTAs for a few waves on 148 SMs, the rest looped inside
+  int cpb = 1;
+  while (cpb < a.ncol && (long long)tiles * ((a.ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
+  dim3 grid((unsigned)tiles, (unsigned)((a.ncol + cpb - 1) / cpb));
+  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm, cpb);
   TF_LAUNCH_CHECK("fine_level_kernel");
 }
 
