@@ -393,14 +393,9 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     const int threads = TX * TY * tm.tz;
     const unsigned tiles = (unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z);
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
-    // small levels: one column per CTA for more CTAs in flight (their blocks stay in L2)
-    if ((long long)tiles * ((a.ncol + cb - 1) / cb) < 4 * 148) {
-      dim3 grid(tiles, a.ncol);
-      block_level_kernel<T, 1><<<grid, threads, sizeof(T) * 3 * HALO, st>>>(a, mode, tm);
-    } else {
-      dim3 grid(tiles, (a.ncol + cb - 1) / cb);
-      block_level_kernel<T, cb><<<grid, threads, sizeof(T) * 3 * HALO * cb, st>>>(a, mode, tm);
-    }
+    dim3 grid(tiles, (a.ncol + cb - 1) / cb);
+    const size_t smem = sizeof(T) * 3 * HALO * cb;
+    block_level_kernel<T, cb><<<grid, threads, smem, st>>>(a, mode, tm);
     TF_LAUNCH_CHECK("block_level_kernel");
   }
 }
