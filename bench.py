@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--precision", default="float32")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -130,6 +131,12 @@ def ours(args):
     moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
     moduli = torch.as_tensor(moduli_host, device=device)
     groups = model.groups()
+    tuned, tuning = None, None
+    if not args.no_autotune:
+        # measured smoother choice (outside the timed region); every candidate solves to the same tolerance
+        from deep_frame_b200.autotune import tune_smoother
+        tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli)
+        mg = system._multigrid()
     # shard the columns of every fixture group across ranks (no collective inside the solve)
     shards = []
     for key, ks, forces in groups:
@@ -204,7 +211,9 @@ def ours(args):
     result = {"ms": ms, "launches_per_step": launches / args.steps, "breakdown": breakdown, "profiled_step_ms": profiled_step_ms,
               "iterations_max": iters, "clocks": clocks.summary(), "world": world, "rank": rank,
               "columns": [len(ks) for _, ks, _ in shards], "ndof": system.ndof, "levels": reports[-1]["levels"],
-              "coarsest_dofs": reports[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in reports)}
+              "coarsest_dofs": reports[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in reports),
+              "smoother": {k: v for k, v in (tuned or mg.settings).items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps")},
+              "tuning": tuning}
     # roofline of the dominant kernel class: the finest-level operator (fine_work = V-cycle smoothing at the work precision)
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     nodes = int(np.prod(np.asarray(mg.padded) + 1))
@@ -333,7 +342,9 @@ def main():
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
                        "outer": "fp64 PCG", "vcycle": args.precision, "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
-                       "pcg_iterations": result["iterations_max"], "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
+                       "pcg_iterations": result["iterations_max"], "smoother": result["smoother"],
+                       "smoother_choice": "autotuned (fastest of 5 schedules, all to the same tolerance)" if result["tuning"] else "reference default",
+                       "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
                        "parallelism": f"rhs-sharded x{result['world']}"},
             "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),
             "roofline": roof, "cpu_baseline": cpu, "breakdown_ms": result["breakdown"], "converged": result["converged"]}

@@ -1,0 +1,62 @@
+"""Measured choice of the V-cycle smoother for a given problem.
+
+The smoother schedule (Chebyshev degree, growth of the sweep count per level,
+or damped Jacobi) changes the cost of a V-cycle and the number of PCG
+iterations, never the converged answer: every candidate solves to the same
+recomputed true relative residual.  ``tune_smoother`` times one full solve of
+every fixture group per candidate on the device and returns the fastest.
+"""
+from time import perf_counter
+
+CANDIDATES = (
+    {"smoother": "chebyshev", "chebyshev_degree": 3, "growth": 2.0},   # the reference's MULTIGRID default
+    {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 2.0},
+    {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5},
+    {"smoother": "chebyshev", "chebyshev_degree": 3, "growth": 1.0},
+    {"smoother": "jacobi", "sweeps": 2, "growth": 2.0},
+)
+
+
+def tune_smoother(system, groups, moduli, base=None, candidates=CANDIDATES, repeats=2):
+    """groups: [(key, forces [R, ndof] CUDA tensor)]; moduli: CUDA float64 tensor.
+
+    Rebuilds ``system.multigrid`` for every candidate; leaves the fastest in place
+    and returns (settings, timings)."""
+    import torch
+    from .topology_multigrid import GeometricMultigrid
+    base = dict(base or system.multigrid_settings or {})
+    timings = []
+    best = None
+    for cand in candidates:
+        settings = {**base, **cand}
+        mg = GeometricMultigrid(system.shape, system.spacing, system.ke, settings, system.me)
+        seconds, iterations, ok = None, [], True
+        for rep in range(repeats + 1):
+            torch.cuda.synchronize()
+            t0 = perf_counter()
+            mg.update_device(moduli)
+            its = []
+            for key, forces in groups:
+                part = system.groups[key][0][1]
+                _, report = mg.solve_device(key, part["fixed"], forces)
+                ok &= report["converged"]
+                its.append(max(report["iterations"]))
+            torch.cuda.synchronize()
+            if rep:   # the first pass builds buffers
+                dt = perf_counter() - t0
+                seconds = dt if seconds is None else min(seconds, dt)
+                iterations = its
+        timings.append({"settings": cand, "seconds": seconds, "iterations": iterations, "converged": bool(ok)})
+        if ok and (best is None or seconds < best[0]):
+            if best is not None:
+                best[2].close()
+            best = (seconds, settings, mg)
+        else:
+            mg.close()
+    if best is None:
+        raise RuntimeError("no smoother candidate converged")
+    if system.multigrid is not None and system.multigrid is not best[2]:
+        system.multigrid.close()
+    system.multigrid = best[2]
+    system.multigrid_settings = best[1]
+    return best[1], timings
