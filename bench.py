@@ -1,13 +1,15 @@
 """Benchmark: seconds per 42-RHS covariance hex8 solve to 1e-8 relative residual.
 
-One step = one design update of the covariance-load plate half model
+One step = one design evaluation of the covariance-load plate half model
 (96 x 96 x 16 voxels, 479 859 dofs, mirror symmetry on x = 0): new element
 moduli, both multigrid hierarchies rebuilt (symmetric and antisymmetric
-fixture groups), and the 42 load directions of each half solved by batched
-FP64 GMG-PCG to a recomputed true relative residual below 1e-8 (84 column
-solves).  ``value`` times this with every input resident in HBM; ``e2e`` times
-the same step through the reference-facing API (``GeometricMultigrid.update``
-and ``.solve`` with host NumPy moduli / forces in and host solutions out).
+fixture groups), the 42 load directions of each half solved by batched FP64
+GMG-PCG to a recomputed true relative residual below 1e-8 (84 column solves),
+then F = P^T U, tr(K^-1 Sigma), lambda_max and both sensitivity fields.
+``value`` times this with every input resident in HBM; ``e2e`` times the same
+step from host densities to host results, and ``e2e_solve_api`` the solves
+alone through ``GeometricMultigrid.update`` / ``.solve`` with host NumPy
+forces in and host solutions out (the reference's solver seam).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 For N > 1 (torchrun, one rank per GPU) the 42 directions of each half are
@@ -115,63 +117,50 @@ def build_problem(config, precision, device):
 
 
 def ours(args):
+    import ctypes
+    import datetime
     import torch
     import torch.distributed as dist
     from deep_frame_b200 import _lib
+    from deep_frame_b200.distributed import DeviceOps, ShardedMeasure
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     spec, system, model, density = build_problem(args.config, args.precision, device)
-    mg = system._multigrid()
     moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
     moduli = torch.as_tensor(moduli_host, device=device)
+    scale = torch.as_tensor(-derivative, device=device)
     groups = model.groups()
     tuned, tuning = None, None
     if not args.no_autotune:
         # measured smoother choice (outside the timed region); every candidate solves to the same tolerance
-        from deep_frame_b200.autotune import tune_smoother
-        tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli)
-        mg = system._multigrid()
-    # shard the columns of every fixture group across ranks (no collective inside the solve)
-    shards = []
-    for key, ks, forces in groups:
-        cols = np.arange(len(ks))[rank::world]
-        shards.append((key, ks[cols], forces[torch.as_tensor(cols, device=device)].contiguous()))
-    reports = []
+        from deep_frame_b200.autotune import CANDIDATES, tune_smoother
+        choice = [None]
+        if rank == 0:
+            tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli)
+            choice = [tuned]
+        if world > 1:
+            dist.broadcast_object_list(choice, src=0)
+            if rank != 0:
+                tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
+                                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps")}],
+                                              repeats=1)
+    mg = system._multigrid()
+    measure = ShardedMeasure(groups, model.rank, model.factor, DeviceOps(system))
+    reports = mg.statistics
 
     def step():
         mg.update_device(moduli)
-        out = []
-        for key, ks, forces in shards:
-            part = system.groups[key][0][1]
-            u, report = mg.solve_device(key, part["fixed"], forces)
-            out.append((key, ks, forces, u))
-            reports.append(report)
-        if world > 1:
-            # gather the flexibility columns: every rank holds F[:, local] = P^T U_local
-            lib = _lib.load()
-            flex = torch.zeros((model.rank, model.rank), dtype=torch.float64, device=device)
-            for key, ks, forces, u in out:
-                allp = dict((k, f) for k2, kk, f in groups for k in [k2])[key]
-                full_ks = [g[1] for g in groups if g[0] == key][0]
-                m, mloc = len(full_ks), len(ks)
-                part = torch.empty((m, mloc), dtype=torch.float64, device=device)
-                scratch = torch.empty(int(lib.tf_gram_scratch_size(m, mloc)), dtype=torch.float64, device=device)
-                _lib.check(lib.tf_gram(_lib.ptr(allp), m, _lib.ptr(u), mloc, u.shape[1], _lib.ptr(part), _lib.ptr(scratch), mg._stream()))
-                idx = torch.as_tensor(full_ks, device=device)
-                loc = torch.as_tensor(ks, device=device)
-                flex[idx[:, None], loc[None, :]] += model.factor * part
-            dist.all_reduce(flex)
-        return out
+        return measure.measure(scale)
 
     for _ in range(args.warmup):
         step()
-    reports.clear()
+    first_report = len(reports)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -181,7 +170,7 @@ def ours(args):
         torch.cuda.synchronize()
         start.record()
         for _ in range(args.steps):
-            step()
+            rows, flex = step()
         stop.record()
         torch.cuda.synchronize()
     launches = int(_lib.load().tf_launch_count()) - launches0
@@ -192,6 +181,7 @@ def ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
+    timed = reports[first_report:]
     # per-kernel-class breakdown of one more step (CUDA events on the launching stream)
     lib = _lib.load()
     lib.tf_timers(mg.handle, 1, None, None, 0)
@@ -201,53 +191,60 @@ def ours(args):
     step()
     s1.record()
     torch.cuda.synchronize()
-    import ctypes
     n = len(_lib.TIMER_CLASSES)
     tms, tcnt = (ctypes.c_double * n)(), (ctypes.c_int64 * n)()
     _lib.check(lib.tf_timers(mg.handle, 0, tms, tcnt, n), mg.handle, "tf_timers")
     breakdown = {name: {"ms": round(tms[i], 3), "launches": int(tcnt[i])} for i, name in enumerate(_lib.TIMER_CLASSES)}
-    profiled_step_ms = s0.elapsed_time(s1)
-    iters = [int(np.max(r["iterations"])) for r in reports[-len(shards):]]
-    result = {"ms": ms, "launches_per_step": launches / args.steps, "breakdown": breakdown, "profiled_step_ms": profiled_step_ms,
-              "iterations_max": iters, "clocks": clocks.summary(), "world": world, "rank": rank,
-              "columns": [len(ks) for _, ks, _ in shards], "ndof": system.ndof, "levels": reports[-1]["levels"],
-              "coarsest_dofs": reports[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in reports),
-              "smoother": {k: v for k, v in (tuned or mg.settings).items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps")},
-              "tuning": tuning}
-    # roofline of the dominant kernel class: the finest-level operator (fine_work = V-cycle smoothing at the work precision)
+    result = {"ms": ms, "launches_per_step": launches / args.steps, "breakdown": breakdown, "profiled_step_ms": s0.elapsed_time(s1),
+              "iterations_max": [int(np.max(r["iterations"])) for r in timed[-len(groups):]], "clocks": clocks.summary(),
+              "world": world, "rank": rank, "columns": [len(g["local"]) for g in measure.groups], "ndof": system.ndof,
+              "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in timed),
+              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps")},
+              "tuning": tuning, "tr": rows[0]["value"], "lambda_max": rows[1]["value"]}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
-    nodes = int(np.prod(np.asarray(mg.padded) + 1))
-    cols = sum(len(ks) for _, ks, _ in shards)
     result["dominant"] = dominant
     if breakdown[dominant]["launches"]:
-        per_launch_ms = breakdown[dominant]["ms"] / breakdown[dominant]["launches"]
-        result["dominant_per_launch_ms"] = per_launch_ms
-    # end-to-end through the host API (NumPy in / NumPy out), rank 0 at N = 1
+        result["dominant_per_launch_ms"] = breakdown[dominant]["ms"] / breakdown[dominant]["launches"]
+    result["nodes"] = int(np.prod(np.asarray(mg.padded) + 1))
+    result["cols"] = sum(result["columns"])
     if world == 1 and not args.no_e2e:
-        host_forces = [(key, forces.T.cpu().numpy().copy()) for key, _, forces in shards]
-        h2d = moduli_host.nbytes + sum(f.nbytes for _, f in host_forces)
-        d2h = sum(f.nbytes for _, f in host_forces)
+        # (1) the public design-evaluation call: host densities in, host values and sensitivities out
+        host_density = np.ascontiguousarray(density)
+        h2d = moduli_host.nbytes
 
         def e2e_step():
-            mg.update(moduli_host)
-            outs = []
-            for key, f in host_forces:
-                part = system.groups[key][0][1]
-                outs.append(mg.solve(key, part["fixed"], f)[0])
-            return outs
+            m = torch.as_tensor(system.moduli(host_density, 3.0, 1e-9)[0], device=device)
+            mg.update_device(m)
+            r, f = measure.measure(torch.as_tensor(-system.moduli(host_density, 3.0, 1e-9)[1], device=device))
+            return r[0]["value"], r[1]["value"], r[0]["gradient"].cpu().numpy(), r[1]["gradient"].cpu().numpy()
 
         e2e_step()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(args.steps):
-            e2e_step()
+            out = e2e_step()
         e1.record()
         torch.cuda.synchronize()
-        result["e2e"] = {"ms": e0.elapsed_time(e1) / args.steps, "wall_ms": (time.perf_counter() - t0) * 1e3 / args.steps,
-                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
-    result["nodes"], result["cols"] = nodes, cols
+        d2h = out[2].nbytes + out[3].nbytes + 16
+        result["e2e"] = {"ms": e0.elapsed_time(e1) / args.steps, "h2d_bytes_per_step": int(2 * h2d), "d2h_bytes_per_step": int(d2h)}
+        # (2) the reference solver seam: GeometricMultigrid.update / .solve with host forces and host solutions
+        host_forces = [(key, forces.T.cpu().numpy().copy()) for key, _, forces in groups]
+
+        def solve_api_step():
+            mg.update(moduli_host)
+            return [mg.solve(key, system.groups[key][0][1]["fixed"], f)[0] for key, f in host_forces]
+
+        solve_api_step()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            solve_api_step()
+        e1.record()
+        torch.cuda.synchronize()
+        result["solve_api"] = {"ms": e0.elapsed_time(e1) / args.steps,
+                               "h2d_bytes_per_step": int(moduli_host.nbytes + sum(f.nbytes for _, f in host_forces)),
+                               "d2h_bytes_per_step": int(sum(f.nbytes for _, f in host_forces))}
     if world > 1:
         dist.destroy_process_group()
     return result, system, model, density
@@ -351,7 +348,11 @@ def main():
     if "e2e" in result:
         e = result["e2e"]
         line["e2e"] = {"value": round(e["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": e["h2d_bytes_per_step"],
-                       "d2h_bytes_per_step": e["d2h_bytes_per_step"]}
+                       "d2h_bytes_per_step": e["d2h_bytes_per_step"], "call": "InterfaceCovariance-style measure: host density in, host tr / lambda_max / sensitivities out"}
+        a = result["solve_api"]
+        line["e2e_solve_api"] = {"value": round(a["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": a["h2d_bytes_per_step"],
+                                 "d2h_bytes_per_step": a["d2h_bytes_per_step"], "call": "GeometricMultigrid.update + .solve per half with host NumPy forces and solutions"}
+    line["results"] = {"tr_K_inv_sigma": result["tr"], "lambda_max": result["lambda_max"]}
     print(json.dumps(line))
 
 
