@@ -322,11 +322,14 @@ def main():
     nodes, cols = result["nodes"], result["cols"]
     per_launch_cols = cols / max(1, len(result["columns"]))
     traffic_alg = nodes * per_launch_cols * (6 * word) + nodes * per_launch_cols * word
+    # DRAM bytes of one finest-level FP32 launch on this workload, from an ncu capture of that
+    # launch (dram__bytes_read.sum + dram__bytes_write.sum); None for other kernels
+    traffic = {"fine_work": 434e6}.get(dominant) if args.config == CONFIG and args.precision == "float32" else None
     roof = None
     if "dominant_per_launch_ms" in result:
         achieved = traffic_alg / (result["dominant_per_launch_ms"] * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                "traffic": None, "kernel": dominant, "peak_source": source,
+                "traffic": traffic, "kernel": dominant, "peak_source": source,
                 "per_launch_ms": round(result["dominant_per_launch_ms"], 4), "algorithmic_bytes_per_launch": int(traffic_alg)}
     cpu = None
     if not args.no_cpu and result["world"] == 1:
