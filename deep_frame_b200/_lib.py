@@ -20,7 +20,8 @@ SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set
            "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
 SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_destroy",
-            "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error", "tf_simp")
+            "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error", "tf_simp",
+            "tf_chol_create", "tf_chol_factor_csr", "tf_chol_solve", "tf_chol_destroy", "tf_chol_last_error")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
 
 
@@ -102,11 +103,16 @@ def load():
             "tf_mma_destroy": [P],
             "tf_mma_last_error": [P],
             "tf_simp": [P, I64, D, D, D, P, P, P, P, P],
+            "tf_chol_create": [I64, ctypes.POINTER(P)],
+            "tf_chol_factor_csr": [P, P, P, P, P],
+            "tf_chol_solve": [P, P, I32, P, P],
+            "tf_chol_destroy": [P],
+            "tf_chol_last_error": [P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
             fn.argtypes = args
-            fn.restype = {"tf_last_error": ctypes.c_char_p, "tf_filter_last_error": ctypes.c_char_p, "tf_mma_last_error": ctypes.c_char_p,
+            fn.restype = {"tf_last_error": ctypes.c_char_p, "tf_filter_last_error": ctypes.c_char_p, "tf_mma_last_error": ctypes.c_char_p, "tf_chol_last_error": ctypes.c_char_p,
                           "tf_gram_scratch_size": ctypes.c_int64, "tf_launch_count": ctypes.c_int64}.get(name, ctypes.c_int)
         _lib = lib
         return lib

@@ -301,3 +301,115 @@ void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, 
 }
 
 }  // namespace tfb
+
+// ---------------------------------------------------------------------------
+// Dense FP64 direct solver of a small sparse SPD system (the drop-in for the
+// reference's CudaDirectSolver, deep_frame/topology_optimization.py:80-244):
+// the CSR matrix is scattered into a dense n x n array, symmetrised, factored
+// (A = L L^T), and L is inverted once; each solve is x = L^-T (L^-1 b).
+// ---------------------------------------------------------------------------
+#include <string>
+#include "tf_b200.h"
+
+namespace {
+__global__ void csr_to_dense_kernel(int n, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                    const double* __restrict__ data, double* __restrict__ A) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double* row = A + (long long)i * n;
+    for (int k = indptr[i]; k < indptr[i + 1]; ++k) {
+      const int j = indices[k];
+      if ((unsigned)j < (unsigned)n) row[j] = data[k];
+    }
+  }
+}
+}  // namespace
+
+struct tf_chol {
+  int n = 0;
+  tfb::DevBuf A, X, tmp, info;
+  bool factored = false;
+  std::string err;
+};
+
+namespace {
+template <typename F>
+int chol_guard(tf_chol* h, F&& f) {
+  try {
+    f();
+    return tfb::TF_OK;
+  } catch (const tfb::Error& e) {
+    if (h) h->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    if (h) h->err = e.what();
+    return tfb::TF_INTERNAL;
+  }
+}
+constexpr int64_t CHOL_MAX_N = 32768;
+}  // namespace
+
+extern "C" int tf_chol_create(int64_t n, tf_chol** out) {
+  if (!out) return tfb::TF_INVALID;
+  *out = nullptr;
+  tf_chol* h = new tf_chol();
+  const int rc = chol_guard(h, [&] {
+    tfb::require(n >= 1 && n <= CHOL_MAX_N, "the dense direct solver handles 1 to 32768 unknowns");
+    h->n = static_cast<int>(n);
+    h->A.alloc(sizeof(double) * n * n);
+    h->X.alloc(sizeof(double) * n * n);
+    h->info.alloc(sizeof(int));
+  });
+  if (rc != tfb::TF_OK) {
+    tfb::record_unhandled_error(h->err);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return tfb::TF_OK;
+}
+
+extern "C" int tf_chol_factor_csr(tf_chol* h, const int32_t* indptr_dev, const int32_t* indices_dev, const double* data_dev,
+                                  void* stream) {
+  if (!h) return tfb::TF_INVALID;
+  return chol_guard(h, [&] {
+    tfb::require(indptr_dev && indices_dev && data_dev, "tf_chol_factor_csr: NULL argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int n = h->n;
+    h->factored = false;
+    TF_CUDA_CHECK(cudaMemsetAsync(h->A.p, 0, h->A.bytes, s));
+    csr_to_dense_kernel<<<tfb::grid_for(n, 128), 128, 0, s>>>(n, indptr_dev, indices_dev, data_dev, h->A.as<double>());
+    TF_LAUNCH_CHECK("csr_to_dense_kernel");
+    tfb::dense_symmetrize(h->A.as<double>(), n, s);
+    TF_CUDA_CHECK(cudaMemsetAsync(h->info.p, 0, sizeof(int), s));
+    tfb::dense_cholesky(h->A.as<double>(), n, h->info.as<int>(), s);
+    int info = 0;
+    TF_CUDA_CHECK(cudaMemcpyAsync(&info, h->info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (info != 0) throw tfb::Error(tfb::TF_NUMERIC, "matrix is not positive definite (pivot " + std::to_string(info) + ")");
+    tfb::dense_trinv(h->A.as<double>(), h->X.as<double>(), n, s);
+    h->factored = true;
+  });
+}
+
+extern "C" int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, double* x_dev, void* stream) {
+  if (!h) return tfb::TF_INVALID;
+  return chol_guard(h, [&] {
+    tfb::require(h->factored, "tf_chol_solve: no factorisation (call tf_chol_factor_csr first)");
+    tfb::require(nrhs >= 1 && b_dev && x_dev, "tf_chol_solve: invalid right-hand sides");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t need = sizeof(double) * (size_t)h->n * nrhs;
+    if (h->tmp.bytes < need) h->tmp.alloc(need);
+    tfb::dense_trimul(h->X.as<double>(), b_dev, h->tmp.as<double>(), h->n, nrhs, 0, nullptr, s);
+    tfb::dense_trimul(h->X.as<double>(), h->tmp.as<double>(), x_dev, h->n, nrhs, 1, nullptr, s);
+  });
+}
+
+extern "C" int tf_chol_destroy(tf_chol* h) {
+  if (h) {
+    cudaDeviceSynchronize();
+    delete h;
+  }
+  return tfb::TF_OK;
+}
+
+extern "C" const char* tf_chol_last_error(const tf_chol* h) { return h ? h->err.c_str() : ""; }

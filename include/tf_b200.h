@@ -218,6 +218,20 @@ TF_API int tf_mma_step(tf_mma* h, int32_t iteration, const double* xval, const d
 TF_API int tf_mma_destroy(tf_mma* h);
 TF_API const char* tf_mma_last_error(const tf_mma* h);
 
+/* ------------------------------------------------------------------------------------
+ * Dense FP64 direct solver of a small SPD system (CudaDirectSolver,
+ * deep_frame/topology_optimization.py:80-244; the reference factors with cuDSS).
+ * n <= 32768; the matrix arrives as device CSR (int32 indptr [n+1], indices, FP64 data)
+ * and is symmetrised; right-hand sides and solutions are [nrhs][n] device blocks.
+ * ------------------------------------------------------------------------------------ */
+typedef struct tf_chol tf_chol;
+TF_API int tf_chol_create(int64_t n, tf_chol** out);
+TF_API int tf_chol_factor_csr(tf_chol* h, const int32_t* indptr_dev, const int32_t* indices_dev, const double* data_dev,
+                              void* stream);
+TF_API int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, double* x_dev, void* stream);
+TF_API int tf_chol_destroy(tf_chol* h);
+TF_API const char* tf_chol_last_error(const tf_chol* h);
+
 /* CUDA-event timing of the kernel classes this handle launches, recorded on the launching
  * stream: 0 FP64 finest operator of the PCG, 1 finest-level smoothing / residual in the work
  * precision, 2 Galerkin-level operators, 3 restriction + prolongation, 4 PCG vector kernels,
@@ -235,7 +249,7 @@ TF_API int64_t tf_launch_count(void);
 TF_API int tf_destroy(tf_handle* h);
 
 /* Message of the last failed call on `h` (or, with h NULL, of the last failed tf_create,
- * tf_filter_create, tf_mma_create or tf_gram_static on this thread). */
+ * tf_filter_create, tf_mma_create, tf_chol_create or tf_gram_static on this thread). */
 TF_API const char* tf_last_error(const tf_handle* h);
 
 #ifdef __cplusplus

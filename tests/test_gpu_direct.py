@@ -1,0 +1,80 @@
+"""Dense device direct solver (CudaDirectSolver drop-in) and the HexElasticity solve paths.
+
+Mirrors the reference's cuDSS tests (tests/test_topology_optimization.py:451-553):
+direct = CPU sparse solve, symbolic reuse, invalid input, cleanup; and the
+multigrid HexElasticity solve = direct solve on compliance, sensitivities and max
+displacement (tests/test_topology_multigrid.py:74-86, rel 1e-7).
+"""
+import numpy as np
+import pytest
+from scipy.sparse.linalg import spsolve
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(shape=(12, 6, 6), seed=0, solver="cuda_cudss", multigrid=None):
+    from deep_frame_b200 import problems
+    from deep_frame_b200.elasticity import HexElasticity
+    domain, density = problems.cantilever(shape, seed)
+    return HexElasticity(domain, linear_solver=solver, multigrid=multigrid), density
+
+
+def test_direct_solver_matches_sparse_solve_and_reuses_structure(cuda):
+    from deep_frame_b200.direct import CudaDirectSolver
+    system, density = _system()
+    moduli, _ = system.moduli(density, 3.0, 1e-9)
+    full = system.matrix(1e-9 + (1 - 1e-9) * density ** 3)
+    free = next(iter(system.groups.values()))[0][1]["free"]
+    reduced = full[free][:, free].tocsc()
+    rhs = np.random.default_rng(1).normal(size=(len(free), 3))
+    solver = CudaDirectSolver(reduced, rhs)
+    x = solver.solve(reduced, rhs)
+    want = spsolve(reduced, rhs)
+    assert np.linalg.norm(x - want) < 1e-9 * np.linalg.norm(want)
+    x2 = solver.substitute(2 * rhs)
+    assert np.linalg.norm(x2 - 2 * want) < 1e-9 * np.linalg.norm(want)
+    scaled = reduced * 3.0
+    assert solver.same_structure(scaled)
+    assert np.linalg.norm(solver.solve(scaled, rhs) - want / 3) < 1e-9 * np.linalg.norm(want)
+    with pytest.raises(ValueError):
+        solver.solve(reduced[:-1, :-1], rhs[:-1])
+    with pytest.raises(ValueError):
+        solver.substitute(rhs[:, :2])
+    assert solver.close() == [] and solver.close() == []
+    with pytest.raises(RuntimeError):
+        solver.solve(reduced, rhs)
+
+
+def test_direct_solver_rejects_indefinite_matrix(cuda):
+    from scipy.sparse import csr_matrix
+    from deep_frame_b200.direct import CudaDirectSolver
+    m = csr_matrix(np.array([[1.0, 2.0], [2.0, 1.0]]))
+    solver = CudaDirectSolver(m, np.ones((2, 1)))
+    with pytest.raises(RuntimeError, match="positive definite"):
+        solver.solve(m, np.ones((2, 1)))
+    solver.close()
+
+
+def test_multigrid_system_solve_matches_direct_system_solve(cuda):
+    direct, density = _system((16, 8, 8), 3)
+    mg, _ = _system((16, 8, 8), 3, "multigrid", {"tolerance": 1e-12, "coarsest_dofs": 200, "precision": "float64"})
+    a = direct.solve(density, 3.0, 1e-9, metrics=True)["tip"]
+    b = mg.solve(density, 3.0, 1e-9, metrics=True)["tip"]
+    assert b["compliance_n_mm"] == pytest.approx(a["compliance_n_mm"], rel=1e-7)
+    assert np.linalg.norm(b["derivative"] - a["derivative"]) <= 1e-7 * np.linalg.norm(a["derivative"])
+    assert b["max_displacement_mm"] == pytest.approx(a["max_displacement_mm"], rel=1e-7)
+    assert direct.close() == [] and mg.close() == []
+
+
+def test_system_solve_matches_reference_superlu_golden(cuda):
+    """Config-1 cantilever (48 x 24 x 24): compliance 1e-6 and sensitivities 1e-5 vs the reference's SuperLU."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "cantilever_48x24x24.npz")
+    system, _ = _system((48, 24, 24), 0, "multigrid", {"precision": "float64", "smoother": "jacobi", "sweeps": 2,
+                                                      "coarsest_dofs": 400, "tolerance": 1e-10})
+    result = system.solve(g["density"], 3.0, 1e-9, metrics=True)["tip"]
+    assert system.multigrid.statistics[-1]["levels"] == 4
+    assert result["compliance_n_mm"] == pytest.approx(float(g["compliance"]), rel=1e-6)
+    assert np.linalg.norm(result["derivative"] - g["derivative"]) < 1e-5 * np.linalg.norm(g["derivative"])
+    assert result["max_displacement_mm"] == pytest.approx(float(g["max_displacement"]), rel=1e-6)
+    system.close()
