@@ -17,9 +17,10 @@ COARSE = {"galerkin": 0, "rediscretize": 1}
 
 # every symbol include/tf_b200.h declares (checked by the CPU test suite)
 SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set_bc", "tf_prepare", "tf_precondition",
-           "tf_solve", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
+           "tf_solve", "tf_solve_guess", "tf_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
-SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_destroy",
+SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_volume", "tf_oc_update",
+            "tf_filter_destroy",
             "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error", "tf_simp",
             "tf_chol_create", "tf_chol_factor_csr", "tf_chol_solve", "tf_chol_destroy", "tf_chol_last_error")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
@@ -52,6 +53,11 @@ class TfMmaSettings(ctypes.Structure):
     _fields_ = [(name, ctypes.c_double) for name in ("move", "asyinit", "asydecr", "asyincr", "asymin", "asymax", "raa0", "albefa", "epsimin")]
 
 
+class TfOcReport(ctypes.Structure):
+    _fields_ = [("multiplier", ctypes.c_double), ("lower", ctypes.c_double), ("volume", ctypes.c_double),
+                ("evaluations", ctypes.c_int32), ("lowest", ctypes.c_int32)]
+
+
 class TfError(RuntimeError):
     def __init__(self, status, message):
         super().__init__(message)
@@ -82,6 +88,7 @@ def load():
             "tf_prepare": [P, U64, ctypes.POINTER(TfReport), P],
             "tf_precondition": [P, U64, P, I32, P, P],
             "tf_solve": [P, U64, P, I32, P, ctypes.POINTER(TfReport), P],
+            "tf_solve_guess": [P, U64, P, I32, P, ctypes.POINTER(TfReport), P],
             "tf_apply": [P, U64, I32, P, I32, P, P],
             "tf_element_energy": [P, P, I32, P, I32, P, P, P, I32, I32, P],
             "tf_gram": [P, I32, P, I32, I64, P, P, P],
@@ -95,6 +102,8 @@ def load():
             "tf_filter_apply": [P, P, P, P, I32, P],
             "tf_filter_sums": [P, P, P],
             "tf_filter_project": [P, P, D, D, I32, P, P, P],
+            "tf_filter_volume": [P, P, P, D, D, I32, P, P],
+            "tf_oc_update": [P, P, P, P, P, D, D, D, D, D, I32, P, ctypes.POINTER(TfOcReport), P],
             "tf_filter_destroy": [P],
             "tf_filter_last_error": [P],
             "tf_mma_create": [I32, I64, ctypes.POINTER(P)],

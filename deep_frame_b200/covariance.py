@@ -99,11 +99,13 @@ class InterfaceCovariance:
         scale = torch.as_tensor(-derivative, dtype=torch.float64, device=mg.device)
         return self.measure_from(self.solve_all(), scale, gradients)
 
-    def solve_all(self):
+    def solve_all(self, initial=None):
+        """Solve every fixture group; ``initial`` maps a group key to a warm-start guess."""
         system = self.system
         solved = []
         for key, ks, forces in self.groups():
-            u, report = system.solve_group_device(key, forces)
+            guess = None if initial is None else initial.get(key)
+            u, report = system.solve_group_device(key, forces, initial=guess)
             solved.append((key, ks, forces, u, report))
         return solved
 

@@ -1,70 +1,9 @@
 // Hierarchy set-up kernels and the device-side PCG vector kernels.
 #pragma once
 #include "tf_kernels.cuh"
+#include "tf_reduce.cuh"
 
 namespace tfb {
-
-constexpr int RED_THREADS = 256;
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-
-// Block-wide reduction of two values (op 0 = sum, 1 = max); result valid in thread 0.
-template <int OP0, int OP1>
-__device__ __forceinline__ void block_reduce2(double& a, double& b) {
-  __shared__ double sa[RED_THREADS / 32], sb[RED_THREADS / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  a = OP0 ? warp_max(a) : warp_sum(a);
-  b = OP1 ? warp_max(b) : warp_sum(b);
-  if (lane == 0) { sa[warp] = a; sb[warp] = b; }
-  __syncthreads();
-  if (warp == 0) {
-    a = lane < RED_THREADS / 32 ? sa[lane] : 0.0;
-    b = lane < RED_THREADS / 32 ? sb[lane] : 0.0;
-    a = OP0 ? warp_max(a) : warp_sum(a);
-    b = OP1 ? warp_max(b) : warp_sum(b);
-  }
-  __syncthreads();
-}
-
-// Deterministic cross-block combine: every block stores its partial; the last
-// block of the column sums the partials in block order.  Returns true in
-// thread 0 of the last block, with the totals in a, b.
-template <int OP0, int OP1>
-__device__ __forceinline__ bool last_block_combine(double& a, double& b, double* partial, unsigned* count, int col) {
-  __shared__ bool is_last;
-  if (threadIdx.x == 0) {
-    double* p = partial + 2 * ((long long)col * gridDim.x + blockIdx.x);
-    p[0] = a;
-    p[1] = b;
-    __threadfence();
-    const unsigned t = atomicAdd(&count[col], 1u);
-    is_last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!is_last) return false;
-  if (threadIdx.x != 0) return false;
-  __threadfence();
-  double ta = OP0 ? 0.0 : 0.0, tb = 0.0;
-  const double* p = partial + 2 * (long long)col * gridDim.x;
-  for (unsigned q = 0; q < gridDim.x; ++q) {
-    const double pa = __ldcg(p + 2 * q), pb = __ldcg(p + 2 * q + 1);
-    ta = OP0 ? fmax(ta, pa) : ta + pa;
-    tb = OP1 ? fmax(tb, pb) : tb + pb;
-  }
-  count[col] = 0;
-  a = ta;
-  b = tb;
-  return true;
-}
 
 struct PcgState {
   double* bnorm;

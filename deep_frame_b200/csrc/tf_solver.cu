@@ -1096,9 +1096,11 @@ extern "C" int tf_set_bc(tf_handle* h, uint64_t key, const int64_t* fixed, int64
   });
 }
 
-extern "C" int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
-                        void* stream) {
-  if (!h) return TF_INVALID;
+namespace {
+// Shared body of tf_solve (start from zero) and tf_solve_guess (start from u_dev, the reference's
+// _pcg(..., initial), topology_multigrid.py:407-417).
+int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report, void* stream,
+               bool warm) {
   return guard(h, [&] {
     auto t0 = std::chrono::steady_clock::now();
     require(nrhs >= 0, "nrhs must be non-negative");
@@ -1145,8 +1147,14 @@ extern "C" int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t
       pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(f_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
                                                                 h->vb.as<double>(), h->colmap.as<int>());
       TF_LAUNCH_CHECK("pad_kernel");
+      if (warm) {
+        // the caller's guess, masked like the forces; pcg then starts from r = b - A x
+        pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(u_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
+                                                                  h->vx.as<double>(), h->colmap.as<int>());
+        TF_LAUNCH_CHECK("pad_kernel");
+      }
       std::vector<int> run(nc, 1);
-      PcgResult r = work_is_double(h) ? pcg<double>(h, hy, nc, run, false, s) : pcg<float>(h, hy, nc, run, false, s);
+      PcgResult r = work_is_double(h) ? pcg<double>(h, hy, nc, run, warm, s) : pcg<float>(h, hy, nc, run, warm, s);
       history.insert(history.end(), r.history.begin(), r.history.end());
       steps += r.steps;
       for (int attempt = 0; attempt < h->s.retries; ++attempt) {
@@ -1207,6 +1215,19 @@ extern "C" int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t
     }
     hy.setup_reported = true;
   });
+}
+}  // namespace
+
+extern "C" int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
+                        void* stream) {
+  if (!h) return TF_INVALID;
+  return solve_impl(h, key, f_dev, nrhs, u_dev, report, stream, false);
+}
+
+extern "C" int tf_solve_guess(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
+                              void* stream) {
+  if (!h) return TF_INVALID;
+  return solve_impl(h, key, f_dev, nrhs, u_dev, report, stream, true);
 }
 
 namespace {

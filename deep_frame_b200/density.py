@@ -5,10 +5,12 @@ Mirrors the reference's ``ConeFilter`` / ``cone_filter`` / ``DensityMap``
 max(r - |offset * h|, 0) between allowed cells, row sums with 1 on forbidden
 cells, ``filtered``, ``project`` (single and robust tanh projections),
 ``physical``, ``fields``, ``volume``, ``pullback`` and the bisection
-``initial`` design.  The convolution, its adjoint and the projection run in
-libtfb200.so; host-array methods keep the reference's NumPy signatures and the
-``*_device`` methods take and return CUDA tensors.  Corridor blends and
-prop-disc volume weights of the reference are not part of this build.
+``initial`` design, and the optimality-criteria update ``_oc_update``
+(:1197-1233).  The convolution, its adjoint, the projection, the fused volume
+and the whole OC multiplier search run in libtfb200.so; host-array methods keep
+the reference's NumPy signatures and the ``*_device`` methods take and return
+CUDA tensors.  Corridor blends and prop-disc volume weights of the reference
+are not part of this build.
 """
 import ctypes
 
@@ -57,13 +59,31 @@ class _Filter:
     def _check(self, status, what):
         if status:
             message = (self.lib.tf_filter_last_error(self.handle) or b"").decode()
-            raise (ValueError if status == 1 else _lib.TfError)(f"{what} failed: {message}")
+            if status == 1:
+                raise ValueError(f"{what} failed: {message}")
+            raise _lib.TfError(status, f"{what} failed: {message}")
 
     def apply(self, x, multiplier=None, adjoint=False, out=None):
         out = self.torch.empty_like(x) if out is None else out
         self._check(self.lib.tf_filter_apply(self.handle, _lib.ptr(x), _lib.ptr(multiplier), _lib.ptr(out), 1 if adjoint else 0,
                                              _lib.stream_of(self.device)), "tf_filter_apply")
         return out
+
+    def volume(self, design, beta, eta, robust=False, weights=None, out=None):
+        out = self.torch.empty(1, dtype=self.torch.float64, device=self.device) if out is None else out
+        self._check(self.lib.tf_filter_volume(self.handle, _lib.ptr(design), _lib.ptr(weights), float(beta), float(eta),
+                                              1 if robust else 0, _lib.ptr(out), _lib.stream_of(self.device)), "tf_filter_volume")
+        return out
+
+    def oc_update(self, design, objective_derivative, volume_derivative, target, minimum, move, beta, eta, robust, weights=None):
+        candidate = self.torch.empty_like(design)
+        report = _lib.TfOcReport()
+        self._check(self.lib.tf_oc_update(self.handle, _lib.ptr(design), _lib.ptr(objective_derivative), _lib.ptr(volume_derivative),
+                                          _lib.ptr(weights), float(target), float(minimum), float(move), float(beta), float(eta),
+                                          1 if robust else 0, _lib.ptr(candidate), ctypes.byref(report), _lib.stream_of(self.device)),
+                    "tf_oc_update")
+        return candidate, {"multiplier": report.multiplier, "lower": report.lower, "volume": report.volume,
+                           "evaluations": int(report.evaluations), "lowest": bool(report.lowest)}
 
     def project(self, filtered, beta, eta, robust=False, derivative=True):
         physical = self.torch.empty_like(filtered)
@@ -91,6 +111,8 @@ class DensityMap:
         import torch
         self.torch = torch
         self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.settings = settings
         if settings.get("corridor") is not None or settings.get("prop_discs") is not None:
             raise NotImplementedError("corridor blends and prop-disc volume weights are not part of this build")
@@ -123,6 +145,25 @@ class DensityMap:
     def pullback_device(self, sensitivity, projection_derivative):
         return self.filter.apply(sensitivity, projection_derivative, adjoint=True)
 
+    def fields_device(self, design):
+        filtered = self.filtered_device(design)
+        return {name: self.project_device(filtered, eta) for name, eta in self.thresholds.items()}, filtered
+
+    def volume_eta(self):
+        """Threshold of the volume field: dilated for the robust projection, else intermediate."""
+        return self.thresholds["dilated"] if self.robust else self.settings["projection_eta"]
+
+    def volume_device(self, design):
+        return float(self.filter.volume(design, self.beta, self.volume_eta(), self.robust).item())
+
+    def oc_update_device(self, design, objective_derivative, volume_derivative, target, move_limit):
+        """Device ``_oc_update``: (candidate tensor, search report)."""
+        for name, value in (("design", design), ("objective_derivative", objective_derivative), ("volume_derivative", volume_derivative)):
+            if value.dtype != self.torch.float64 or value.numel() != self.n or not value.is_contiguous() or value.device != self.device:
+                raise ValueError(f"{name} must be a contiguous float64 tensor of {self.n} cells on {self.device}")
+        return self.filter.oc_update(design, objective_derivative, volume_derivative, target,
+                                     self.settings["minimum_design_density"], move_limit, self.beta, self.volume_eta(), self.robust)
+
     # --------------------------------------------------------------- host --
     def _host(self, tensor):
         return tensor.cpu().numpy()
@@ -148,9 +189,10 @@ class DensityMap:
         return {name: self.project(filtered, eta) for name, eta in self.thresholds.items()}, filtered
 
     def volume(self, design):
-        if self.robust:
-            return float(np.sum(self.weights * self.project(self.filtered(design), self.thresholds["dilated"])[0]))
-        return float(np.sum(self.weights * self.physical(design)[0]))
+        design = np.asarray(design, dtype=float).ravel()
+        if design.size != self.n or not np.all(np.isfinite(design)) or np.any(design < 0) or np.any(design > 1):
+            raise ValueError("Design densities must be finite and within [0, 1]")
+        return self.volume_device(self._dev(design))
 
     def pullback(self, sensitivity, projection_derivative):
         return self._host(self.pullback_device(self._dev(sensitivity), self._dev(projection_derivative)))
@@ -175,3 +217,22 @@ class DensityMap:
 
     def close(self):
         self.filter.close()
+
+
+def _oc_update(design, objective_derivative, volume_derivative, mapping, target, settings, move_limit):
+    """The reference's ``_oc_update`` (topology_optimization.py:1197-1233) with NumPy arrays, run on the device.
+
+    ``settings["minimum_design_density"]`` must match the mapping's settings; errors raise RuntimeError
+    ("Invalid OC sensitivities" / "OC could not bracket the volume multiplier") as in the reference."""
+    if settings["minimum_design_density"] != mapping.settings["minimum_design_density"]:
+        mapping = _with_minimum(mapping, settings["minimum_design_density"])
+    candidate, _ = mapping.oc_update_device(mapping._dev(design), mapping._dev(objective_derivative), mapping._dev(volume_derivative),
+                                            target, move_limit)
+    return candidate.cpu().numpy()
+
+
+def _with_minimum(mapping, minimum):
+    import copy
+    clone = copy.copy(mapping)
+    clone.settings = {**mapping.settings, "minimum_design_density": minimum}
+    return clone

@@ -51,7 +51,9 @@ class MMA:
                                       ptr(lam), ctypes.byref(newton), _lib.stream_of(self.device))
         if status:
             message = (self.lib.tf_mma_last_error(self.handle) or b"").decode()
-            raise (ValueError if status == 1 else _lib.TfError)(f"tf_mma_step failed: {message}")
+            if status == 1:
+                raise ValueError(f"tf_mma_step failed: {message}")
+            raise _lib.TfError(status, f"tf_mma_step failed: {message}")
         self.newton_iterations = int(newton.value)
         return xnew, y, float(z.value), lam
 

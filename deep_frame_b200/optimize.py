@@ -11,6 +11,11 @@ gradients pulled back through the filter, then one MMA step with the
 reference's settings (f and g scaled by 100, a0 = 1, a = 0, c = 1e4, d = 1,
 asyinit 0.5, asydecr 0.7, asyincr 1.2, raa0 1e-5).  Every field stays on the
 device; the host sees scalars and the 42 x 42 flexibility matrix.
+
+``warm_start=True`` starts every design iteration's PCG from the previous
+iteration's displacements instead of zero (the reference always starts from
+zero); the converged answer is the same to the solver tolerance, the iteration
+count drops as the design settles.
 """
 from time import perf_counter
 
@@ -27,7 +32,7 @@ MMA_SETTINGS = {"scale": 100.0, "asyinit": 0.5, "asydecr": 0.7, "asyincr": 1.2, 
 
 class CovarianceSimp:
     def __init__(self, domain, covariance, volume_fraction=0.15, filter_radius=1.5, penalization=3.0, min_stiffness_ratio=1e-9,
-                 move=0.2, multigrid=None, device="cuda", objective_scale=None):
+                 move=0.2, multigrid=None, device="cuda", objective_scale=None, warm_start=False):
         import torch
         self.torch = torch
         self.device = torch.device(device)
@@ -42,6 +47,8 @@ class CovarianceSimp:
         self.free = torch.as_tensor(np.flatnonzero(self.map.free), device=self.device)
         self.mma = MMA(1, len(self.free), self.device)
         self.objective_scale = objective_scale
+        self.warm_start = bool(warm_start)
+        self.previous = None
         self.lib = _lib.load()
         n = self.system.nelem
         f64 = dict(dtype=torch.float64, device=self.device)
@@ -64,7 +71,9 @@ class CovarianceSimp:
                                   _lib.ptr(self.moduli), _lib.ptr(self.dE), _lib.ptr(self.volume), _lib.stream_of(self.device))
         _lib.check(status, None, "tf_simp")
         mg.update_device(self.moduli)
-        solved = self.model.solve_all()
+        solved = self.model.solve_all(self.previous if self.warm_start else None)
+        if self.warm_start:
+            self.previous = {key: u for key, _, _, u, _ in solved}
         rows = self.model.measure_from(solved, -self.dE, gradients=True, worst_gradient=False)
         tr = rows[0]["value"]
         if self.objective_scale is None:

@@ -215,8 +215,11 @@ class GeometricMultigrid:
         report["seconds"] = perf_counter() - started
         return flat, report
 
-    def solve_device(self, key, fixed, forces, out=None, support=None):
-        """Device-resident solve: forces [R, ndof] contiguous CUDA float64; returns (u [R, ndof], report)."""
+    def solve_device(self, key, fixed, forces, out=None, support=None, initial=None):
+        """Device-resident solve: forces [R, ndof] contiguous CUDA float64; returns (u [R, ndof], report).
+
+        ``initial`` ([R, ndof] CUDA float64) starts PCG from that guess instead of zero, as the
+        reference's ``_pcg(hierarchy, rhs, initial)`` does for its retries."""
         torch = self.torch
         floating = support is not None and self.settings["projection"]
         if floating:
@@ -229,6 +232,11 @@ class GeometricMultigrid:
         count = forces.shape[0]
         ident = self._key((key, False), fixed)
         out = torch.empty_like(forces) if out is None else out
+        if initial is not None:
+            if initial.shape != forces.shape or initial.dtype != torch.float64 or not initial.is_cuda:
+                raise ValueError("initial must be a CUDA float64 tensor shaped like forces")
+            if initial.data_ptr() != out.data_ptr():
+                out.copy_(initial)
         iterations = np.zeros(count, dtype=np.int32)
         relative = np.zeros(count, dtype=np.float64)
         history = np.zeros(self.settings["max_iterations"] * (1 + self.settings["retries"]) + 8, dtype=np.float64)
@@ -237,8 +245,9 @@ class GeometricMultigrid:
         report.relative_residual = relative.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         report.history = history.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         report.history_capacity = len(history)
-        _lib.check(self.lib.tf_solve(self.handle, ident, _lib.ptr(forces), count, _lib.ptr(out), ctypes.byref(report),
-                                     self._stream()), self.handle, "tf_solve")
+        entry = self.lib.tf_solve if initial is None else self.lib.tf_solve_guess
+        _lib.check(entry(self.handle, ident, _lib.ptr(forces), count, _lib.ptr(out), ctypes.byref(report), self._stream()),
+                   self.handle, "tf_solve" if initial is None else "tf_solve_guess")
         levels = int(report.levels)
         result = {"iterations": iterations.tolist(), "relative_residual": relative.tolist(),
                   "converged": bool(report.converged), "history": [history[:report.history_len].tolist()],

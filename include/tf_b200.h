@@ -118,6 +118,13 @@ TF_API int tf_set_bc(tf_handle* h, uint64_t key, const int64_t* fixed, int64_t c
 TF_API int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
              void* stream);
 
+/* tf_solve started from an initial guess: u_dev is read as the guess (Dirichlet dofs are
+ * masked to zero) and overwritten by the solution.  The reference's _pcg(hierarchy, rhs,
+ * initial) (topology_multigrid.py:407-417, used by its retries at :393) starts from
+ * r = b - A x0 the same way; zero-force columns still return zero. */
+TF_API int tf_solve_guess(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
+                          void* stream);
+
 /* GeometricMultigrid.hierarchy(key, fixed) (topology_multigrid.py:145-208): build (or reuse)
  * the hierarchy of `key` now and fill the level fields of `report` (levels, coarsest_dofs,
  * setup_s, lambda_max); report may be NULL. */
@@ -190,6 +197,30 @@ TF_API int tf_filter_sums(const tf_filter* f, double* sums_dev, void* stream);
 /* Threshold projection with derivative; robust != 0 selects the eroded/dilated form. */
 TF_API int tf_filter_project(tf_filter* f, const double* filtered_dev, double beta, double eta, int32_t robust,
                              double* physical_dev, double* derivative_dev, void* stream);
+/* DensityMap.volume (topology_optimization.py:1146-1151): *volume_dev = sum(weights *
+ * project(filtered(design), eta)) with weights NULL = ones; one fused launch with a
+ * deterministic reduction.  Pass the dilated threshold for the robust volume. */
+TF_API int tf_filter_volume(tf_filter* f, const double* design_dev, const double* weights_dev, double beta, double eta,
+                            int32_t robust, double* volume_dev, void* stream);
+
+/* Optimality-criteria update _oc_update (topology_optimization.py:1197-1233): ratios
+ * max(1e-30, -dC/max(dV, 1e-12 max dV)) on the free cells, move-limited bounds, the
+ * lowest-design shortcut, multiplier bracketing (x2, at most 100) and bisection (at most
+ * 70, relative width 1e-8) against `target` of the volume above evaluated at threshold
+ * `eta`.  The search runs on the device; the host reads its state once per 8 rounds.
+ * Status TF_NUMERIC with "Invalid OC sensitivities" or "OC could not bracket the volume
+ * multiplier" mirrors the reference's RuntimeErrors.  candidate_dev must not alias design_dev. */
+typedef struct tf_oc_report {
+  double multiplier;   /* accepted multiplier (the bracket's upper end); 0 for the lowest design */
+  double lower;        /* lower end of the final bracket */
+  double volume;       /* volume of the last evaluated proposal */
+  int32_t evaluations; /* volume evaluations */
+  int32_t lowest;      /* 1 when the lowest design already exceeded the target */
+} tf_oc_report;
+TF_API int tf_oc_update(tf_filter* f, const double* design_dev, const double* objective_derivative_dev,
+                        const double* volume_derivative_dev, const double* weights_dev, double target, double minimum_density,
+                        double move_limit, double beta, double eta, int32_t robust, double* candidate_dev, tf_oc_report* report,
+                        void* stream);
 TF_API int tf_filter_destroy(tf_filter* f);
 TF_API const char* tf_filter_last_error(const tf_filter* f);
 

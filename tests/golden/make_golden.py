@@ -163,15 +163,71 @@ def covariance(topt, tprob):
     tp.close()
 
 
+def optimality_criteria(topt):
+    """Reference OC driver runs and standalone _oc_update calls on the reference's beam test domains
+    (tests/test_topology_optimization.py:16-35, :139-147, :231-245, :491-535)."""
+    import json
+    from copy import deepcopy
+    from tests.test_topology_optimization import ROBUST_RUN, beam_domain
+    out = {}
+    runs = {
+        "single": ((5, 3, 3), (2.0, 2.0, 2.0), {"volume_fraction": 0.65, "filter_radius_mm": 3.1, "max_iterations": 3, "change_tolerance": 1e-12}),
+        "robust": ((8, 4, 4), (1.0, 1.0, 1.0), {**ROBUST_RUN, "volume_fraction": 0.5, "beta_schedule": [1, 4], "beta_interval": 2,
+                                                 "beta_minimum_iterations": 2, "max_iterations": 4, "change_tolerance": 1e-12,
+                                                 "move_limit_late_beta": 4}),
+    }
+    for name, (shape, spacing, settings) in runs.items():
+        domain = beam_domain(shape, spacing)
+        result = topt.optimize_topology(deepcopy(domain), settings)
+        assert result["status"] == "ok", result["diagnostics"]
+        system = topt.HexElasticity(domain)
+        cases = [(case["name"], case["fixed"], case["parts"][0]["force"]) for case in system.cases if case["analysis"] == "static"]
+        out.update({f"{name}_shape": np.asarray(shape), f"{name}_spacing": np.asarray(spacing), f"{name}_settings": json.dumps(settings),
+                    f"{name}_ke": system.ke, f"{name}_young": system.young, f"{name}_allowed": domain["allowed"].ravel(),
+                    f"{name}_preserve": domain["preserve"].ravel(), f"{name}_case_names": json.dumps([c[0] for c in cases]),
+                    f"{name}_density": result["density"].ravel(), f"{name}_design": result["design_density"].ravel(),
+                    f"{name}_objective": np.asarray([e["objective"] for e in result["history"]]),
+                    f"{name}_compliance": np.asarray([[e["compliances_n_mm"][c[0]] for c in cases] for e in result["history"]]),
+                    f"{name}_change": np.asarray([np.nan if e["maximum_design_change"] is None else e["maximum_design_change"] for e in result["history"]])})
+        for k, (_, fixed, force) in enumerate(cases):
+            out[f"{name}_fixed_{k}"], out[f"{name}_force_{k}"] = fixed, force
+        if name == "robust":
+            out.update(robust_eroded=result["eroded_density"].ravel(), robust_dilated=result["dilated_density"].ravel(),
+                       robust_beta=np.asarray([e["projection_beta"] for e in result["history"]]),
+                       robust_move=np.asarray([np.nan if e["move_limit"] is None else e["move_limit"] for e in result["history"]]),
+                       robust_volume_target=np.asarray([e["dilated_volume_target"] for e in result["history"]]))
+    # standalone updates on the robust map (beta 4) of the 6x4x4 beam
+    domain = beam_domain((6, 4, 4), (1.0, 1.0, 1.0))
+    mapping = topt.DensityMap(domain, topt._settings({"projection": "robust", "filter_radius_mm": 2.6}))
+    mapping.beta = 4.0
+    design = np.random.default_rng(5).uniform(0.2, 0.8, mapping.n)
+    design[mapping.preserve] = 1
+    fields, _ = mapping.fields(design)
+    objective = -np.random.default_rng(2).uniform(0.5, 1.5, mapping.n)
+    volume = mapping.pullback(np.ones(mapping.n), fields["dilated"][1])
+    target = 0.97 * mapping.volume(design)
+    out.update(update_design=design, update_objective=objective, update_volume_derivative=volume, update_target=target,
+               update_candidate=topt._oc_update(design, objective, volume, mapping, target, mapping.settings, 0.2),
+               update_lowest_target=0.5 * mapping.volume(design),
+               update_lowest=topt._oc_update(design, objective, volume, mapping, 0.5 * mapping.volume(design), mapping.settings, 0.05),
+               update_allowed=domain["allowed"].ravel(), update_preserve=domain["preserve"].ravel())
+    np.savez_compressed(OUT / "oc.npz", **out)
+
+
 def main(source):
+    """Regenerate every fixture; ``--only NAME[,NAME]`` limits it to the named generators."""
     topt, tmg, tprob = load_reference(source)
-    hex8(topt)
-    operator(topt, tmg, tprob)
-    direct(topt, (16, 8, 8), 0, "cantilever_small")
-    density_filter(topt)
-    covariance(topt, tprob)
-    if "--skip-config1" not in sys.argv:
-        direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")
+    steps = {"hex8": lambda: hex8(topt), "operator": lambda: operator(topt, tmg, tprob),
+             "cantilever_small": lambda: direct(topt, (16, 8, 8), 0, "cantilever_small"), "filter": lambda: density_filter(topt),
+             "covariance": lambda: covariance(topt, tprob), "oc": lambda: optimality_criteria(topt),
+             "cantilever_48x24x24": lambda: direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")}
+    only = next((arg.split("=", 1)[1] for arg in sys.argv if arg.startswith("--only=")), None)
+    for name, step in steps.items():
+        if only is not None and name not in only.split(","):
+            continue
+        if name == "cantilever_48x24x24" and "--skip-config1" in sys.argv:
+            continue
+        step()
 
 
 if __name__ == "__main__":

@@ -92,3 +92,38 @@ def test_batched_columns_match_single_columns(cuda):
     expected = direct(shape, k0, moduli, fixed, forces)
     assert np.linalg.norm(flat - expected) < 1e-7 * np.linalg.norm(expected)
     mg.close()
+
+
+def test_warm_start_matches_cold_solution_with_fewer_iterations(cuda):
+    """tf_solve_guess: starting from the solution of a nearby design converges to the same answer faster."""
+    import torch
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    shape = (16, 8, 8)
+    k0, rho, moduli, fixed, force = cantilever(shape, 4)
+    rng = np.random.default_rng(11)
+    forces = np.column_stack([force, rng.normal(size=force.size), np.zeros(force.size)])
+    forces[fixed] = 0
+    mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 200, "precision": "float64", "tolerance": 1e-10})
+    nearby = 1e-9 + (1 - 1e-9) * np.clip(rho * (1 + 0.02 * rng.normal(size=rho.size)), 0.01, 1.0) ** 3
+    mg.update(nearby)
+    f = torch.as_tensor(np.ascontiguousarray(forces.T), device="cuda")
+    guess, _ = mg.solve_device("w", fixed, f)
+    guess = guess.clone()
+    mg.update(moduli)
+    cold, cold_report = mg.solve_device("w", fixed, f)
+    cold = cold.clone()
+    warm, warm_report = mg.solve_device("w", fixed, f, initial=guess)
+    assert warm_report["converged"] and cold_report["converged"]
+    assert warm_report["zero_rhs_columns"] == 1 and not torch.any(warm[2])
+    assert max(warm_report["iterations"][:2]) < max(cold_report["iterations"][:2])
+    expected = direct(shape, k0, moduli, fixed, forces)
+    for c in range(2):
+        got = warm[c].cpu().numpy()
+        assert np.linalg.norm(got - expected[:, c]) < 1e-7 * np.linalg.norm(expected[:, c])
+    # a guess that is already the solution still takes one step and stays put
+    again, again_report = mg.solve_device("w", fixed, f, initial=warm.clone())
+    assert max(again_report["iterations"]) <= 2
+    assert torch.linalg.vector_norm(again - warm) <= 1e-9 * torch.linalg.vector_norm(warm)
+    with pytest.raises(ValueError):
+        mg.solve_device("w", fixed, f, initial=guess[:2])
+    mg.close()
