@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
+    ap.add_argument("--simp-compare", action="store_true", help="also run the plain FP64 V-cycle and compare the designs")
+    ap.add_argument("--warm-start", action="store_true", help="SIMP: start every PCG from the previous design's solution")
     return ap.parse_args()
 
 
@@ -305,10 +308,65 @@ def reference(args):
     return line
 
 
+def simp(args):
+    """--simp N: iterations/s of the covariance SIMP + MMA loop (the mixed-precision loop of the 128 x 128 x 24 plate).
+
+    Every iteration: filter, SIMP moduli, both hierarchies, 2 x 42 solves to the tolerance, F, tr, the tr
+    sensitivity, pullbacks and one device MMA step.  Timed with CUDA events on the current stream around
+    the whole loop (host work between launches included).  With --simp-compare the plain FP64 V-cycle runs
+    the same loop and the final physical densities, tr histories and times are compared."""
+    import torch
+    from deep_frame_b200 import _lib, problems
+    from deep_frame_b200.optimize import CovarianceSimp
+    config = args.config if args.config != CONFIG else "plate_128x128x24"
+    spec = problems.CONFIGS[config]
+    domain, _, cov = problems.plate(spec["shape"], 0)
+    smoother = {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5}
+    precisions = [args.precision] + (["float64"] if args.simp_compare and args.precision != "float64" else [])
+    runs, physical = {}, {}
+    for precision in precisions:
+        loop = CovarianceSimp(domain, cov, volume_fraction=0.15, filter_radius=1.5, move=0.2, warm_start=args.warm_start,
+                              multigrid={"precision": precision, "tolerance": spec["tolerance"], **smoother})
+        loop.run(1)                                   # buffers, constant slots and MMA workspace (not timed)
+        loop.objective_scale, loop.previous = None, None
+        torch.cuda.synchronize()
+        launches0 = int(_lib.load().tf_launch_count())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(0) as clocks:
+            e0.record()
+            x, history = loop.run(args.simp)
+            e1.record()
+            torch.cuda.synchronize()
+        seconds = e0.elapsed_time(e1) / 1e3
+        physical[precision] = loop.map.filtered_device(x).cpu().numpy()     # physical density (beta = 0)
+        runs[precision] = {"iter_per_s": args.simp / seconds, "seconds": seconds, "tr_history": [r["tr"] for r in history],
+                           "final_tr": history[-1]["tr"], "final_volume": history[-1]["volume"],
+                           "pcg_iterations_mean": float(np.mean([max(r["pcg_iterations"]) for r in history])),
+                           "gpu_launches": int(_lib.load().tf_launch_count()) - launches0, "clocks": clocks.summary()}
+        loop.close()
+    main_run = runs[args.precision]
+    line = {"metric": "SIMP iter/s (covariance tr objective, MMA)", "value": round(main_run["iter_per_s"], 4), "unit": "iter/s",
+            "n_gpus": 1, "steps": args.simp, "warmup": 1, "higher_is_better": True, "dtype": "f64 outer / " + args.precision + " V-cycle",
+            "data": "synthetic",
+            "config": {"workload": config, "iterations": args.simp, "volume_fraction": 0.15, "filter_radius": 1.5, "penalization": 3.0,
+                       "move": 0.2, "rhs_per_half": 42, "tolerance": spec["tolerance"], "smoother": smoother, "warm_start": args.warm_start},
+            "clocks": main_run["clocks"], "gpu_launches": main_run["gpu_launches"],
+            "runs": {p: {k: v for k, v in r.items() if k not in ("tr_history", "clocks")} for p, r in runs.items()}}
+    if "float64" in runs and args.precision != "float64":
+        a, b = runs[args.precision]["tr_history"], runs["float64"]["tr_history"]
+        line["vs_fp64"] = {"final_density_max_abs": float(np.max(np.abs(physical[args.precision] - physical["float64"]))),
+                           "tr_history_max_rel": float(np.max(np.abs(np.asarray(a) / np.asarray(b) - 1))),
+                           "speedup": runs[args.precision]["iter_per_s"] / runs["float64"]["iter_per_s"]}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference(args)
+        return
+    if args.simp:
+        simp(args)
         return
     result, system, model, density = ours(args)
     if result["rank"] != 0:
