@@ -569,6 +569,68 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) block_level_kernel(const Leve
   }
 }
 
+// Galerkin levels as assembled 27-point stencils: S[(d * 9 + 3 q + r)][node] is the 3 x 3 coupling of
+// the node with its neighbour node + d, summed over the elements holding both.  Per node and column
+// that is 243 FMA and 243 / CB coefficient loads, against 576 of each for the element blocks.
+template <typename T, int CB>
+__global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);   // [CB][HALO][3]
+  const int c0 = blockIdx.y * CB;
+  if (a.gate && !*a.gate) return;
+  const int nc = min(CB, a.ncol - c0);
+  bool any = false;
+  for (int c = 0; c < nc; ++c) any |= (!a.active || a.active[c0 + c]);
+  if (!any) return;
+  const Geo& g = a.g;
+  const int b = blockIdx.x;
+  const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
+  const int tz = tm.tz;
+  const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
+  const long long off = (long long)c0 * a.colstride;
+#pragma unroll
+  for (int c = 0; c < CB; ++c) {
+    if (c < nc) stage_tile(su + c * HALO * 3, g, a.u + off + c * a.colstride, a.mask, x0, y0, z0, tz);
+  }
+  __syncthreads();
+  const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
+  const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const long long n = ((long long)i * g.ny + j) * g.nz + k;
+  const long long nst = g.nnode;
+  const T* sp = a.E + n;
+  T out[CB][3];
+#pragma unroll
+  for (int c = 0; c < CB; ++c) { out[c][0] = T(0); out[c][1] = T(0); out[c][2] = T(0); }
+  const int cbase = 3 * (((lx + 1) * HY + (ly + 1)) * HZ + (lz + 1));
+#pragma unroll
+  for (int di = -1; di <= 1; ++di) {
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+#pragma unroll
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int d = ((di + 1) * 3 + (dj + 1)) * 3 + (dk + 1);
+        const int noff = cbase + 3 * ((di * HY + dj) * HZ + dk);
+        T sv[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) sv[q] = sp[(long long)(d * 9 + q) * nst];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+          const T* p = su + c * HALO * 3 + noff;
+          const T u0 = p[0], u1 = p[1], u2 = p[2];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) out[c][q] = fma(sv[3 * q + 2], u2, fma(sv[3 * q + 1], u1, fma(sv[3 * q], u0, out[c][q])));
+        }
+      }
+    }
+  }
+  const unsigned m = a.mask ? a.mask[n] : 7u;
+#pragma unroll
+  for (int c = 0; c < CB; ++c) {
+    if (c < nc && (!a.active || a.active[c0 + c])) epilogue(a, mode, off + c * a.colstride, n, m, out[c]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Element energies u_e^T K0 u_e.  With comb == nullptr, column r contributes
 // coef[r] * u_r,e^T K0 u_r,e; otherwise combination j forms w = U comb[:, j]

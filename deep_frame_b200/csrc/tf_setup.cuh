@@ -222,6 +222,48 @@ __global__ void __launch_bounds__(128) galerkin_kernel(const __grid_constant__ G
   }
 }
 
+// Assembled 27-point stencil of a Galerkin level from its [nelem][576] FP64 element blocks (block row
+// 3 corner + q, column 3 corner + r): one thread per (neighbour offset d, node) sums the 3 x 3 blocks
+// coupling the node (corner cn of element e) with node + d (corner cm of e) over the elements holding
+// both, in a fixed element order.  Output entry-major [243][nnode] in FP64, and in FP32 when s32 is set.
+__global__ void stencil_assemble_kernel(Geo g, const double* __restrict__ blocks, double* __restrict__ s64,
+                                        float* __restrict__ s32) {
+  const long long nnode = g.nnode;
+  const long long total = 27 * nnode;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int d = static_cast<int>(t / nnode);
+    const long long n = t % nnode;
+    const int k = static_cast<int>(n % g.nz);
+    const long long r1 = n / g.nz;
+    const int j = static_cast<int>(r1 % g.ny), i = static_cast<int>(r1 / g.ny);
+    const int di = d / 9 - 1, dj = (d / 3) % 3 - 1, dk = d % 3 - 1;
+    double acc[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+      const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
+      if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
+      const int ei = i - 1 + ox, ej = j - 1 + oy, ek = k - 1 + oz;
+      if (!((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez)) continue;
+      const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+      const int cm = corner_id(cx, cy, cz);
+      const double* bp = blocks + (((long long)ei * g.ey + ej) * g.ez + ek) * 576 + (3 * cn) * 24 + 3 * cm;
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr) acc[3 * q + rr] += bp[q * 24 + rr];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const long long o = (long long)(d * 9 + q) * nnode + n;
+      s64[o] = acc[q];
+      if (s32) s32[o] = static_cast<float>(acc[q]);
+    }
+  }
+}
+
 // [nelem][576] FP64 blocks -> entry-major [576][nelem] copy in T (tiled through shared memory).
 template <typename T>
 __global__ void blocks_soa_kernel(const double* __restrict__ aos, T* __restrict__ soa, long long nelem) {

@@ -40,8 +40,8 @@ struct Level {
   long long ndof = 0, nelem = 0;
   DevBuf mask;      // uint8 [nnode]
   DevBuf blocks64;  // Galerkin blocks [nelem][576] (levels >= 1), used by the set-up
-  DevBuf blocks64s; // entry-major FP64 copy [576][nelem] for the operator
-  DevBuf blocksw;   // entry-major FP32 copy (FP32 work precision only)
+  DevBuf stencil64; // assembled 27-point stencil, entry-major FP64 [243][nnode], for the operator
+  DevBuf stencilw;  // FP32 copy (FP32 work precision only)
   DevBuf inv64;     // inverse diagonal [ndof]
   DevBuf invw;      // FP32 copy (FP32 work precision only)
   double lambda_max = 1.0;
@@ -269,7 +269,7 @@ template <typename T>
 const T* level_E(tf_handle* h, Hierarchy& hy, int l, bool precise) {
   const bool dbl = std::is_same<T, double>::value;
   if (l == 0) return static_cast<const T*>(dbl ? h->moduli64.p : h->modulif.p);
-  return static_cast<const T*>(dbl ? hy.lv[l].blocks64s.p : hy.lv[l].blocksw.p);
+  return static_cast<const T*>(dbl ? hy.lv[l].stencil64.p : hy.lv[l].stencilw.p);
 }
 template <typename T>
 const T* level_inv(Hierarchy& hy, int l) {
@@ -395,8 +395,8 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
     dim3 grid(tiles, (a.ncol + cb - 1) / cb);
     const size_t smem = sizeof(T) * 3 * HALO * cb;
-    block_level_kernel<T, cb><<<grid, threads, smem, st>>>(a, mode, tm);
-    TF_LAUNCH_CHECK("block_level_kernel");
+    stencil_level_kernel<T, cb><<<grid, threads, smem, st>>>(a, mode, tm);
+    TF_LAUNCH_CHECK("stencil_level_kernel");
   }
 }
 
@@ -632,15 +632,11 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
                                                                             c.mask.as<uint8_t>(), c.inv64.as<double>(),
                                                                             dbl ? nullptr : c.invw.as<float>());
     TF_LAUNCH_CHECK("coarse_mask_inv_kernel");
-    const dim3 tgrid((unsigned)((c.nelem + 31) / 32), 9);
-    c.blocks64s.ensure(sizeof(double) * 576 * c.nelem);
-    blocks_soa_kernel<double><<<tgrid, 256, 0, st>>>(c.blocks64.as<double>(), c.blocks64s.as<double>(), c.nelem);
-    TF_LAUNCH_CHECK("blocks_soa_kernel");
-    if (!dbl) {
-      c.blocksw.ensure(sizeof(float) * 576 * c.nelem);
-      blocks_soa_kernel<float><<<tgrid, 256, 0, st>>>(c.blocks64.as<double>(), c.blocksw.as<float>(), c.nelem);
-      TF_LAUNCH_CHECK("blocks_soa_kernel");
-    }
+    c.stencil64.ensure(sizeof(double) * 243 * c.g.nnode);
+    if (!dbl) c.stencilw.ensure(sizeof(float) * 243 * c.g.nnode);
+    stencil_assemble_kernel<<<grid_for(27 * c.g.nnode, 256), 256, 0, st>>>(c.g, c.blocks64.as<double>(), c.stencil64.as<double>(),
+                                                                           dbl ? nullptr : c.stencilw.as<float>());
+    TF_LAUNCH_CHECK("stencil_assemble_kernel");
   }
   // lambda_max(D^-1 A) of every smoothed level, in the work precision
   if (dbl) ensure_vbufs<double>(h, 1); else ensure_vbufs<float>(h, 1);
