@@ -395,6 +395,11 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
     dim3 grid(tiles, (a.ncol + cb - 1) / cb);
     const size_t smem = sizeof(T) * 3 * HALO * cb;
+    static bool configured = false;   // per instantiation and process; the attribute is per function
+    if (!configured) {
+      TF_CUDA_CHECK(cudaFuncSetAttribute(stencil_level_kernel<T, cb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured = true;
+    }
     stencil_level_kernel<T, cb><<<grid, threads, smem, st>>>(a, mode, tm);
     TF_LAUNCH_CHECK("stencil_level_kernel");
   }
