@@ -86,17 +86,32 @@ class CovarianceSimp:
         return {"f0": f0, "df0": df0, "g": vol - 1.0, "dg": dg, "tr": tr, "lambda_max": rows[1]["value"], "volume": vol * self.volume_max,
                 "pcg_iterations": iterations, "physical": physical}
 
-    def run(self, iterations, x=None, callback=None):
+    def run(self, iterations, x=None, callback=None, state=None, checkpoint=None, checkpoint_interval=1):
+        """Run ``iterations`` SIMP + MMA iterations from the design ``x`` (default: uniform volume fraction).
+
+        ``state`` resumes an earlier run: the MMA iteration counter, previous iterates and asymptotes
+        over the free cells (``old1``, ``old2``, ``low``, ``upp``, as ``results.save_mma_state`` keeps
+        them) and the objective normalisation; the resumed run then takes the same steps as an
+        uninterrupted one.  ``checkpoint(x, state, history)`` is called every ``checkpoint_interval``
+        iterations with the state needed to resume.  The final state is kept in ``self.state``."""
         torch = self.torch
-        x = self.start() if x is None else x.clone()
+        x = self.start() if x is None else torch.as_tensor(x, dtype=torch.float64, device=self.device).clone()
         free = self.free
         xf = x[free].contiguous()
-        xold1, xold2 = xf.clone(), xf.clone()
-        low, upp = torch.zeros_like(xf), torch.ones_like(xf)
+        dev = lambda v: torch.as_tensor(v, dtype=torch.float64, device=self.device).reshape(-1).clone()
+        if state is None:
+            first = 1
+            xold1, xold2 = xf.clone(), xf.clone()
+            low, upp = torch.zeros_like(xf), torch.ones_like(xf)
+        else:
+            first = int(state["iteration"])
+            xold1, xold2, low, upp = (dev(state[key]) for key in ("old1", "old2", "low", "upp"))
+            if state.get("objective_scale") is not None:
+                self.objective_scale = float(state["objective_scale"])
         zeros, ones = torch.zeros_like(xf), torch.ones_like(xf)
         s = MMA_SETTINGS
         history = []
-        for it in range(1, iterations + 1):
+        for it in range(first, first + iterations):
             t0 = perf_counter()
             res = self.evaluate(x)
             df0 = (s["scale"] * res["df0"][free]).contiguous()
@@ -113,8 +128,11 @@ class CovarianceSimp:
                    "g": res["g"], "change": change, "pcg_iterations": res["pcg_iterations"], "newton": self.mma.newton_iterations,
                    "seconds": perf_counter() - t0}
             history.append(row)
+            self.state = {"iteration": it + 1, "old1": xold1, "old2": xold2, "low": low, "upp": upp, "objective_scale": self.objective_scale}
             if callback:
                 callback(row)
+            if checkpoint and len(history) % checkpoint_interval == 0:
+                checkpoint(x, self.state, history)
         return x, history
 
     def close(self):

@@ -139,3 +139,15 @@ def test_device_fields_are_ordered_and_respect_masks(cuda):
             assert np.allclose(fields[name][1], ref[name][1], rtol=1e-12, atol=1e-12)
         assert np.all(fields["eroded"][0] <= fields["intermediate"][0]) and np.all(fields["intermediate"][0] <= fields["dilated"][0])
         mapping.close()
+
+
+def test_outcome_files_round_trip(cuda, tmp_path):
+    from deep_frame_b200 import results
+    result = run("single")
+    shape = tuple(int(s) for s in GOLDEN["single_shape"])
+    dom = beam_domain(shape, tuple(GOLDEN["single_spacing"]))
+    record = results.write_outcome(tmp_path, dom, result, name="single")
+    back = results.read_outcome(tmp_path, record)
+    assert np.array_equal(back["density"], result["density"]) and np.array_equal(back["design_density"], result["design_density"])
+    assert back["summary"]["objective_final"] == result["summary"]["objective_final"]
+    assert [e["objective"] for e in back["history"]] == [e["objective"] for e in result["history"]]

@@ -88,3 +88,27 @@ def test_warm_started_simp_loop_matches_oracle_loop(cuda):
     assert sum(max(r["pcg_iterations"]) for r in history[1:]) <= sum(max(r["pcg_iterations"]) for r in cold_history[1:])
     warm.close()
     cold.close()
+
+
+def test_simp_run_resumes_from_saved_mma_state(cuda, tmp_path):
+    """Two iterations, the MMA state written to disk and read back, two more iterations = four in one run."""
+    from deep_frame_b200 import problems, results
+    from deep_frame_b200.optimize import CovarianceSimp
+    shape = (16, 12, 4)
+    domain, _, cov = problems.plate(shape, 2)
+    settings = {"tolerance": 1e-11, "coarsest_dofs": 300, "precision": "float64"}
+    straight = CovarianceSimp(domain, cov, volume_fraction=0.3, filter_radius=1.5, move=0.2, multigrid=settings)
+    x4, history4 = straight.run(4)
+    first = CovarianceSimp(domain, cov, volume_fraction=0.3, filter_radius=1.5, move=0.2, multigrid=settings)
+    saved = []
+    x2, _ = first.run(2, checkpoint=lambda x, state, history: results.save_mma_state(tmp_path / "mma.npz", x, state, history) or saved.append(1),
+                      checkpoint_interval=2)
+    assert saved == [1]
+    design, state, history = results.load_mma_state(tmp_path / "mma.npz")
+    second = CovarianceSimp(domain, cov, volume_fraction=0.3, filter_radius=1.5, move=0.2, multigrid=settings)
+    x, resumed = second.run(2, x=design, state=state)
+    assert [row["iteration"] for row in resumed] == [3, 4] and len(history) == 2
+    assert np.max(np.abs(x.cpu().numpy() - x4.cpu().numpy())) < 1e-10
+    assert resumed[-1]["tr"] == pytest.approx(history4[-1]["tr"], rel=1e-10)
+    for loop in (straight, first, second):
+        loop.close()
