@@ -144,6 +144,9 @@ struct tf_handle {
   double ke[576]{};
   K0Param<double> k64{};
   K0Param<float> k32{};
+  K0Param<double> m64{};   // consistent element mass M0 (tf_create's me), for tf_mass_apply
+  bool have_me = false;
+  DevBuf mass64, lumped64;  // padded element masses and lumped nodal masses of the last tf_mass_apply
   GalerkinParam W{};
   DevBuf Q, K0dev, k0diag;
   DevBuf moduli_un, moduli64, modulif;
@@ -958,7 +961,13 @@ extern "C" int tf_create(const tf_grid* grid, const double* ke, const double* me
       h->k64.k[t] = ke[t];
       h->k32.k[t] = static_cast<float>(ke[t]);
     }
-    (void)me;
+    if (me) {
+      for (int t = 0; t < 576; ++t) {
+        require(std::isfinite(me[t]), "me must be finite");
+        h->m64.k[t] = me[t];
+      }
+      h->have_me = true;
+    }
     {
       // reflection symmetry of ke (box element, axis-aligned orthotropic material)
       double kmax = 0.0, err = 0.0;
@@ -1305,6 +1314,79 @@ extern "C" int tf_apply(tf_handle* h, uint64_t key, int32_t use_mask, const doub
     TF_LAUNCH_CHECK("pad_kernel");
     fine_apply64(h, hy, h->vb.as<double>(), nullptr, h->vq.as<double>(), MODE_APPLY, nrhs, nullptr, nullptr, s);
     unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vq.as<double>(), h->un, h->geo[0], y_dev, nun, nullptr);
+    TF_LAUNCH_CHECK("unpad_kernel");
+  });
+}
+
+namespace {
+// y = mask * (sum_e mass_e M0 u_e + lumped * u) on the padded finest grid, u already masked; one thread
+// per (node, column), 8 elements x 8 corners x 9 FMA per node in a fixed order (deterministic).
+__global__ void mass_node_kernel(const __grid_constant__ K0Param<double> M, Geo g, const double* __restrict__ mass,
+                                 const double* __restrict__ lumped, const uint8_t* __restrict__ mask,
+                                 const double* __restrict__ u, long long colstride, double* __restrict__ y) {
+  const int col = blockIdx.y;
+  const double* uc = u + (long long)col * colstride;
+  double* yc = y + (long long)col * colstride;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nnode; n += (long long)gridDim.x * blockDim.x) {
+    const int k = static_cast<int>(n % g.nz);
+    const long long r = n / g.nz;
+    const int j = static_cast<int>(r % g.ny), i = static_cast<int>(r / g.ny);
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int e = 0; e < 8; ++e) {
+      const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+      const int ei = i - 1 + ox, ej = j - 1 + oy, ek = k - 1 + oz;
+      if (!((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez)) continue;
+      const double me = mass[((long long)ei * g.ey + ej) * g.ez + ek];
+      if (me == 0.0) continue;
+      const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
+      for (int cm = 0; cm < 8; ++cm) {
+        const long long nm = ((long long)(ei + corner_x(cm)) * g.ny + (ej + corner_y(cm))) * g.nz + (ek + corner_z(cm));
+        const double u0 = uc[3 * nm], u1 = uc[3 * nm + 1], u2 = uc[3 * nm + 2];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const double* row = M.k + (3 * cn + q) * 24 + 3 * cm;
+          acc[q] = fma(me, fma(row[2], u2, fma(row[1], u1, row[0] * u0)), acc[q]);
+        }
+      }
+    }
+    const unsigned m = mask ? mask[n] : 7u;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double l = lumped ? lumped[3 * n + q] * uc[3 * n + q] : 0.0;
+      yc[3 * n + q] = ((m >> q) & 1u) ? acc[q] + l : 0.0;
+    }
+  }
+}
+}  // namespace
+
+extern "C" int tf_mass_apply(tf_handle* h, uint64_t key, const double* mass_dev, const double* lumped_dev, const double* u_dev,
+                             int32_t nrhs, double* y_dev, void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(h->have_me, "the handle was created without an element mass matrix");
+    require(mass_dev != nullptr, "element masses must not be NULL");
+    require(nrhs >= 0 && (nrhs == 0 || (u_dev && y_dev)), "invalid mass operator arguments");
+    require(h->have_moduli, "update(moduli) must be called before the mass operator (it uses the hierarchy mask)");
+    if (nrhs == 0) return;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Hierarchy& hy = get_hierarchy(h, key, s);
+    const Geo& pd = h->geo[0];
+    const long long nun = 3 * h->un.nnode;
+    h->mass64.ensure(sizeof(double) * (size_t)pd.ex * pd.ey * pd.ez);
+    pad_moduli_kernel<<<grid_for((long long)pd.ex * pd.ey * pd.ez, 256), 256, 0, s>>>(h->un, pd, mass_dev, h->mass64.as<double>(), nullptr);
+    TF_LAUNCH_CHECK("pad_moduli_kernel");
+    if (lumped_dev) {
+      h->lumped64.ensure(sizeof(double) * 3 * pd.nnode);
+      pad_kernel<<<cols_grid(pd.nnode, 1), 256, 0, s>>>(lumped_dev, nun, h->un, pd, nullptr, h->lumped64.as<double>(), nullptr);
+      TF_LAUNCH_CHECK("pad_kernel");
+    }
+    ensure_pcg(h, nrhs);
+    pad_kernel<<<cols_grid(pd.nnode, nrhs), 256, 0, s>>>(u_dev, nun, h->un, pd, hy.lv[0].mask.as<uint8_t>(), h->vb.as<double>(), nullptr);
+    TF_LAUNCH_CHECK("pad_kernel");
+    mass_node_kernel<<<cols_grid(pd.nnode, nrhs), 256, 0, s>>>(h->m64, pd, h->mass64.as<double>(), lumped_dev ? h->lumped64.as<double>() : nullptr,
+                                                               hy.lv[0].mask.as<uint8_t>(), h->vb.as<double>(), 3 * pd.nnode, h->vq.as<double>());
+    TF_LAUNCH_CHECK("mass_node_kernel");
+    unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vq.as<double>(), h->un, pd, y_dev, nun, nullptr);
     TF_LAUNCH_CHECK("unpad_kernel");
   });
 }

@@ -324,6 +324,140 @@ class GeometricMultigrid:
         return out
 
     # ----------------------------------------------------------- lifecycle --
+    # -------------------------------------------------------------- modes --
+    def mass_device(self, columns, key, fixed, mass, lumped=None, out=None):
+        """y = mask (sum_e mass_e M0 u_e + lumped u) on [R, ndof] device columns (tf_mass_apply)."""
+        if self.me64 is None:
+            raise ValueError("mass operator needs the element mass matrix (me) at construction")
+        out = self.torch.empty_like(columns) if out is None else out
+        ident = self._key((key, False), fixed)
+        _lib.check(self.lib.tf_mass_apply(self.handle, ident, _lib.ptr(mass), _lib.ptr(lumped), _lib.ptr(columns), columns.shape[0],
+                                          _lib.ptr(out), self._stream()), self.handle, "tf_mass_apply")
+        return out
+
+    def eigenpairs(self, key, fixed, mass, lumped, count, initial=None):
+        """Lowest ``count`` eigenpairs of K v = lambda M v by LOBPCG preconditioned with the V-cycle.
+
+        The reference's GeometricMultigrid.eigenpairs (topology_multigrid.py:488-534): a block of
+        count + eigen_guard vectors, SVQB M-orthonormalisation, Rayleigh-Ritz on [X, W, P], search
+        directions only for the columns above eigen_tolerance, explicit re-application of K and M every
+        eigen_refresh steps and before convergence is accepted.  ``mass`` are element masses [nelem],
+        ``lumped`` nodal masses [ndof] (or None); ``initial`` a [count + eigen_guard, ndof] block to
+        start from (e.g. the previous design's vectors).  Returns (values[:count] as NumPy, the device
+        vectors [count + eigen_guard, ndof] M-orthonormal, report).  The small dense Gram and Ritz
+        problems are solved on the host in FP64; K, M, the V-cycle and the block products run on the
+        device."""
+        torch = self.torch
+        torch.cuda.synchronize(self.device)
+        started = perf_counter()
+        settings, tolerance, drop = self.settings, float(self.settings["eigen_tolerance"]), float(self.settings["eigen_drop"])
+        if self.moduli is None:
+            raise ValueError("update(moduli) must be called before eigenpairs")
+        hierarchy = self.hierarchy((key, False), fixed)
+        ident = hierarchy["id"]
+        dev = lambda v: torch.as_tensor(np.ascontiguousarray(np.asarray(v, dtype=float).ravel()), device=self.device)
+        mass = dev(mass)
+        if mass.numel() != self.nelem:
+            raise ValueError(f"expected {self.nelem} element masses")
+        lumped = None if lumped is None else dev(lumped)
+        if lumped is not None and lumped.numel() != self.ndof:
+            raise ValueError(f"expected {self.ndof} lumped nodal masses")
+        ones = torch.ones((1, self.ndof), dtype=torch.float64, device=self.device)
+        zero_mass = torch.zeros_like(mass)
+        mask = self.mass_device(ones, key, fixed, zero_mass, ones[0])[0]        # the hierarchy's live-dof mask (0 / 1)
+
+        def apply(v):
+            v = (v * mask).contiguous()
+            return [v, self.apply_device(v, key, fixed), self.mass_device(v, key, fixed, mass, lumped)]
+
+        def gram(a, b):
+            return (a @ b.T).cpu().numpy()
+
+        def combine(blocks, coefficients):
+            c = torch.as_tensor(coefficients, device=self.device)
+            return [c.T @ block for block in blocks]
+
+        def norms(blocks):
+            return (blocks[0] * blocks[2]).sum(1).cpu().numpy()
+
+        def svqb(blocks, reference=None):
+            g = gram(blocks[0], blocks[2])
+            g = (g + g.T) / 2
+            diagonal = np.diag(g).copy()
+            limit = drop * (diagonal.max() if reference is None else reference)
+            live = diagonal > limit
+            coefficients = np.zeros((len(diagonal), 0))
+            if live.any():
+                scale = 1 / np.sqrt(diagonal[live])
+                values, rotation = np.linalg.eigh(scale[:, None] * g[np.ix_(live, live)] * scale[None, :])
+                keep = values > drop * values.max()
+                coefficients = np.zeros((len(diagonal), int(keep.sum())))
+                coefficients[live] = scale[:, None] * rotation[:, keep] / np.sqrt(values[keep])
+            return combine(blocks, coefficients)
+
+        def project(blocks, basis):
+            c = basis[2] @ blocks[0].T
+            return [block - c.T @ base for block, base in zip(blocks, basis)]
+
+        def rayleigh(blocks, size):
+            stiffness, g = gram(blocks[0], blocks[1]), gram(blocks[0], blocks[2])
+            values, rotation = np.linalg.eigh((g + g.T) / 2)
+            basis = rotation[:, values > drop * values.max()]
+            basis = basis / np.sqrt(np.diag(basis.T @ g @ basis))
+            reduced = basis.T @ stiffness @ basis
+            values, inner = np.linalg.eigh((reduced + reduced.T) / 2)
+            return values[:size], basis @ inner[:, :size]
+
+        def residual(blocks, values):
+            v = torch.as_tensor(values, device=self.device)
+            r = blocks[1] - v[:, None] * blocks[2]
+            return r, (torch.linalg.vector_norm(r, dim=1) / torch.linalg.vector_norm(blocks[1], dim=1)).cpu().numpy()
+
+        size = int(count) + int(settings["eigen_guard"])
+        if initial is None or tuple(initial.shape) != (size, self.ndof):
+            generator = torch.Generator(device=self.device).manual_seed(int(settings["eigen_seed"]))
+            initial = torch.rand((size, self.ndof), generator=generator, device=self.device, dtype=torch.float64) - 0.5
+        blocks = svqb(apply(torch.as_tensor(initial, dtype=torch.float64, device=self.device)))
+        values, rotation = rayleigh(blocks, size)
+        current, previous, step, history = combine(blocks, rotation), None, 0, []
+        while True:
+            res, relative = residual(current, values)
+            if step % settings["eigen_refresh"] == 0 or bool((relative[:count] < tolerance).all()):
+                current = apply(current[0])
+                res, relative = residual(current, values)
+            history.append(float(relative[:count].max()))
+            if bool((relative[:count] < tolerance).all()) or step >= settings["eigen_iterations"]:
+                break
+            active = torch.as_tensor(np.flatnonzero(relative >= tolerance), device=self.device)
+            z = torch.empty_like(res)
+            _lib.check(self.lib.tf_precondition(self.handle, ident, _lib.ptr(res.contiguous()), res.shape[0], _lib.ptr(z), self._stream()),
+                       self.handle, "tf_precondition")
+            search = apply(z[active])
+            search = svqb(project(project(search, current), current), norms(search))
+            parts = [current, search]
+            if previous is not None:
+                reference = norms(previous)
+                previous = svqb(project(project(project(previous, current), search), search), reference)
+                if previous[0].shape[0]:
+                    parts.append(previous)
+            blocks = [torch.cat(group) for group in zip(*parts)]
+            values, rotation = rayleigh(blocks, size)
+            current = combine(blocks, rotation)
+            rotation[:size] = 0
+            previous = combine(blocks, rotation)
+            step += 1
+        blocks = svqb(apply(current[0]))
+        values, rotation = rayleigh(blocks, size)
+        current = combine(blocks, rotation)
+        relative = residual(current, values)[1]
+        torch.cuda.synchronize(self.device)
+        report = {"iterations": step, "relative_residual": relative[:count].tolist(), "converged": bool((relative[:count] < tolerance).all()),
+                  "history": history, "seconds": perf_counter() - started, "setup_s": hierarchy.pop("setup_s", 0.0),
+                  "levels": len(hierarchy["levels"]), "coarsest_dofs": hierarchy["coarsest"]["dofs"], "kernel": None,
+                  "lambda_max": [level.lambda_max for level in hierarchy["levels"][:-1]]}
+        self.statistics.append(report)
+        return values[:count].copy(), current[0], report
+
     def diagnostics(self):
         return {"settings": self.settings, "levels": [{"shape": list(level.shape), "spacing_mm": level.spacing.tolist()} for level in self.levels],
                 "padded_shape": list(self.padded), "solves": self.statistics[-64:]}

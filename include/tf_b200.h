@@ -125,6 +125,13 @@ TF_API int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrh
 TF_API int tf_solve_guess(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
                           void* stream);
 
+/* Mass operator of GeometricMultigrid.eigenpairs (topology_multigrid.py:491-496): y = mask *
+ * (sum_e mass_e M0 (mask u)_e + lumped * u), with M0 the `me` given to tf_create, mass_dev the
+ * element masses [nelem] (unpadded, C order), lumped_dev the lumped nodal masses [ndof] (may be
+ * NULL) and mask the live-dof mask of hierarchy `key`; u_dev, y_dev are [nrhs][ndof] device FP64. */
+TF_API int tf_mass_apply(tf_handle* h, uint64_t key, const double* mass_dev, const double* lumped_dev, const double* u_dev,
+                         int32_t nrhs, double* y_dev, void* stream);
+
 /* GeometricMultigrid.hierarchy(key, fixed) (topology_multigrid.py:145-208): build (or reuse)
  * the hierarchy of `key` now and fill the level fields of `report` (levels, coarsest_dofs,
  * setup_s, lambda_max); report may be NULL. */
