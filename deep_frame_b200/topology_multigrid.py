@@ -219,11 +219,16 @@ class GeometricMultigrid:
         """Device-resident solve: forces [R, ndof] contiguous CUDA float64; returns (u [R, ndof], report).
 
         ``initial`` ([R, ndof] CUDA float64) starts PCG from that guess instead of zero, as the
-        reference's ``_pcg(hierarchy, rhs, initial)`` does for its retries."""
+        reference's ``_pcg(hierarchy, rhs, initial)`` does for its retries.
+
+        ``support`` (the statically determinate support dofs of an inertia-relief part, contained in
+        ``fixed``) is accepted for the reference's signature: the reference then solves the floating
+        structure with the rigid modes projected out and shifts the result to zero at the support
+        (topology_multigrid.py:340-349,368-370); for balanced loads that is the solution with every
+        dof of ``fixed`` held, which is what this solve computes."""
         torch = self.torch
-        floating = support is not None and self.settings["projection"]
-        if floating:
-            raise NotImplementedError("floating (inertia-relief) supports are not available in this build")
+        if support is not None and not np.isin(np.asarray(support, dtype=np.int64), np.asarray(fixed, dtype=np.int64)).all():
+            raise ValueError("support dofs must be part of fixed")
         started = perf_counter()
         if self.moduli is None:
             raise ValueError("update(moduli) must be called before solve")

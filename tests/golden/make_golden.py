@@ -214,12 +214,81 @@ def optimality_criteria(topt):
     np.savez_compressed(OUT / "oc.npz", **out)
 
 
+def _domain_json(domain):
+    """A domain dict as JSON text (boolean masks as nested lists)."""
+    import json
+    return json.dumps(domain, default=lambda value: value.tolist() if hasattr(value, "tolist") else float(value))
+
+
+def inertia_relief(topt):
+    """Reference inertia-relief cases (free-flying frame, determinate support, d'Alembert loads) solved by
+    SuperLU: the tiny half-model domain of tests/test_topology_problem.py:156-172 and the full / half
+    relief domain of tests/test_topology_optimization.py:585-612."""
+    from tests.test_topology_problem import tiny_domain
+    out = {}
+
+    def halves(domain, axis=0):
+        """Full (mirror-symmetrised masks) and half (cells on the positive side, symmetry plane at 0) domains."""
+        allowed = domain["allowed"] & np.flip(domain["allowed"], axis)
+        preserve = (domain["preserve"] | np.flip(domain["preserve"], axis)) & allowed
+        full = {**domain, "allowed": allowed, "preserve": preserve, "forbidden": ~allowed}
+        n = domain["grid"]["shape"][axis]
+        grid = {**domain["grid"], "shape": list(domain["grid"]["shape"]), "origin_mm": list(domain["grid"]["origin_mm"])}
+        grid["shape"][axis], grid["origin_mm"][axis] = n // 2, 0.0
+        cut = tuple(slice(n // 2, None) if d == axis else slice(None) for d in range(3))
+        half = {**full, "grid": grid, "symmetry": {"axis": axis, "plane_mm": 0.0},
+                **{key: full[key][cut].copy() for key in ("allowed", "preserve", "forbidden")}}
+        return full, half
+    shape = (8, 4, 4)
+    box = lambda low, high: {"kind": "box", "min_mm": low, "max_mm": high}
+    preserve = np.zeros(shape, dtype=bool)
+    preserve[[0, -1]] = True
+    relief = {"point_masses": [{"region": box([-8.01, -0.01, -0.01], [-5.99, 8.01, 0.01]), "mass_g": 3.0},
+                               {"region": box([3.99, 1.99, 7.99], [8.01, 6.01, 8.01]), "mass_g": 5.0}], "preserve_mass_g": 2.0}
+    loads = {"thrust": [{"region": box([5.99, -0.01, 7.99], [8.01, 8.01, 8.01]), "force_n": [0.0, 0.0, 2.0]},
+                        {"region": box([-8.01, -0.01, 7.99], [-5.99, 8.01, 8.01]), "force_n": [0.0, 0.0, 2.0]}],
+             "crash": [{"region": box([1.99, 7.99, 3.99], [6.01, 8.01, 8.01]), "force_n": [0.4, -3.0, 0.5]}]}
+    relief_domain = {"grid": {"shape": list(shape), "spacing_mm": [2.0, 2.0, 2.0], "origin_mm": [-8.0, 0.0, 0.0], "order": "C", "axis_order": "xyz"},
+                     "allowed": np.ones(shape, dtype=bool), "preserve": preserve, "forbidden": np.zeros(shape, dtype=bool),
+                     "material": {"young_modulus_mpa": 4430.0, "poisson_ratio": 0.3, "density_g_cm3": 1.09}, "point_masses": [],
+                     "load_cases": [{"name": name, "analysis": "static", "fixed_regions": [], "loads": load, "inertia_relief": relief} for name, load in loads.items()]}
+    full, half = halves(relief_domain)
+    domains = {"tiny": tiny_domain(), "relief_full": full, "relief_half": half}
+    for name, domain in domains.items():
+        system = topt.HexElasticity(domain, linear_solver="cpu_superlu")
+        density = np.random.default_rng(3).uniform(0.2, 1.0, system.nelem)
+        result = system.solve(density, metrics=True)
+        out[f"{name}_domain"] = _domain_json(domain)
+        out[f"{name}_density"] = density
+        out[f"{name}_support"] = system.support[1] if system.support is not None else np.zeros(0, dtype=np.int64)
+        names = sorted(result)
+        out[f"{name}_cases"] = np.asarray(names)
+        for case_name in names:
+            entry = result[case_name]
+            out[f"{name}_{case_name}_compliance"] = entry["compliance_n_mm"]
+            out[f"{name}_{case_name}_derivative"] = entry["derivative"]
+            out[f"{name}_{case_name}_max_displacement"] = entry["max_displacement_mm"]
+            case = next(c for c in system.cases if c["name"] == case_name)
+            if "inertia_relief" in case:
+                ir = case["inertia_relief"]
+                out[f"{name}_{case_name}_mass_g"] = ir["mass_g"]
+                out[f"{name}_{case_name}_center"] = np.asarray(ir["center_of_mass_mm"])
+                out[f"{name}_{case_name}_acceleration"] = np.asarray(ir["acceleration_n_per_g"])
+            for k, part in enumerate(case["parts"]):
+                out[f"{name}_{case_name}_part{k}_fixed"] = part["fixed"]
+                out[f"{name}_{case_name}_part{k}_force"] = part["force"]
+                out[f"{name}_{case_name}_part{k}_support"] = part["support"]
+        system.close()
+    np.savez_compressed(OUT / "inertia_relief.npz", **out)
+
+
 def main(source):
     """Regenerate every fixture; ``--only NAME[,NAME]`` limits it to the named generators."""
     topt, tmg, tprob = load_reference(source)
     steps = {"hex8": lambda: hex8(topt), "operator": lambda: operator(topt, tmg, tprob),
              "cantilever_small": lambda: direct(topt, (16, 8, 8), 0, "cantilever_small"), "filter": lambda: density_filter(topt),
              "covariance": lambda: covariance(topt, tprob), "oc": lambda: optimality_criteria(topt),
+             "inertia_relief": lambda: inertia_relief(topt),
              "cantilever_48x24x24": lambda: direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")}
     only = next((arg.split("=", 1)[1] for arg in sys.argv if arg.startswith("--only=")), None)
     for name, step in steps.items():
