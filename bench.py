@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tensor-cores", action="store_true", help="FP32 finest-level V-cycle apply on tcgen05 (TF32)")
     ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
     ap.add_argument("--simp-compare", action="store_true", help="also run the plain FP64 V-cycle and compare the designs")
     ap.add_argument("--warm-start", action="store_true", help="SIMP: start every PCG from the previous design's solution")
@@ -108,13 +109,14 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_problem(config, precision, device):
+def build_problem(config, precision, device, tensor_cores=False):
     from deep_frame_b200 import problems
     from deep_frame_b200.covariance import InterfaceCovariance
     from deep_frame_b200.elasticity import HexElasticity
     spec = problems.CONFIGS[config]
     domain, density, cov = problems.plate(spec["shape"], 0)
-    system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": spec["tolerance"], "device": str(device)})
+    system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": spec["tolerance"], "device": str(device),
+                                              "tensor_cores": tensor_cores})
     model = InterfaceCovariance(system, cov, domain["interfaces"])
     return spec, system, model, density
 
@@ -134,7 +136,7 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    spec, system, model, density = build_problem(args.config, args.precision, device)
+    spec, system, model, density = build_problem(args.config, args.precision, device, args.tensor_cores)
     moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
     moduli = torch.as_tensor(moduli_host, device=device)
     scale = torch.as_tensor(-derivative, device=device)
@@ -151,7 +153,7 @@ def ours(args):
             dist.broadcast_object_list(choice, src=0)
             if rank != 0:
                 tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
-                                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps")}],
+                                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores")}],
                                               repeats=1)
     mg = system._multigrid()
     measure = ShardedMeasure(groups, model.rank, model.factor, DeviceOps(system))
@@ -202,7 +204,7 @@ def ours(args):
               "iterations_max": [int(np.max(r["iterations"])) for r in timed[-len(groups):]], "clocks": clocks.summary(),
               "world": world, "rank": rank, "columns": [len(g["local"]) for g in measure.groups], "ndof": system.ndof,
               "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in timed),
-              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps")},
+              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores")},
               "tuning": tuning, "tr": rows[0]["value"], "lambda_max": rows[1]["value"]}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     result["dominant"] = dominant
@@ -399,9 +401,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
-                       "outer": "fp64 PCG", "vcycle": args.precision, "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
+                       "outer": "fp64 PCG", "vcycle": args.precision + (" (finest apply: tcgen05 TF32)" if result["smoother"].get("tensor_cores") else ""), "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
                        "pcg_iterations": result["iterations_max"], "smoother": result["smoother"],
-                       "smoother_choice": "autotuned (fastest of 5 schedules, all to the same tolerance)" if result["tuning"] else "reference default",
+                       "smoother_choice": "autotuned (fastest of 7 schedules / finest-apply units, all to the same tolerance)" if result["tuning"] else "reference default",
                        "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
                        "parallelism": f"rhs-sharded x{result['world']}"},
             "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),

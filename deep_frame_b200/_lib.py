@@ -30,7 +30,7 @@ class TfSettings(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("smoother", ctypes.c_int32), ("cycle", ctypes.c_int32),
                 ("coarse", ctypes.c_int32), ("sweeps", ctypes.c_int32), ("chebyshev_degree", ctypes.c_int32),
                 ("max_levels", ctypes.c_int32), ("power_iterations", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
-                ("retries", ctypes.c_int32), ("batch", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("retries", ctypes.c_int32), ("batch", ctypes.c_int32), ("tensor_cores", ctypes.c_int32),
                 ("coarsest_dofs", ctypes.c_int64), ("damping", ctypes.c_double), ("chebyshev_ratio", ctypes.c_double),
                 ("growth", ctypes.c_double), ("tolerance", ctypes.c_double), ("dead_ratio", ctypes.c_double),
                 ("zero_rhs", ctypes.c_double)]

@@ -24,6 +24,7 @@
 #include "tf_common.h"
 #include "tf_dense.h"
 #include "tf_setup.cuh"
+#include "tf_tc.cuh"
 
 using namespace tfb;
 
@@ -147,6 +148,7 @@ struct tf_handle {
   K0Param<double> m64{};   // consistent element mass M0 (tf_create's me), for tf_mass_apply
   bool have_me = false;
   DevBuf mass64, lumped64;  // padded element masses and lumped nodal masses of the last tf_mass_apply
+  DevBuf tc_err;            // int: set by the tensor-core finest-level kernel when an MMA wait timed out
   GalerkinParam W{};
   DevBuf Q, K0dev, k0diag;
   DevBuf moduli_un, moduli64, modulif;
@@ -367,8 +369,51 @@ void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   TF_LAUNCH_CHECK("fine_level_kernel");
 }
 
+// Tensor-core finest level (FP32 work precision, settings.tensor_cores): tiles of 8 x 8 x tz nodes
+// (tz = 8 or 9, whichever wastes less), columns looped inside the CTA so every CTA's set-up (K0
+// operand, element moduli, TMEM allocation) is spread over several columns.
+void launch_fine_tc(tf_handle* h, const LevelArgs<float>& a, int mode, cudaStream_t st) {
+  static bool configured = false;   // per process; the attribute is per function
+  if (!configured) {
+    TF_CUDA_CHECK(cudaFuncSetAttribute(tc::fine_tc_kernel<MODE_APPLY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES));
+    TF_CUDA_CHECK(cudaFuncSetAttribute(tc::fine_tc_kernel<MODE_RESID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES));
+    TF_CUDA_CHECK(cudaFuncSetAttribute(tc::fine_tc_kernel<MODE_JACOBI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES));
+    TF_CUDA_CHECK(cudaFuncSetAttribute(tc::fine_tc_kernel<MODE_CHEB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES));
+    configured = true;
+  }
+  if (!h->tc_err.p) {
+    h->tc_err.alloc(sizeof(int));
+    TF_CUDA_CHECK(cudaMemsetAsync(h->tc_err.p, 0, sizeof(int), st));
+  }
+  require(a.g.nnode < (1LL << 31), "grid too large for the tensor-core finest-level apply");
+  tc::TcTiles tm;
+  const int nz = a.g.nz;
+  tm.tz = ((nz + 8) / 9) * 9 < ((nz + 7) / 8) * 8 ? 9 : 8;
+  tm.tiles_x = (a.g.nx + tc::NXT - 1) / tc::NXT;
+  tm.tiles_y = (a.g.ny + tc::NYT - 1) / tc::NYT;
+  tm.tiles_z = (nz + tm.tz - 1) / tm.tz;
+  const long long tiles = (long long)tm.tiles_x * tm.tiles_y * tm.tiles_z;
+  int cpb = 1;
+  while (cpb < a.ncol && tiles * ((a.ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
+  dim3 grid((unsigned)tiles, (unsigned)((a.ncol + cpb - 1) / cpb));
+  int* err = h->tc_err.as<int>();
+  switch (mode) {
+    case MODE_APPLY: tc::fine_tc_kernel<MODE_APPLY><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(h->k32, a, tm, cpb, err); break;
+    case MODE_RESID: tc::fine_tc_kernel<MODE_RESID><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(h->k32, a, tm, cpb, err); break;
+    case MODE_JACOBI: tc::fine_tc_kernel<MODE_JACOBI><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(h->k32, a, tm, cpb, err); break;
+    default: tc::fine_tc_kernel<MODE_CHEB><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(h->k32, a, tm, cpb, err); break;
+  }
+  TF_LAUNCH_CHECK("fine_tc_kernel");
+}
+
 template <typename T>
 void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (h->s.tensor_cores) {
+      launch_fine_tc(h, a, mode, st);
+      return;
+    }
+  }
   const int slot = k0_slot(h);
   const int nz = a.g.nz;
   const bool nine = h->k0_reflect && ((nz + 8) / 9) * 9 < ((nz + 7) / 8) * 8;
@@ -1107,6 +1152,19 @@ extern "C" int tf_set_bc(tf_handle* h, uint64_t key, const int64_t* fixed, int64
 }
 
 namespace {
+// A tensor-core finest-level launch whose MMA wait ran out sets tc_err and skips the rest of its
+// columns; surface that as an error of the call instead of returning a wrong answer.
+void check_tensor_core_error(tf_handle* h, cudaStream_t s) {
+  if (!h->tc_err.p) return;
+  int v = 0;
+  TF_CUDA_CHECK(cudaMemcpyAsync(&v, h->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TF_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (v) {
+    TF_CUDA_CHECK(cudaMemsetAsync(h->tc_err.p, 0, sizeof(int), s));
+    throw Error(TF_INTERNAL, "tensor-core finest-level apply: an MMA completion wait timed out");
+  }
+}
+
 // Shared body of tf_solve (start from zero) and tf_solve_guess (start from u_dev, the reference's
 // _pcg(..., initial), topology_multigrid.py:407-417).
 int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report, void* stream,
@@ -1199,6 +1257,7 @@ int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, do
       ++batches;
     }
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    check_tensor_core_error(h, s);
     bool converged = true;
     for (int c : live) converged &= rel[c] < h->s.tolerance;
     if (report) {
@@ -1284,6 +1343,7 @@ extern "C" int tf_precondition(tf_handle* h, uint64_t key, const double* r_dev, 
     unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vz.as<double>(), h->un, h->geo[0], z_dev, nun, nullptr);
     TF_LAUNCH_CHECK("unpad_kernel");
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
+    check_tensor_core_error(h, s);
   });
 }
 

@@ -26,7 +26,7 @@ MULTIGRID = {"coarse": "galerkin", "coarsest_dofs": 8000, "max_levels": 8, "smoo
              "power_iterations": 20, "precision": "float32", "tolerance": 1e-8, "max_iterations": 2000, "batch": 0,
              "projection": True, "coarsest_projection": True, "dead_ratio": 1e-12, "zero_rhs": 1e-12, "retries": 2,
              "device": "cuda", "eigen_tolerance": 1e-8, "eigen_iterations": 300, "eigen_guard": 2, "eigen_refresh": 10,
-             "eigen_drop": 1e-12, "eigen_seed": 0}
+             "eigen_drop": 1e-12, "eigen_seed": 0, "tensor_cores": False}
 PRECISIONS = ("float64", "float32", "bfloat16", "float16")
 
 
@@ -58,6 +58,7 @@ def _native_settings(settings):
         setattr(s, name, int(settings[name]))
     for name in ("damping", "chebyshev_ratio", "growth", "tolerance", "dead_ratio", "zero_rhs"):
         setattr(s, name, float(settings[name]))
+    s.tensor_cores = 1 if settings.get("tensor_cores") else 0
     return s
 
 

@@ -63,7 +63,8 @@ typedef struct tf_settings {
   int32_t max_iterations;     /* PCG iteration limit */
   int32_t retries;            /* FP64 re-runs of columns that missed the tolerance */
   int32_t batch;              /* columns per PCG launch (0 = all live columns at once) */
-  int32_t reserved;
+  int32_t tensor_cores;       /* 1: FP32 finest-level V-cycle apply on the tensor cores (tcgen05, TF32 operands,
+                                 FP32 accumulation); 0: FP32 CUDA-core stencil.  FP64 applies are unaffected. */
   int64_t coarsest_dofs;      /* level count grows until the coarsest grid has <= this many dofs */
   double damping;             /* Jacobi damping */
   double chebyshev_ratio;     /* lambda_max / lambda_min of the Chebyshev interval */

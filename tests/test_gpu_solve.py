@@ -127,3 +127,32 @@ def test_warm_start_matches_cold_solution_with_fewer_iterations(cuda):
     with pytest.raises(ValueError):
         mg.solve_device("w", fixed, f, initial=guess[:2])
     mg.close()
+
+
+@pytest.mark.parametrize("shape", [(24, 12, 10), (16, 8, 16), (12, 20, 7)])
+def test_tensor_core_vcycle_matches_cuda_core_vcycle(cuda, shape):
+    """settings.tensor_cores: the FP32 finest-level apply on tcgen05 (TF32 operands) solves to the same answer.
+
+    The tensor-core apply is ~1e-3 accurate (TF32 operand rounding), so it changes the preconditioner a
+    little, never the converged solution: both V-cycles must give the direct solution to the tolerance,
+    similar iteration counts and the same lambda_max estimates to ~1e-2."""
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    k0, _, moduli, fixed, force = cantilever(shape, 6)
+    rng = np.random.default_rng(12)
+    forces = np.column_stack([force, rng.normal(size=(force.size, 4))])
+    forces[fixed] = 0
+    expected = direct(shape, k0, moduli, fixed, forces)
+    runs = {}
+    for tensor in (False, True):
+        mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 300, "precision": "float32", "tolerance": 1e-10,
+                                                        "tensor_cores": tensor})
+        mg.update(moduli)
+        solution, report = mg.solve("c", fixed, forces)
+        assert report["converged"], report
+        for c in range(forces.shape[1]):
+            assert np.linalg.norm(solution[:, c] - expected[:, c]) < 1e-7 * np.linalg.norm(expected[:, c])
+        runs[tensor] = report
+        mg.close()
+    assert max(runs[True]["iterations"]) <= 1.3 * max(runs[False]["iterations"]) + 2
+    lam_tc, lam_cc = np.asarray(runs[True]["lambda_max"]), np.asarray(runs[False]["lambda_max"])
+    assert np.max(np.abs(lam_tc / lam_cc - 1)) < 1e-2
