@@ -48,7 +48,9 @@ def parse():
     ap.add_argument("--tensor-cores", action="store_true", help="FP32 finest-level V-cycle apply on tcgen05 (TF32)")
     ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
     ap.add_argument("--simp-compare", action="store_true", help="also run the plain FP64 V-cycle and compare the designs")
-    ap.add_argument("--warm-start", action="store_true", help="SIMP: start every PCG from the previous design's solution")
+    ap.add_argument("--warm-start", type=int, default=0, nargs="?", const=-1,
+                    help="SIMP: start every PCG from the previous design's solution (no value), or from the energy-optimal "
+                         "combination of the last M designs' solutions (--warm-start M)")
     return ap.parse_args()
 
 
@@ -327,10 +329,11 @@ def simp(args):
     precisions = [args.precision] + (["float64"] if args.simp_compare and args.precision != "float64" else [])
     runs, physical = {}, {}
     for precision in precisions:
-        loop = CovarianceSimp(domain, cov, volume_fraction=0.15, filter_radius=1.5, move=0.2, warm_start=args.warm_start,
+        warm = True if args.warm_start == -1 else int(args.warm_start)
+        loop = CovarianceSimp(domain, cov, volume_fraction=0.15, filter_radius=1.5, move=0.2, warm_start=warm,
                               multigrid={"precision": precision, "tolerance": spec["tolerance"], **smoother})
         loop.run(1)                                   # buffers, constant slots and MMA workspace (not timed)
-        loop.objective_scale, loop.previous = None, None
+        loop.objective_scale, loop.previous, loop.basis = None, None, {}
         torch.cuda.synchronize()
         launches0 = int(_lib.load().tf_launch_count())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -70,23 +70,25 @@ def test_device_simp_loop_matches_oracle_loop(cuda):
     simp2.close()
 
 
-def test_warm_started_simp_loop_matches_oracle_loop(cuda):
-    """warm_start=True reuses the previous design's displacements; the designs still follow the oracle."""
+@pytest.mark.parametrize("warm", [True, 2])
+def test_warm_started_simp_loop_matches_oracle_loop(cuda, warm):
+    """warm_start=True reuses the previous design's displacements, warm_start=2 their energy-optimal
+    combination for the new stiffness; the designs still follow the oracle."""
     from deep_frame_b200 import problems
     from deep_frame_b200.optimize import CovarianceSimp
     shape = (16, 12, 4)
     domain, _, cov = problems.plate(shape, 2)
     settings = {"tolerance": 1e-11, "coarsest_dofs": 300, "precision": "float64"}
-    warm = CovarianceSimp(domain, cov, volume_fraction=0.3, filter_radius=1.5, move=0.2, multigrid=settings, warm_start=True)
+    loop = CovarianceSimp(domain, cov, volume_fraction=0.3, filter_radius=1.5, move=0.2, multigrid=settings, warm_start=warm)
     cold = CovarianceSimp(domain, cov, volume_fraction=0.3, filter_radius=1.5, move=0.2, multigrid=settings)
-    x, history = warm.run(4)
+    x, history = loop.run(4)
     _, cold_history = cold.run(4)
-    expected = oracle_loop(warm.system, warm.model, shape, 4, 0.3, 1.5, 3.0, 1e-9, 0.2)
+    expected = oracle_loop(loop.system, loop.model, shape, 4, 0.3, 1.5, 3.0, 1e-9, 0.2)
     for it, (row, (xo, tr)) in enumerate(zip(history, expected)):
         assert row["tr"] == pytest.approx(tr, rel=1e-6), it
     assert np.max(np.abs(x.cpu().numpy() - expected[-1][0])) < 1e-4
     assert sum(max(r["pcg_iterations"]) for r in history[1:]) <= sum(max(r["pcg_iterations"]) for r in cold_history[1:])
-    warm.close()
+    loop.close()
     cold.close()
 
 
