@@ -23,6 +23,8 @@ SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_
             "tf_filter_destroy",
             "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error", "tf_simp",
             "tf_chol_create", "tf_chol_factor_csr", "tf_chol_solve", "tf_chol_destroy", "tf_chol_last_error")
+SYMBOLS += ("tf_nn_last_error", "tf_nn_gemm", "tf_nn_im2col", "tf_nn_col2im", "tf_nn_bias_act", "tf_nn_act_back", "tf_nn_pool",
+            "tf_nn_resample", "tf_nn_mse", "tf_nn_mse_scratch_doubles", "tf_nn_adam")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
 
 
@@ -118,11 +120,23 @@ def load():
             "tf_chol_solve": [P, P, I32, P, P],
             "tf_chol_destroy": [P],
             "tf_chol_last_error": [P],
+            "tf_nn_last_error": [],
+            "tf_nn_gemm": [I32, I32, I32, I32, I32, ctypes.c_float, P, I32, P, I32, ctypes.c_float, P, I32, P, I64, P],
+            "tf_nn_im2col": [P, I32, P, P, P],
+            "tf_nn_col2im": [P, I32, P, P, P],
+            "tf_nn_bias_act": [P, P, I32, I64, I32, P],
+            "tf_nn_act_back": [P, P, I32, I64, I32, P, I32, P],
+            "tf_nn_pool": [P, I32, P, P, P, P],
+            "tf_nn_resample": [P, I32, P, P, I32, P, P],
+            "tf_nn_mse": [P, P, P, I64, D, P, P, P, P],
+            "tf_nn_mse_scratch_doubles": [],
+            "tf_nn_adam": [P, P, P, P, I64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, I32, P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
             fn.argtypes = args
             fn.restype = {"tf_last_error": ctypes.c_char_p, "tf_filter_last_error": ctypes.c_char_p, "tf_mma_last_error": ctypes.c_char_p, "tf_chol_last_error": ctypes.c_char_p,
+                          "tf_nn_last_error": ctypes.c_char_p, "tf_nn_mse_scratch_doubles": ctypes.c_int64,
                           "tf_gram_scratch_size": ctypes.c_int64, "tf_launch_count": ctypes.c_int64}.get(name, ctypes.c_int)
         _lib = lib
         return lib

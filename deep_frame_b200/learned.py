@@ -1,0 +1,217 @@
+"""Learned initial guess for the covariance solves: a small 3-D convolutional encoder / decoder.
+
+The network maps, per load column, the node fields (load f scaled by max|f|, log10 of the node
+stiffness, live mask) to the shape of the displacement u (the target is u / rms(u)); the scale of
+the guess is then fixed by one operator apply, x0 = alpha y with alpha = (y . f) / (y . K y), the
+energy-optimal multiple of the prediction.  It is trained on (density, load, displacement) snapshots
+the solver itself produces along SIMP trajectories and judged by the iterations GMG-PCG needs from
+its guess to the same tolerance; ``GuessPolicy`` drops it whenever it does not reduce them.
+
+Layers (channel-major FP32 node grids, every kernel in libtfb200.so, deterministic):
+  level 0: conv 5->c0, conv c0->c0          level 1 (pool): conv c0->c1, conv c1->c1
+  level 2 (pool): conv c1->c2, conv c2->c2   up + concat(level 1): conv (c2+c1)->c1
+  up + concat(level 0): conv (c1+c0)->c0, conv c0->3 (linear)
+Convolutions are 3 x 3 x 3 with zero padding (im2col + SGEMM), ReLU after every hidden layer.
+The reference has no counterpart: this is the learned part of the B200 design.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+IN_CHANNELS = 5
+
+
+def _shape3(shape):
+    return (ctypes.c_int32 * 3)(*[int(s) for s in shape])
+
+
+def _half(shape):
+    return tuple((int(s) + 1) // 2 for s in shape)
+
+
+class GuessNet:
+    def __init__(self, channels=(8, 16, 32), seed=0, device="cuda"):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        self.lib = _lib.load()
+        c0, c1, c2 = channels
+        self.channels = tuple(channels)
+        # (cin, cout, relu) in execution order
+        self.specs = [(IN_CHANNELS, c0, 1), (c0, c0, 1), (c0, c1, 1), (c1, c1, 1), (c1, c2, 1), (c2, c2, 1),
+                      (c2 + c1, c1, 1), (c1 + c0, c0, 1), (c0, 3, 0)]
+        rng = np.random.default_rng(seed)
+        self.params = []
+        for cin, cout, relu in self.specs:
+            scale = np.sqrt((2.0 if relu else 1.0) / (cin * 27))
+            w = torch.as_tensor(rng.normal(0.0, scale, (cout, cin * 27)).astype(np.float32), device=self.device)
+            b = torch.zeros(cout, dtype=torch.float32, device=self.device)
+            self.params.append([w, b])
+        self.grads = [[torch.zeros_like(w), torch.zeros_like(b)] for w, b in self.params]
+        self.moments = [[(torch.zeros_like(w), torch.zeros_like(w)), (torch.zeros_like(b), torch.zeros_like(b))] for w, b in self.params]
+        self.step_count = 0
+        self.work = torch.empty(0, dtype=torch.float32, device=self.device)
+        self.mse_scratch = torch.zeros(int(self.lib.tf_nn_mse_scratch_doubles()) + 1, dtype=torch.float64, device=self.device)
+
+    # ------------------------------------------------------------ plumbing --
+    def _stream(self):
+        return _lib.stream_of(self.device)
+
+    def _check(self, status, what):
+        if status:
+            message = (self.lib.tf_nn_last_error() or b"").decode()
+            if status == 1:
+                raise ValueError(f"{what} failed: {message}")
+            raise _lib.TfError(status, f"{what} failed: {message}")
+
+    def _gemm(self, ta, tb, m, n, k, a, lda, b, ldb, c, ldc, beta=0.0):
+        need = 64 * m * n
+        if self.work.numel() < need:
+            self.work = self.torch.empty(need, dtype=self.torch.float32, device=self.device)
+        self._check(self.lib.tf_nn_gemm(ta, tb, m, n, k, 1.0, _lib.ptr(a), lda, _lib.ptr(b), ldb, float(beta), _lib.ptr(c), ldc,
+                                        _lib.ptr(self.work), self.work.numel(), self._stream()), "tf_nn_gemm")
+
+    def _conv(self, index, x, shape, cache):
+        torch = self.torch
+        cin, cout, relu = self.specs[index]
+        w, b = self.params[index]
+        n = int(np.prod(shape))
+        col = torch.empty((cin * 27, n), dtype=torch.float32, device=self.device)
+        self._check(self.lib.tf_nn_im2col(_lib.ptr(x), cin, _shape3(shape), _lib.ptr(col), self._stream()), "tf_nn_im2col")
+        y = torch.empty((cout, n), dtype=torch.float32, device=self.device)
+        self._gemm(0, 0, cout, n, cin * 27, w, cin * 27, col, n, y, n)
+        self._check(self.lib.tf_nn_bias_act(_lib.ptr(y), _lib.ptr(b), cout, n, relu, self._stream()), "tf_nn_bias_act")
+        if cache is not None:
+            cache[index] = (col, y, shape)
+        return y
+
+    def _conv_back(self, index, dy, cache, accumulate):
+        """dy: gradient w.r.t. this layer's output (modified in place); returns the input gradient."""
+        torch = self.torch
+        cin, cout, relu = self.specs[index]
+        w, _ = self.params[index]
+        gw, gb = self.grads[index]
+        col, y, shape = cache[index]
+        n = int(np.prod(shape))
+        self._check(self.lib.tf_nn_act_back(_lib.ptr(dy), _lib.ptr(y), cout, n, relu, _lib.ptr(gb), 1 if accumulate else 0, self._stream()),
+                    "tf_nn_act_back")
+        self._gemm(0, 1, cout, cin * 27, n, dy, n, col, n, gw, cin * 27, beta=1.0 if accumulate else 0.0)
+        dcol = torch.empty((cin * 27, n), dtype=torch.float32, device=self.device)
+        self._gemm(1, 0, cin * 27, n, cout, w, cin * 27, dy, n, dcol, n)
+        dx = torch.empty((cin, n), dtype=torch.float32, device=self.device)
+        self._check(self.lib.tf_nn_col2im(_lib.ptr(dcol), cin, _shape3(shape), _lib.ptr(dx), self._stream()), "tf_nn_col2im")
+        return dx
+
+    def _pool(self, x, channels, fine):
+        coarse = _half(fine)
+        out = self.torch.empty((channels, int(np.prod(coarse))), dtype=self.torch.float32, device=self.device)
+        self._check(self.lib.tf_nn_pool(_lib.ptr(x), channels, _shape3(fine), _shape3(coarse), _lib.ptr(out), self._stream()), "tf_nn_pool")
+        return out
+
+    def _resample(self, x, channels, fine, mode):
+        coarse = _half(fine)
+        n = int(np.prod(coarse if mode == 2 else fine))
+        out = self.torch.empty((channels, n), dtype=self.torch.float32, device=self.device)
+        self._check(self.lib.tf_nn_resample(_lib.ptr(x), channels, _shape3(fine), _shape3(coarse), mode, _lib.ptr(out), self._stream()),
+                    "tf_nn_resample")
+        return out
+
+    # ------------------------------------------------------------- network --
+    def forward(self, x, shape, cache=None):
+        """x: [5, n] FP32 features on the node grid `shape`; returns [3, n]."""
+        torch = self.torch
+        c0, c1, c2 = self.channels
+        s0 = tuple(int(s) for s in shape)
+        s1 = _half(s0)
+        s2 = _half(s1)
+        e0 = self._conv(1, self._conv(0, x.contiguous(), s0, cache), s0, cache)
+        e1 = self._conv(3, self._conv(2, self._pool(e0, c0, s0), s1, cache), s1, cache)
+        e2 = self._conv(5, self._conv(4, self._pool(e1, c1, s1), s2, cache), s2, cache)
+        d1 = self._conv(6, torch.cat([self._resample(e2, c2, s1, 0), e1]).contiguous(), s1, cache)
+        d0 = self._conv(7, torch.cat([self._resample(d1, c1, s0, 0), e0]).contiguous(), s0, cache)
+        return self._conv(8, d0, s0, cache)
+
+    def backward(self, dy, shape, cache, accumulate):
+        """Gradients of all parameters (added to the stored ones when accumulate) from dy = dL/d output."""
+        c0, c1, c2 = self.channels
+        s0 = tuple(int(s) for s in shape)
+        s1 = _half(s0)
+        dd0 = self._conv_back(8, dy.contiguous(), cache, accumulate)
+        dcat0 = self._conv_back(7, dd0, cache, accumulate)
+        dd1 = self._resample(dcat0[:c1].contiguous(), c1, s0, 2)
+        de0 = dcat0[c1:].clone()
+        dcat1 = self._conv_back(6, dd1, cache, accumulate)
+        de2 = self._resample(dcat1[:c2].contiguous(), c2, s1, 2)
+        de1 = dcat1[c2:].clone()
+        dp2 = self._conv_back(4, self._conv_back(5, de2, cache, accumulate), cache, accumulate)
+        de1 += self._resample(dp2, c1, s1, 1)
+        dp1 = self._conv_back(2, self._conv_back(3, de1, cache, accumulate), cache, accumulate)
+        de0 += self._resample(dp1, c0, s0, 1)
+        self._conv_back(0, self._conv_back(1, de0, cache, accumulate), cache, accumulate)
+
+    def loss(self, y, target, weight=None, want_grad=True):
+        """Mean squared error over the weighted entries; returns (loss tensor [1] FP64, dL/dy or None)."""
+        torch = self.torch
+        count = float(weight.sum()) if weight is not None else float(y.numel())
+        dy = torch.empty_like(y) if want_grad else None
+        out = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self._check(self.lib.tf_nn_mse(_lib.ptr(y), _lib.ptr(target), _lib.ptr(weight), y.numel(), max(count, 1.0), _lib.ptr(dy),
+                                       _lib.ptr(self.mse_scratch), _lib.ptr(out), self._stream()), "tf_nn_mse")
+        return out, dy
+
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, scale=1.0):
+        """One Adam step on the stored gradients (multiplied by `scale`, e.g. 1 / batch size)."""
+        self.step_count += 1
+        for (p_w, p_b), (g_w, g_b), ((m_w, v_w), (m_b, v_b)) in zip(self.params, self.grads, self.moments):
+            for p, g, m, v in ((p_w, g_w, m_w, v_w), (p_b, g_b, m_b, v_b)):
+                if scale != 1.0:
+                    g.mul_(scale)
+                self._check(self.lib.tf_nn_adam(_lib.ptr(p), _lib.ptr(g), _lib.ptr(m), _lib.ptr(v), p.numel(), lr, beta1, beta2, eps,
+                                                self.step_count, self._stream()), "tf_nn_adam")
+
+    def state(self):
+        return [(w.cpu().numpy(), b.cpu().numpy()) for w, b in self.params]
+
+
+# ------------------------------------------------------------------ features --
+def node_stiffness(moduli, shape):
+    """log10 of the mean modulus of the (up to 8) elements around every node, scaled to about [-1, 0]."""
+    e = np.asarray(moduli, dtype=float).reshape(shape)
+    nodes = tuple(s + 1 for s in shape)
+    total, count = np.zeros(nodes), np.zeros(nodes)
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                total[dx:dx + shape[0], dy:dy + shape[1], dz:dz + shape[2]] += e
+                count[dx:dx + shape[0], dy:dy + shape[1], dz:dz + shape[2]] += 1
+    return np.log10(np.maximum(total / np.maximum(count, 1), 1e-12)) / 9.0
+
+
+def features(force, stiffness, live):
+    """[5, n] FP32: force / max|force| (3 channels, dof = 3 node + comp), node stiffness, node live flag."""
+    f = np.asarray(force, dtype=float).reshape(-1, 3)
+    scale = max(np.abs(f).max(), 1e-300)
+    x = np.concatenate([(f / scale).T, stiffness.reshape(1, -1), live.reshape(1, -1)], axis=0)
+    return x.astype(np.float32), scale
+
+
+def target(u):
+    """u / rms(u) as [3, n] FP32 and the rms."""
+    v = np.asarray(u, dtype=float).reshape(-1, 3)
+    rms = max(float(np.sqrt(np.mean(v ** 2))), 1e-300)
+    return (v / rms).T.astype(np.float32), rms
+
+
+class GuessPolicy:
+    """Use the network's guess only while it saves PCG iterations over the comparison start."""
+
+    def __init__(self, net):
+        self.net, self.enabled, self.record = net, True, []
+
+    def judge(self, iterations_with, iterations_without):
+        self.record.append((int(iterations_with), int(iterations_without)))
+        if iterations_with >= iterations_without:
+            self.enabled = False
+        return self.enabled

@@ -233,6 +233,38 @@ TF_API int tf_filter_destroy(tf_filter* f);
 TF_API const char* tf_filter_last_error(const tf_filter* f);
 
 /* ------------------------------------------------------------------------------------
+ * Learned initial guess (no counterpart in the reference: the small convolutional
+ * network that maps (density, load) to a displacement guess for PCG).  Layers of a 3-D
+ * encoder / decoder on channel-major [C][nx][ny][nz] FP32 node grids; every kernel is
+ * deterministic.  Errors: tf_nn_last_error().
+ * ------------------------------------------------------------------------------------ */
+TF_API const char* tf_nn_last_error(void);
+/* C = alpha op(A) op(B) + beta C (row-major; op = transpose when trans* != 0), split over K with
+ * partial tiles in `work` (>= m * n floats, up to 64 * m * n used) summed in a fixed order. */
+TF_API int tf_nn_gemm(int32_t transa, int32_t transb, int32_t m, int32_t n, int32_t k, float alpha, const float* a, int32_t lda,
+                      const float* b, int32_t ldb, float beta, float* c, int32_t ldc, float* work, int64_t work_floats, void* stream);
+/* col[(c * 27 + tap)][v] = in[c][v + offset(tap)], 3 x 3 x 3 taps, zero outside; col2im is its adjoint. */
+TF_API int tf_nn_im2col(const float* in, int32_t channels, const int32_t shape[3], float* col, void* stream);
+TF_API int tf_nn_col2im(const float* col, int32_t channels, const int32_t shape[3], float* out, void* stream);
+/* x = act(x + bias[c]) in place (relu != 0: max(., 0)); act_back: dy *= (y > 0) for relu, dbias (+)= sum over voxels. */
+TF_API int tf_nn_bias_act(float* x, const float* bias, int32_t channels, int64_t n, int32_t relu, void* stream);
+TF_API int tf_nn_act_back(float* dy, const float* y, int32_t channels, int64_t n, int32_t relu, float* dbias, int32_t accumulate,
+                          void* stream);
+/* 2 x 2 x 2 average pooling (coarse extent = ceil(fine / 2)); resample mode 0 = nearest upsampling,
+ * 1 = pooling adjoint, 2 = upsampling adjoint. */
+TF_API int tf_nn_pool(const float* in, int32_t channels, const int32_t fine[3], const int32_t coarse[3], float* out, void* stream);
+TF_API int tf_nn_resample(const float* in, int32_t channels, const int32_t fine[3], const int32_t coarse[3], int32_t mode, float* out,
+                          void* stream);
+/* *loss_dev = sum w (y - t)^2 / count, dy = its gradient (dy may be NULL; w may be NULL = 1); scratch holds
+ * tf_nn_mse_scratch_doubles() doubles. */
+TF_API int tf_nn_mse(const float* y, const float* target, const float* weight, int64_t n, double count, float* dy, double* scratch,
+                     double* loss_dev, void* stream);
+TF_API int64_t tf_nn_mse_scratch_doubles(void);
+/* Adam with bias correction (step counts from 1). */
+TF_API int tf_nn_adam(float* param, const float* grad, float* m, float* v, int64_t n, float lr, float beta1, float beta2, float eps,
+                      int32_t step, void* stream);
+
+/* ------------------------------------------------------------------------------------
  * Method of moving asymptotes (mmapy.mmasub as called from
  * deep_frame/topology_optimizers.py:61-63): asymptotes, move limits, convex
  * approximation and the primal-dual interior-point subproblem, n variables on the
