@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tensor-cores", action="store_true", help="FP32 finest-level V-cycle apply on tcgen05 (TF32)")
+    ap.add_argument("--learned", action="store_true", help="train the learned initial guess and report PCG with / without it")
     ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
     ap.add_argument("--simp-compare", action="store_true", help="also run the plain FP64 V-cycle and compare the designs")
     ap.add_argument("--warm-start", type=int, default=0, nargs="?", const=-1,
@@ -365,8 +366,54 @@ def simp(args):
     print(json.dumps(line))
 
 
+def learned_guess(args):
+    """--learned: train the convolutional initial guess on SIMP snapshots of a 48 x 48 x 8 plate (seed 0),
+    then time one covariance solve (2 x 42 columns to 1e-8) from zero and from the network's guess
+    (inference included) on held-out densities: a later design of a seed-1 trajectory at the training
+    size, the seeded 96 x 96 x 16 plate density and the seeded 192 x 192 x 32 plate density."""
+    import torch
+    from deep_frame_b200 import learned, problems
+    settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5}
+    train_shape = (48, 48, 8)
+    domain, _, cov = problems.plate(train_shape, 0)
+    t0 = time.perf_counter()
+    snapshots, live, grid = learned.record_trajectory(domain, cov, 16, multigrid=settings)
+    record_s = time.perf_counter() - t0
+    net = learned.GuessNet(channels=(8, 16, 32), seed=0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = learned.train(net, snapshots, live, grid, epochs=6, batch=8, lr=2e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    cases = {}
+    held_domain, _, held_cov = problems.plate(train_shape, 1)
+    held, _, _ = learned.record_trajectory(held_domain, held_cov, 12, multigrid=settings)
+    cases["plate_48x48x8_seed1_design12"] = learned.compare(net, held_domain, held_cov, held[-1][0], multigrid=settings)
+    for shape in ((96, 96, 16), (192, 192, 32)):
+        dom, density, cv = problems.plate(shape, 0)
+        from deep_frame_b200.elasticity import HexElasticity
+        moduli = HexElasticity(dom, multigrid=settings).moduli(density, 3.0, 1e-9)[0]
+        cases["plate_%dx%dx%d" % shape] = learned.compare(net, dom, cv, moduli, multigrid=settings)
+    policy = learned.GuessPolicy(net)
+    for row in cases.values():
+        policy.judge(row["network"]["mean_iterations"], row["zero"]["mean_iterations"])
+    line = {"metric": "PCG iterations / seconds to 1e-8 with and without the learned initial guess", "unit": "iterations",
+            "n_gpus": 1, "data": "synthetic (SIMP trajectory snapshots of seeded plates)",
+            "config": {"network": "3-level conv encoder/decoder, channels (8, 16, 32), 9 conv layers, FP32, hand-written kernels",
+                       "training": {"shape": list(train_shape), "designs": len(snapshots), "samples": int(sum(1 for _ in learned.samples(snapshots, live, grid))),
+                                    "epochs": 6, "losses": [round(v, 5) for v in losses], "record_s": round(record_s, 2), "train_s": round(train_s, 2)},
+                       "solver": settings},
+            "cases": {name: {label: {k: (round(v, 4) if isinstance(v, float) else v) for k, v in row[label].items() if k != "iterations"}
+                             for label in row} for name, row in cases.items()},
+            "network_kept": policy.enabled}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.learned:
+        learned_guess(args)
+        return
     if args.impl == "reference":
         reference(args)
         return

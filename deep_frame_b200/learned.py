@@ -215,3 +215,134 @@ class GuessPolicy:
         if iterations_with >= iterations_without:
             self.enabled = False
         return self.enabled
+
+
+# ------------------------------------------------------------ training data --
+def record_trajectory(domain, covariance, iterations, multigrid=None, device="cuda", keep=None):
+    """Run the covariance SIMP + MMA loop and keep, per iteration, the element moduli and every group's
+    (forces, displacements) on the host: [(moduli, {key: (forces [R, ndof], u [R, ndof])})]."""
+    from .optimize import CovarianceSimp
+    loop = CovarianceSimp(domain, covariance, volume_fraction=0.15, filter_radius=1.5, move=0.2,
+                          multigrid={**(multigrid or {}), "device": str(device)})
+    snapshots = []
+    original = loop.model.solve_all
+
+    def solve_and_keep(initial=None):
+        solved = original(initial)
+        groups = {key: (forces.cpu().numpy(), u.cpu().numpy()) for key, _, forces, u, _ in solved}
+        snapshots.append((loop.moduli.cpu().numpy().copy(), groups))
+        return solved
+
+    loop.model.solve_all = solve_and_keep
+    try:
+        loop.run(iterations)
+    finally:
+        loop.model.solve_all = original
+    system = loop.system
+    live = {key: _live_nodes(system, key) for key in system.groups}
+    loop.close()
+    return snapshots, live, system.shape
+
+
+def _live_nodes(system, key):
+    """Per node: 1 where any dof is free in fixture group `key`, and the [3, n] dof mask."""
+    free = np.zeros(system.ndof, dtype=np.float32)
+    free[system.groups[key][0][1]["free"]] = 1.0
+    dofs = free.reshape(-1, 3)
+    return dofs.max(axis=1), dofs.T.copy()
+
+
+def samples(snapshots, live, shape):
+    """Yield (x [5, n], target [3, n], weight [3, n]) FP32 for every column of every snapshot."""
+    for moduli, groups in snapshots:
+        stiffness = node_stiffness(moduli, shape)
+        for key, (forces, u) in groups.items():
+            node_live, dof_live = live[key]
+            for j in range(forces.shape[0]):
+                if not np.any(forces[j]):
+                    continue
+                x, _ = features(forces[j], stiffness, node_live)
+                t, _ = target(u[j])
+                yield x, t, dof_live
+
+
+def train(net, snapshots, live, shape, epochs=6, batch=8, lr=2e-3, seed=0):
+    """Adam on the mean squared error of u / rms(u); returns the mean loss of every epoch."""
+    torch = net.torch
+    data = [tuple(torch.as_tensor(a, device=net.device) for a in item) for item in samples(snapshots, live, shape)]
+    order = np.random.default_rng(seed).permutation(len(data))
+    node_shape = tuple(s + 1 for s in shape)
+    history = []
+    for epoch in range(epochs):
+        total, seen = 0.0, 0
+        for start in range(0, len(order), batch):
+            chunk = order[start:start + batch]
+            losses = []
+            for position, index in enumerate(chunk):
+                x, t, w = data[index]
+                cache = {}
+                y = net.forward(x, node_shape, cache)
+                loss, dy = net.loss(y, t, w)
+                net.backward(dy, node_shape, cache, accumulate=position > 0)
+                losses.append(loss)
+            net.adam(lr=lr, scale=1.0 / len(chunk))
+            total += float(torch.cat(losses).sum())
+            seen += len(chunk)
+        history.append(total / max(seen, 1))
+        order = np.random.default_rng(seed + epoch + 1).permutation(len(data))
+    return history
+
+
+def predict(net, multigrid, key, fixed, forces, moduli, shape, live):
+    """Initial guesses [R, ndof] FP64 for a group's force block: the network's shape, scaled per column
+    to the energy-optimal multiple (one masked operator apply for all columns)."""
+    torch = net.torch
+    stiffness = node_stiffness(moduli, shape)
+    node_live, dof_live = live
+    node_shape = tuple(s + 1 for s in shape)
+    host = forces.cpu().numpy()
+    shapes = np.zeros_like(host)
+    for j in range(host.shape[0]):
+        if not np.any(host[j]):
+            continue
+        x, _ = features(host[j], stiffness, node_live)
+        y = net.forward(torch.as_tensor(x, device=net.device), node_shape).cpu().numpy()
+        shapes[j] = (y * dof_live).T.reshape(-1)
+    guess = torch.as_tensor(shapes, dtype=torch.float64, device=forces.device)
+    applied = multigrid.apply_device(guess.contiguous(), key, fixed)
+    energy = (guess * applied).sum(1)
+    work = (guess * forces).sum(1)
+    alpha = torch.where(energy > 0, work / energy.clamp_min(1e-300), torch.zeros_like(energy))
+    return (alpha[:, None] * guess).contiguous()
+
+
+def compare(net, domain, covariance, design_moduli, multigrid=None, device="cuda"):
+    """PCG iterations and seconds of one covariance solve (both halves) from zero and from the network's
+    guess (inference included), for the element moduli `design_moduli`."""
+    import time
+    import torch
+    from .covariance import InterfaceCovariance
+    from .elasticity import HexElasticity
+    system = HexElasticity(domain, multigrid={**(multigrid or {}), "device": str(device)})
+    model = InterfaceCovariance(system, covariance, domain["interfaces"])
+    mg = system._multigrid()
+    mg.update_device(torch.as_tensor(design_moduli, device=device))
+    out = {"zero": {"iterations": [], "seconds": 0.0}, "network": {"iterations": [], "seconds": 0.0}}
+    for key, _, forces in model.groups():     # hierarchy set-up outside the timings
+        system.solve_group_device(key, forces)
+    for label in ("zero", "network"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for key, _, forces in model.groups():
+            fixed = system.groups[key][0][1]["fixed"]
+            guess = None if label == "zero" else predict(net, mg, key, fixed, forces, design_moduli, system.shape, _live_nodes(system, key))
+            _, report = system.solve_group_device(key, forces, initial=guess)
+            out[label]["iterations"] += report["iterations"]
+        torch.cuda.synchronize()
+        out[label]["seconds"] = time.perf_counter() - t0
+    system.close()
+    for label in out:
+        its = [i for i in out[label]["iterations"] if i > 0]
+        out[label]["mean_iterations"] = float(np.mean(its)) if its else 0.0
+        out[label]["max_iterations"] = int(max(its)) if its else 0
+    return out

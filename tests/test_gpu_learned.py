@@ -56,3 +56,21 @@ def test_adam_steps_reduce_the_loss(cuda):
         net.backward(dy, shape, cache, accumulate=False)
         net.adam(lr=3e-3)
     assert losses[-1] < 0.7 * losses[0]
+
+
+def test_trajectory_training_and_guess_pipeline(cuda):
+    """Snapshots from a short SIMP trajectory train the network; PCG from its guess reaches the same tolerance."""
+    from deep_frame_b200 import learned, problems
+    shape = (24, 24, 6)
+    domain, _, cov = problems.plate(shape, 0)
+    settings = {"coarsest_dofs": 2000, "tolerance": 1e-8}
+    snapshots, live, grid = learned.record_trajectory(domain, cov, 4, multigrid=settings)
+    assert len(snapshots) == 4 and grid == shape
+    net = learned.GuessNet(channels=(4, 8, 8), seed=0)
+    history = learned.train(net, snapshots[:3], live, grid, epochs=2, batch=8)
+    assert len(history) == 2 and all(np.isfinite(history))
+    result = learned.compare(net, domain, cov, snapshots[3][0], multigrid=settings)
+    assert result["zero"]["mean_iterations"] > 0 and result["network"]["mean_iterations"] > 0
+    policy = learned.GuessPolicy(net)
+    kept = policy.judge(result["network"]["mean_iterations"], result["zero"]["mean_iterations"])
+    assert kept == (result["network"]["mean_iterations"] < result["zero"]["mean_iterations"])
