@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tensor-cores", action="store_true", help="FP32 finest-level V-cycle apply on tcgen05 (TF32)")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="solve N independent seeded plates of uneven size and RHS count concurrently and report solves/s")
     ap.add_argument("--learned", action="store_true", help="train the learned initial guess and report PCG with / without it")
     ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
     ap.add_argument("--simp-compare", action="store_true", help="also run the plain FP64 V-cycle and compare the designs")
@@ -366,6 +368,81 @@ def simp(args):
     print(json.dumps(line))
 
 
+def instances(args):
+    """--instances N: N independent seeded plate instances (grids from 64 x 64 x 12 to 160 x 160 x 24,
+    6 to 42 load columns per half), each with its own solver handle and CUDA stream on its own host
+    thread, solved concurrently to 1e-8.  After one untimed round (buffers, hierarchies, constant
+    slots) the wall time of one concurrent round gives solves/s (one solve = all columns of both
+    halves of one instance) and column solves/s."""
+    import threading
+    import torch
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    rng = np.random.default_rng(2026)
+    sizes = [(64, 64, 12), (80, 80, 12), (96, 96, 16), (112, 112, 16), (128, 128, 16), (128, 128, 24), (144, 144, 24), (160, 160, 24)]
+    specs = []
+    for i in range(args.instances):
+        shape = sizes[int(rng.integers(len(sizes)))]
+        specs.append((shape, int(rng.integers(6, 43)), i))
+    settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5}
+    work = []
+    for shape, rhs, seed in specs:
+        domain, density, cov = problems.plate(shape, seed)
+        system = HexElasticity(domain, multigrid=dict(settings))
+        model = InterfaceCovariance(system, cov, domain["interfaces"])
+        moduli = torch.as_tensor(system.moduli(density, 3.0, 1e-9)[0], device="cuda")
+        groups = [(key, forces[:rhs].contiguous()) for key, _, forces in model.groups()]
+        work.append({"system": system, "moduli": moduli, "groups": groups, "stream": torch.cuda.Stream(), "shape": shape, "rhs": rhs})
+    errors = []
+
+    def solve(item):
+        try:
+            with torch.cuda.stream(item["stream"]):
+                mg = item["system"]._multigrid()
+                mg.update_device(item["moduli"])
+                its = []
+                for key, forces in item["groups"]:
+                    _, report = item["system"].solve_group_device(key, forces)
+                    its.append(max(report["iterations"]))
+                item["iterations"] = its
+                item["stream"].synchronize()
+        except Exception as error:          # surfaced after the join
+            errors.append(repr(error))
+
+    def round_():
+        threads = [threading.Thread(target=solve, args=(item,)) for item in work]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    round_()                                  # untimed: allocations, hierarchies, constant slots
+    seconds = round_()
+    if errors:
+        raise RuntimeError("; ".join(errors))
+    columns = sum(2 * item["rhs"] for item in work)
+    serial = 0.0
+    for item in work:                          # the same instances one after another, for comparison
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solve(item)
+        serial += time.perf_counter() - t0
+    line = {"metric": "independent uneven instances: solves/s", "value": round(len(work) / seconds, 4), "unit": "solves/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"instances": [{"shape": list(item["shape"]), "rhs_per_half": item["rhs"], "pcg_iterations": item.get("iterations")}
+                                     for item in work], "tolerance": 1e-8, "concurrency": "one host thread + CUDA stream + solver handle per instance"},
+            "seconds": round(seconds, 4), "column_solves_per_s": round(columns / seconds, 2), "serial_seconds": round(serial, 4),
+            "concurrency_speedup": round(serial / seconds, 3)}
+    for item in work:
+        item["system"].close()
+    print(json.dumps(line))
+
+
 def learned_guess(args):
     """--learned: train the convolutional initial guess on SIMP snapshots of a 48 x 48 x 8 plate (seed 0),
     then time one covariance solve (2 x 42 columns to 1e-8) from zero and from the network's guess
@@ -413,6 +490,9 @@ def main():
     args = parse()
     if args.learned:
         learned_guess(args)
+        return
+    if args.instances:
+        instances(args)
         return
     if args.impl == "reference":
         reference(args)
