@@ -201,55 +201,6 @@ __global__ void __launch_bounds__(256) trinv_row_kernel(const double* L, double*
   }
 }
 
-// C[c][i] = sum_k op(X)[i][k] B[c][k] for a lower-triangular X (op = identity or transpose).
-// Columns of B and C are contiguous ([ncol][n]).  Inactive columns are skipped.
-__global__ void __launch_bounds__(256) trimul_kernel(const double* X, const double* B, double* C, int n, int ncol,
-                                                     int transpose, const int* active, const int* colmap) {
-  // tile: 64 rows x 8 columns, K in chunks of 32
-  __shared__ double As[64][33];
-  __shared__ double Bs[8][33];
-  const int r0 = blockIdx.x * 64;
-  const int c0 = blockIdx.y * 8;
-  const int tr = threadIdx.x / 4;        // 0..63 row in tile
-  const int tc = (threadIdx.x % 4) * 2;  // 0,2,4,6 column pair
-  bool any = false;
-  for (int c = c0; c < min(c0 + 8, ncol); ++c) any |= (!active || active[colmap ? colmap[c] : c]);
-  if (!any) return;
-  double acc0 = 0.0, acc1 = 0.0;
-  // lower-triangular X: row i uses k <= i; X^T row i uses k >= i
-  const int kbeg = transpose ? r0 : 0;
-  const int kend = transpose ? n : min(n, r0 + 64);
-  for (int k0 = (kbeg / 32) * 32; k0 < kend; k0 += 32) {
-    for (int t = threadIdx.x; t < 64 * 32; t += blockDim.x) {
-      // keep the global reads contiguous: k fastest for X, row fastest for X^T
-      const int r = transpose ? t % 64 : t / 32;
-      const int k = transpose ? t / 64 : t % 32;
-      const int i = r0 + r, kk = k0 + k;
-      double v = 0.0;
-      if (i < n && kk < n) v = transpose ? X[(long long)kk * n + i] : X[(long long)i * n + kk];
-      As[r][k] = v;
-    }
-    for (int t = threadIdx.x; t < 8 * 32; t += blockDim.x) {
-      const int c = t / 32, k = t % 32;
-      const int col = c0 + c, kk = k0 + k;
-      Bs[c][k] = (col < ncol && kk < n) ? B[(long long)col * n + kk] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const double a = As[tr][k];
-      acc0 += a * Bs[tc][k];
-      acc1 += a * Bs[tc + 1][k];
-    }
-    __syncthreads();
-  }
-  const int i = r0 + tr;
-  if (i < n) {
-    if (c0 + tc < ncol) C[(long long)(c0 + tc) * n + i] = acc0;
-    if (c0 + tc + 1 < ncol) C[(long long)(c0 + tc + 1) * n + i] = acc1;
-  }
-}
-
 __global__ void symmetrize_kernel(double* A, int n) {
   const long long total = (long long)n * n;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -293,11 +244,83 @@ void dense_trinv(const double* L, double* X, int n, cudaStream_t s) {
   }
 }
 
-void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active,
+// Split-K form of C = op(X) B: CTA (row block rb, K chunk kc, column group) multiplies 32 rows of op(X)
+// restricted to K chunk kc (256 wide) with up to 48 columns of B and stores the partial tile; chunks
+// that lie entirely in the zero triangle of op(X) are skipped.  trimul_sum_kernel adds the partials of
+// every row in chunk order (deterministic) into C.  Balanced over 148 SMs for the coarsest sizes
+// (a few thousand unknowns), where a whole-K row tile would leave most SMs idle.
+constexpr int TM_RB = 32, TM_KCH = 256, TM_KS = 32, TM_CW = 48;
+
+__device__ __forceinline__ bool trimul_chunk_live(int i0, int kc, int transpose) {
+  return transpose ? (kc + 1) * TM_KCH - 1 >= i0 : kc * TM_KCH <= i0 + TM_RB - 1;
+}
+
+__global__ void __launch_bounds__(256) trimul_split_kernel(const double* __restrict__ X, const double* __restrict__ B,
+                                                           double* __restrict__ P, int n, int ncol, int transpose) {
+  __shared__ double Xs[TM_RB][TM_KS + 1];
+  __shared__ double Bs[TM_CW][TM_KS + 1];
+  const int i0 = blockIdx.x * TM_RB, kc = blockIdx.y, c0 = blockIdx.z * TM_CW;
+  if (!trimul_chunk_live(i0, kc, transpose)) return;
+  const int t = threadIdx.x, r = t % TM_RB, cg = t / TM_RB;   // 8 column groups of 6
+  const int k_lo = kc * TM_KCH, k_hi = min(n, k_lo + TM_KCH);
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int k0 = k_lo; k0 < k_hi; k0 += TM_KS) {
+    for (int e = t; e < TM_RB * TM_KS; e += 256) {
+      // contiguous global reads: k fastest for X rows, row fastest for X^T
+      const int rr = transpose ? e % TM_RB : e / TM_KS, kk = transpose ? e / TM_RB : e % TM_KS;
+      const int i = i0 + rr, k = k0 + kk;
+      double v = 0.0;
+      if (i < n && k < k_hi) v = transpose ? X[(long long)k * n + i] : X[(long long)i * n + k];
+      Xs[rr][kk] = v;
+    }
+    for (int e = t; e < TM_CW * TM_KS; e += 256) {
+      const int cc = e / TM_KS, kk = e % TM_KS, col = c0 + cc, k = k0 + kk;
+      Bs[cc][kk] = (col < ncol && k < k_hi) ? B[(long long)col * n + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < TM_KS; ++kk) {
+      const double a = Xs[r][kk];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[q] = fma(a, Bs[cg * 6 + q][kk], acc[q]);
+    }
+    __syncthreads();
+  }
+  const int i = i0 + r;
+  if (i >= n) return;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const int col = c0 + cg * 6 + q;
+    if (col < ncol) P[((long long)kc * ncol + col) * n + i] = acc[q];
+  }
+}
+
+__global__ void trimul_sum_kernel(const double* __restrict__ P, double* __restrict__ C, int n, int ncol, int nchunks, int transpose,
+                                  const int* __restrict__ active) {
+  const long long total = (long long)n * ncol;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+    const int col = static_cast<int>(idx / n), i = static_cast<int>(idx % n);
+    if (active && !active[col]) continue;
+    const int i0 = (i / TM_RB) * TM_RB;
+    double s = 0.0;
+    for (int kc = 0; kc < nchunks; ++kc)
+      if (trimul_chunk_live(i0, kc, transpose)) s += P[((long long)kc * ncol + col) * n + i];
+    C[(long long)col * n + i] = s;
+  }
+}
+
+size_t dense_trimul_work(int n, int ncol) {
+  return sizeof(double) * (size_t)((n + TM_KCH - 1) / TM_KCH) * ncol * (size_t)n;
+}
+
+void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active, double* work,
                   cudaStream_t s) {
-  dim3 grid((n + 63) / 64, (ncol + 7) / 8);
-  trimul_kernel<<<grid, 256, 0, s>>>(X, B, C, n, ncol, transpose, active, nullptr);
-  TF_LAUNCH_CHECK("trimul_kernel");
+  const int nchunks = (n + TM_KCH - 1) / TM_KCH;
+  dim3 grid((n + TM_RB - 1) / TM_RB, nchunks, (ncol + TM_CW - 1) / TM_CW);
+  trimul_split_kernel<<<grid, 256, 0, s>>>(X, B, work, n, ncol, transpose);
+  TF_LAUNCH_CHECK("trimul_split_kernel");
+  trimul_sum_kernel<<<grid_for((long long)n * ncol, 256), 256, 0, s>>>(work, C, n, ncol, nchunks, transpose, active);
+  TF_LAUNCH_CHECK("trimul_sum_kernel");
 }
 
 }  // namespace tfb
@@ -308,6 +331,7 @@ void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, 
 // the CSR matrix is scattered into a dense n x n array, symmetrised, factored
 // (A = L L^T), and L is inverted once; each solve is x = L^-T (L^-1 b).
 // ---------------------------------------------------------------------------
+#include <algorithm>
 #include <string>
 #include "tf_b200.h"
 
@@ -326,7 +350,7 @@ __global__ void csr_to_dense_kernel(int n, const int32_t* __restrict__ indptr, c
 
 struct tf_chol {
   int n = 0;
-  tfb::DevBuf A, X, tmp, info;
+  tfb::DevBuf A, X, tmp, info, work;
   bool factored = false;
   std::string err;
 };
@@ -399,8 +423,9 @@ extern "C" int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, doub
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t need = sizeof(double) * (size_t)h->n * nrhs;
     if (h->tmp.bytes < need) h->tmp.alloc(need);
-    tfb::dense_trimul(h->X.as<double>(), b_dev, h->tmp.as<double>(), h->n, nrhs, 0, nullptr, s);
-    tfb::dense_trimul(h->X.as<double>(), h->tmp.as<double>(), x_dev, h->n, nrhs, 1, nullptr, s);
+    h->work.ensure(std::max(h->work.bytes, tfb::dense_trimul_work(h->n, nrhs)));
+    tfb::dense_trimul(h->X.as<double>(), b_dev, h->tmp.as<double>(), h->n, nrhs, 0, nullptr, h->work.as<double>(), s);
+    tfb::dense_trimul(h->X.as<double>(), h->tmp.as<double>(), x_dev, h->n, nrhs, 1, nullptr, h->work.as<double>(), s);
   });
 }
 

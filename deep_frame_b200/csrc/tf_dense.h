@@ -1,5 +1,6 @@
 // Dense FP64 helpers for the coarsest multigrid level.
 #pragma once
+#include <cstddef>
 #include <cuda_runtime.h>
 
 namespace tfb {
@@ -10,6 +11,8 @@ void dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s);
 // X = L^-1 for the lower-triangular factor L (X is lower triangular, upper part zero).
 void dense_trinv(const double* L, double* X, int n, cudaStream_t s);
 // C = op(X) B with X lower triangular, B and C stored as [ncol][n]; op = X or X^T.
-void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active,
+// work: dense_trimul_work(n, ncol) bytes of split-K partials.
+void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active, double* work,
                   cudaStream_t s);
+size_t dense_trimul_work(int n, int ncol);
 }  // namespace tfb

@@ -149,6 +149,7 @@ struct tf_handle {
   bool have_me = false;
   DevBuf mass64, lumped64;  // padded element masses and lumped nodal masses of the last tf_mass_apply
   DevBuf tc_err;            // int: set by the tensor-core finest-level kernel when an MMA wait timed out
+  DevBuf trimul_work;       // split-K partials of the coarsest triangular products
   GalerkinParam W{};
   DevBuf Q, K0dev, k0diag;
   DevBuf moduli_un, moduli64, modulif;
@@ -484,8 +485,10 @@ void coarsest_solve(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int ncol, const i
   dim3 g1 = cols_grid(n, ncol);
   coarsest_gather_kernel<T><<<g1, 256, 0, st>>>(b, nd, hy.live.as<long long>(), n, h->cb.as<double>(), active);
   TF_LAUNCH_CHECK("coarsest_gather_kernel");
-  dense_trimul(hy.X.as<double>(), h->cb.as<double>(), h->cy.as<double>(), n, ncol, 0, active, st);
-  dense_trimul(hy.X.as<double>(), h->cy.as<double>(), h->cb.as<double>(), n, ncol, 1, active, st);
+  const size_t need = dense_trimul_work(n, ncol);
+  if (h->trimul_work.bytes < need) h->trimul_work.alloc(need);
+  dense_trimul(hy.X.as<double>(), h->cb.as<double>(), h->cy.as<double>(), n, ncol, 0, active, h->trimul_work.as<double>(), st);
+  dense_trimul(hy.X.as<double>(), h->cy.as<double>(), h->cb.as<double>(), n, ncol, 1, active, h->trimul_work.as<double>(), st);
   coarsest_scatter_kernel<T><<<g1, 256, 0, st>>>(h->cb.as<double>(), hy.live.as<long long>(), n, x, nd, active);
   TF_LAUNCH_CHECK("coarsest_scatter_kernel");
 }
