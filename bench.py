@@ -158,7 +158,7 @@ def ours(args):
             dist.broadcast_object_list(choice, src=0)
             if rank != 0:
                 tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
-                                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores")}],
+                                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores", "coarsest_dofs")}],
                                               repeats=1)
     mg = system._multigrid()
     measure = ShardedMeasure(groups, model.rank, model.factor, DeviceOps(system))
@@ -209,7 +209,7 @@ def ours(args):
               "iterations_max": [int(np.max(r["iterations"])) for r in timed[-len(groups):]], "clocks": clocks.summary(),
               "world": world, "rank": rank, "columns": [len(g["local"]) for g in measure.groups], "ndof": system.ndof,
               "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in timed),
-              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores")},
+              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores", "coarsest_dofs")},
               "tuning": tuning, "tr": rows[0]["value"], "lambda_max": rows[1]["value"]}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     result["dominant"] = dominant
@@ -533,7 +533,7 @@ def main():
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
                        "outer": "fp64 PCG", "vcycle": args.precision + (" (finest apply: tcgen05 TF32)" if result["smoother"].get("tensor_cores") else ""), "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
                        "pcg_iterations": result["iterations_max"], "smoother": result["smoother"],
-                       "smoother_choice": "autotuned (fastest of 7 schedules / finest-apply units, all to the same tolerance)" if result["tuning"] else "reference default",
+                       "smoother_choice": "autotuned (fastest of 8 schedules / depths / finest-apply units, all to the same tolerance)" if result["tuning"] else "reference default",
                        "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
                        "parallelism": f"rhs-sharded x{result['world']}"},
             "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),

@@ -1,8 +1,8 @@
 """Measured choice of the V-cycle smoother for a given problem.
 
 The smoother schedule (Chebyshev degree, growth of the sweep count per level,
-or damped Jacobi) and the finest-level apply (FP32 CUDA cores or TF32 tensor
-cores) change the cost of a V-cycle and the number of PCG iterations, never
+or damped Jacobi), the depth of the hierarchy and the finest-level apply (FP32
+CUDA cores or TF32 tensor cores) change the cost of a V-cycle and the number of PCG iterations, never
 the converged answer: every candidate solves to the same
 recomputed true relative residual.  ``tune_smoother`` times one full solve of
 every fixture group per candidate on the device and returns the fastest.
@@ -15,6 +15,8 @@ CANDIDATES = (
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5},
     {"smoother": "chebyshev", "chebyshev_degree": 3, "growth": 1.0},
     {"smoother": "jacobi", "sweeps": 2, "growth": 2.0},
+    # one more level (a coarsest grid of a few hundred dofs: cheaper dense factor, longer V-cycle)
+    {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5, "coarsest_dofs": 1200},
     # the same schedules with the finest-level V-cycle apply on the tensor cores (TF32 operands)
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5, "tensor_cores": True},
     {"smoother": "chebyshev", "chebyshev_degree": 3, "growth": 2.0, "tensor_cores": True},
