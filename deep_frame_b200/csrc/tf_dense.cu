@@ -2,202 +2,303 @@
 //
 // The reference factors its coarsest Galerkin matrix with cuDSS (sparse FP64
 // Cholesky, deep_frame/topology_multigrid.py:230-283).  Here the coarsest grid
-// is kept small (a few thousand dofs), factored once per hierarchy by a blocked
-// right-looking Cholesky, and the factor is inverted (X = L^-1).  Every
-// coarsest solve in a V-cycle is then two triangular matrix products,
-// x = X^T (X b), one launch each, instead of 2 * n / NB dependent substitution
-// steps.
+// is kept small (a few thousand dofs) and, once per hierarchy, a blocked
+// right-looking Cholesky and the inversion of its factor (X = L^-1) run
+// together, two launches per 32-wide panel.  Every coarsest solve in a V-cycle
+// is then two triangular matrix products, x = X^T (X b), instead of 2 * n / 32
+// dependent substitution steps.
 #include "tf_common.h"
 #include "tf_dense.h"
 
 namespace tfb {
 
 namespace {
-constexpr int NB = 32;     // panel width
-constexpr int TILE = 64;   // syrk / product tile
+// Blocked Cholesky factorisation fused with the inversion of its factor.  Per 32-wide panel k
+// (rows / columns k0 = 32 k .. k0 + 31) two launches: factor_diag_kernel (one CTA) factors the
+// diagonal block W_kk = L_kk L_kk^T, final after the previous panel's update, and stores
+// Linv_kk = L_kk^-1 in `work`; factor_step_kernel then runs three kinds of CTA:
+//  * trailing tiles (ti >= tj, 64 x 64): L_i = W_ik Linv_kk^T for the tile's two row ranges, then
+//    W_ij -= L_i L_j^T (the Schur complement; W is the input matrix and is overwritten);
+//  * inverse tiles (a row tile below the panel x 64 columns j < k0 + 32): X_k = Linv_kk R_k for
+//    those columns, then R_ij -= L_i X_k.  R lives in the output buffer X; it starts as the identity
+//    and, when panel k runs, block row k of R is the right-hand side of L_kk X_k = R_k;
+//  * finishing tiles: block row k - 1 of R is complete after panel k - 1 and is replaced in place by
+//    X_{k-1} = Linv_{k-1} R_{k-1}.
+// The three kinds read and write disjoint parts of W, X and `work`, so a launch needs no other
+// synchronisation; a last launch finishes the last block row.  L itself is never stored: the
+// coarsest solve only uses X = L^-1 (x = X^T X b).
+constexpr int FB = 32;       // panel width
+constexpr int FT = 64;       // update tile
+constexpr int FP = FT + 1;   // shared-memory pitch of the K-major operand tiles
+constexpr int F_THREADS = 256;
 
-// Factor the NB x NB diagonal block at (k0, k0) in place (lower).
-__global__ void potrf_diag_kernel(double* A, int n, int k0, int* info) {
-  __shared__ double s[NB][NB + 1];
-  const int nb = min(NB, n - k0);
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t % nb;
-    s[r][c] = A[(long long)(k0 + r) * n + k0 + c];
+struct DiagShared {
+  double L[FB][FB + 1];    // factor of the diagonal block
+  double Li[FB][FB + 1];   // its inverse
+  double col[FB];          // the current column of L
+  double dinv[FB];         // 1 / L_rr
+};
+
+struct FactorShared {
+  double Li[FB][FB + 1];   // inverse of the diagonal factor
+  double A[FB][FP];        // K-major left operand (L_i^T)
+  double B[FB][FP];        // K-major right operand (L_j^T or X_k)
+  double T[FB][FP];        // staging
+};
+
+// CTA counts of the update launch of panel k (the same arithmetic on host and device)
+struct FactorStep {
+  int trailing, syrk, ctiles, upd, lead, finish;
+  __host__ __device__ FactorStep(int n, int k) {
+    const int nblk = (n + FB - 1) / FB;
+    const int k0 = k * FB, start = k0 + FB;
+    trailing = k < nblk ? (max(0, n - start) + FT - 1) / FT : 0;
+    syrk = trailing * (trailing + 1) / 2;
+    ctiles = (min(start, n) + FT - 1) / FT;
+    upd = trailing * ctiles;
+    lead = syrk + upd;
+    finish = k >= 1 ? (min(k0, n) + FT - 1) / FT : 0;
+  }
+};
+
+// Factor and invert the diagonal block at (k0, k0) (rows beyond n padded with the identity) and
+// store Linv in Dk; a non-positive pivot is replaced by 1 and reported as 1 + its global index in
+// *info (when *info is still 0).  One CTA; the elimination itself is one warp.
+__global__ void __launch_bounds__(F_THREADS, 1) factor_diag_kernel(const double* __restrict__ W, int n, int k0,
+                                                                   double* __restrict__ Dk, int* __restrict__ info) {
+  __shared__ DiagShared s;
+  const int nb = min(FB, n - k0);
+  {
+    double v[FB * FB / F_THREADS];
+#pragma unroll
+    for (int q = 0; q < FB * FB / F_THREADS; ++q) {
+      const int e = threadIdx.x + q * F_THREADS, r = e / FB, c = e % FB;
+      v[q] = (r == c) ? 1.0 : 0.0;
+      if (r < nb && c < nb) v[q] = (c <= r) ? W[(long long)(k0 + r) * n + k0 + c] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < FB * FB / F_THREADS; ++q) {
+      const int e = threadIdx.x + q * F_THREADS;
+      s.L[e / FB][e % FB] = v[q];
+    }
   }
   __syncthreads();
-  for (int k = 0; k < nb; ++k) {
-    if (threadIdx.x == 0) {
-      const double d = s[k][k];
-      if (!(d > 0.0)) {
-        if (*info == 0) *info = k0 + k + 1;
-        s[k][k] = 1.0;
-      } else {
-        s[k][k] = sqrt(d);
+  if (threadIdx.x < 32) {
+    // Lane r holds the not yet eliminated part of row r in registers, a[j] = W_r,k+j at pivot k;
+    // the row shifts left by one per pivot so that the pivot loop runs rolled: unrolled, the code
+    // executes once per launch and is bound by instruction fetch.
+    const int lane = threadIdx.x;
+    double a[FB];
+#pragma unroll
+    for (int c = 0; c < FB; ++c) a[c] = s.L[lane][c];
+    int bad = 0;
+#pragma unroll 1
+    for (int k = 0; k < FB; ++k) {
+      double piv = __shfl_sync(0xffffffffu, a[0], k);
+      if (!(piv > 0.0)) {
+        if (bad == 0) bad = k + 1;
+        piv = 1.0;
       }
+      const double rs = rsqrt(piv);
+      const double l = (lane == k) ? piv * rs : a[0] * rs;   // L_rk (rows above k: unused)
+      if (lane == k) s.dinv[k] = rs;
+      if (lane >= k) s.L[lane][k] = l;
+      s.col[lane] = l;
+      __syncwarp();
+#pragma unroll
+      for (int j = 1; j < FB; ++j) {
+        const int c = k + j;
+        if (c < FB && lane >= c) a[j] = fma(-l, s.col[c], a[j]);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j + 1 < FB; ++j) a[j] = a[j + 1];
+      a[FB - 1] = 0.0;
     }
-    __syncthreads();
-    for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) s[r][k] /= s[k][k];
-    __syncthreads();
-    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-      const int r = t / nb, c = t % nb;
-      if (r > k && c > k && c <= r) s[r][c] -= s[r][k] * s[c][k];
+    __syncwarp();
+    // lane c: column c of L^-1 by right-looking forward substitution (short dependency chain),
+    // v[j] = pending entry t + j, shifted the same way
+    double v[FB];
+#pragma unroll
+    for (int r = 0; r < FB; ++r) v[r] = (r == lane) ? 1.0 : 0.0;
+#pragma unroll 1
+    for (int t = 0; t < FB; ++t) {
+      const double x = v[0] * s.dinv[t];
+      s.Li[t][lane] = x;
+#pragma unroll
+      for (int j = 1; j < FB; ++j) {
+        const int r = t + j;
+        if (r < FB) v[j] = fma(-s.L[r][t], x, v[j]);
+      }
+#pragma unroll
+      for (int j = 0; j + 1 < FB; ++j) v[j] = v[j + 1];
+      v[FB - 1] = 0.0;
     }
-    __syncthreads();
+    if (lane == 0 && bad && *info == 0) *info = k0 + bad;
   }
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t % nb;
-    A[(long long)(k0 + r) * n + k0 + c] = (c <= r) ? s[r][c] : 0.0;
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < FB * FB / F_THREADS; ++q) {
+    const int e = threadIdx.x + q * F_THREADS;
+    Dk[e] = s.Li[e / FB][e % FB];
   }
 }
 
-// Rows below the diagonal block: A[i, k0:k0+nb] <- A[i, k0:k0+nb] L_kk^-T.
-__global__ void trsm_panel_kernel(double* A, int n, int k0) {
-  __shared__ double L[NB][NB + 1];
-  const int nb = min(NB, n - k0);
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t % nb;
-    L[r][c] = A[(long long)(k0 + r) * n + k0 + c];
-  }
-  __syncthreads();
-  for (int i = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double x[NB];
-    double* row = A + (long long)i * n + k0;
+// s.Li <- the 32 x 32 block Dk
+__device__ void load_inverse(const double* __restrict__ Dk, FactorShared& s) {
+  double v[FB * FB / F_THREADS];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) x[c] = (c < nb) ? row[c] : 0.0;
+  for (int q = 0; q < FB * FB / F_THREADS; ++q) v[q] = Dk[threadIdx.x + q * F_THREADS];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) {
-      if (c < nb) {
-        double v = x[c];
-#pragma unroll
-        for (int t = 0; t < NB; ++t)
-          if (t < c) v -= x[t] * L[c][t];
-        x[c] = v / L[c][c];
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-      if (c < nb) row[c] = x[c];
+  for (int q = 0; q < FB * FB / F_THREADS; ++q) {
+    const int e = threadIdx.x + q * F_THREADS;
+    s.Li[e / FB][e % FB] = v[q];
   }
 }
 
-// Trailing update of the lower triangle: A[i][j] -= sum_t P[i][t] P[j][t], i >= j >= k0 + nb.
-__global__ void __launch_bounds__(256) syrk_update_kernel(double* A, int n, int k0) {
-  const int nb = min(NB, n - k0);
-  const int start = k0 + nb;
-  const int m = n - start;
-  const int tiles = (m + TILE - 1) / TILE;
-  // map blockIdx.x to a lower-triangular tile pair (ti >= tj)
-  int b = blockIdx.x, ti = 0;
-  while (b >= ti + 1) { b -= ti + 1; ++ti; }
-  const int tj = b;
-  if (ti >= tiles) return;
-  __shared__ double Pi[TILE][NB + 1];
-  __shared__ double Pj[TILE][NB + 1];
-  const int i0 = start + ti * TILE, j0 = start + tj * TILE;
-  for (int t = threadIdx.x; t < TILE * NB; t += blockDim.x) {
-    const int r = t / NB, c = t % NB;
-    Pi[r][c] = (i0 + r < n && c < nb) ? A[(long long)(i0 + r) * n + k0 + c] : 0.0;
-    Pj[r][c] = (j0 + r < n && c < nb) ? A[(long long)(j0 + r) * n + k0 + c] : 0.0;
+// out = Li T (32 x 64); Li lower triangular.  The finishing and the inverse tiles both form X_k with
+// this routine, so the stored X_k has the bits the updates used.
+__device__ void tri_times(const double (*Li)[FB + 1], const double (*T)[FP], double (*out)[FP]) {
+  const int r0 = 2 * (threadIdx.x / 16), c0 = threadIdx.x % 16;
+  double acc[2][4] = {};
+#pragma unroll 8
+  for (int t = 0; t < FB; ++t) {
+    const double l0 = Li[r0][t], l1 = Li[r0 + 1][t];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double b = T[t][c0 + 16 * q];
+      acc[0][q] = fma(l0, b, acc[0][q]);
+      acc[1][q] = fma(l1, b, acc[1][q]);
+    }
   }
-  __syncthreads();
-  const int tr = (threadIdx.x / 16) * 4, tc = (threadIdx.x % 16) * 4;
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) out[r0 + p][c0 + 16 * q] = acc[p][q];
+}
+
+// T[t][r] <- W[i0 + r][k0 + t]: 64 panel rows below the diagonal block, transposed; 0 beyond n.
+__device__ void load_panel(const double* __restrict__ W, int n, int k0, int i0, double (*T)[FP]) {
+  double v[FT * FB / F_THREADS];
+#pragma unroll
+  for (int q = 0; q < FT * FB / F_THREADS; ++q) {
+    const int e = threadIdx.x + q * F_THREADS, r = e / FB, t = e % FB, i = i0 + r;
+    v[q] = (i < n) ? W[(long long)i * n + k0 + t] : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < FT * FB / F_THREADS; ++q) {
+    const int e = threadIdx.x + q * F_THREADS;
+    T[e % FB][e / FB] = v[q];
+  }
+}
+
+// T[t][c] <- R[k0 + t][j0 + c] for columns below col_end (0 elsewhere).  The diagonal block of R is
+// the identity and is not stored: no update reaches it before its block row is finished.
+__device__ void load_rows(const double* __restrict__ R, int n, int k0, int j0, int col_end, double (*T)[FP]) {
+  double v[FB * FT / F_THREADS];
+#pragma unroll
+  for (int q = 0; q < FB * FT / F_THREADS; ++q) {
+    const int e = threadIdx.x + q * F_THREADS, t = e / FT, c = e % FT, i = k0 + t, j = j0 + c;
+    v[q] = 0.0;
+    if (i < n && j < col_end) v[q] = (j >= k0) ? (j == i ? 1.0 : 0.0) : R[(long long)i * n + j];
+  }
+#pragma unroll
+  for (int q = 0; q < FB * FT / F_THREADS; ++q) {
+    const int e = threadIdx.x + q * F_THREADS;
+    T[e / FT][e % FT] = v[q];
+  }
+}
+
+// C[i0 + r][j0 + c] -= sum_t A[t][r] B[t][c] for rows below n, columns below col_end (and j <= i
+// when `lower`).  The old values of C are fetched before the products so their latency overlaps.
+__device__ void update_tile(double* __restrict__ C, int n, int i0, int j0, int col_end, bool lower, const double (*A)[FP],
+                            const double (*B)[FP]) {
+  const int rr = threadIdx.x / 16, cc = threadIdx.x % 16;
+  double old[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int i = i0 + rr + 16 * p;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = j0 + cc + 16 * q;
+      old[p][q] = (i < n && j < col_end && (!lower || j <= i)) ? C[(long long)i * n + j] : 0.0;
+    }
+  }
   double acc[4][4] = {};
-  for (int t = 0; t < NB; ++t) {
-    double a[4], bb[4];
+#pragma unroll 4
+  for (int t = 0; t < FB; ++t) {
+    double a[4], b[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) { a[q] = Pi[tr + q][t]; bb[q] = Pj[tc + q][t]; }
+    for (int p = 0; p < 4; ++p) a[p] = A[t][rr + 16 * p];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) b[q] = B[t][cc + 16 * q];
 #pragma unroll
     for (int p = 0; p < 4; ++p)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * bb[q];
+      for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
   }
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
-    const int i = i0 + tr + p;
-    if (i >= n) continue;
+    const int i = i0 + rr + 16 * p;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int j = j0 + tc + q;
-      if (j >= n || j > i) continue;
-      A[(long long)i * n + j] -= acc[p][q];
+      const int j = j0 + cc + 16 * q;
+      if (i < n && j < col_end && (!lower || j <= i)) C[(long long)i * n + j] = old[p][q] - acc[p][q];
     }
   }
 }
 
-// Invert every NB x NB lower-triangular diagonal block of L into X.
-__global__ void trinv_diag_kernel(const double* L, double* X, int n) {
-  __shared__ double s[NB][NB + 1];
-  __shared__ double x[NB][NB + 1];
-  const int k0 = blockIdx.x * NB;
-  const int nb = min(NB, n - k0);
-  for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
-    const int r = t / NB, c = t % NB;
-    s[r][c] = (r < nb && c < nb) ? L[(long long)(k0 + r) * n + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  // column c of the inverse by forward substitution (one thread per column)
-  for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-    for (int r = 0; r < nb; ++r) {
-      double v = (r == c) ? 1.0 : 0.0;
-      for (int t = c; t < r; ++t) v -= s[r][t] * x[t][c];
-      x[r][c] = (r < c) ? 0.0 : v / s[r][r];
+__global__ void __launch_bounds__(F_THREADS, 2) factor_step_kernel(double* __restrict__ W, double* __restrict__ X,
+                                                                   const double* __restrict__ D, int n, int k) {
+  extern __shared__ __align__(16) unsigned char f_smem[];
+  FactorShared& s = *reinterpret_cast<FactorShared*>(f_smem);
+  const FactorStep st(n, k);
+  const int k0 = k * FB, start = k0 + FB;
+  const int b = blockIdx.x;
+  if (b >= st.lead) {
+    // finishing tile: X_{k-1} = Linv_{k-1} R_{k-1} for 64 columns
+    const int p0 = k0 - FB, col_end = min(k0, n), j0 = (b - st.lead) * FT;
+    load_inverse(D + (long long)(k - 1) * FB * FB, s);
+    load_rows(X, n, p0, j0, col_end, s.T);
+    __syncthreads();
+    tri_times(s.Li, s.T, s.A);
+    __syncthreads();
+    for (int e = threadIdx.x; e < FB * FT; e += blockDim.x) {
+      const int r = e / FT, c = e % FT, i = p0 + r, j = j0 + c;
+      if (i < n && j < col_end) X[(long long)i * n + j] = s.A[r][c];
     }
+    return;
   }
-  __syncthreads();
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t % nb;
-    X[(long long)(k0 + r) * n + k0 + c] = x[r][c];
-  }
-}
-
-// Block row bi of X = L^-1:  X[bi][bj] = -X[bi][bi] * sum_{bk=bj}^{bi-1} L[bi][bk] X[bk][bj]  (one CTA per bj < bi).
-__global__ void __launch_bounds__(256) trinv_row_kernel(const double* L, double* X, int n, int bi) {
-  const int bj = blockIdx.x;
-  __shared__ double La[NB][NB + 1];
-  __shared__ double Xb[NB][NB + 1];
-  __shared__ double S[NB][NB + 1];
-  const int i0 = bi * NB, j0 = bj * NB;
-  const int ni = min(NB, n - i0);
-  // each thread owns 4 entries of the NB x NB tile
-  double acc[4] = {0, 0, 0, 0};
-  for (int bk = bj; bk < bi; ++bk) {
-    const int k0 = bk * NB;
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
-      const int r = t / NB, c = t % NB;
-      La[r][c] = (r < ni) ? L[(long long)(i0 + r) * n + k0 + c] : 0.0;
-      Xb[r][c] = X[(long long)(k0 + r) * n + j0 + c];
+  load_inverse(D + (long long)k * FB * FB, s);
+  if (b < st.syrk) {
+    int ti = 0, r = b;
+    while (r > ti) {
+      r -= ti + 1;
+      ++ti;
+    }
+    const int tj = r;
+    const int i0 = start + ti * FT, j0 = start + tj * FT;
+    load_panel(W, n, k0, i0, s.T);
+    if (ti != tj) load_panel(W, n, k0, j0, s.B);
+    __syncthreads();
+    tri_times(s.Li, s.T, s.A);
+    if (ti != tj) {
+      __syncthreads();
+      tri_times(s.Li, s.B, s.T);
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int t = threadIdx.x + q * 256;
-      const int r = t / NB, c = t % NB;
-      double v = 0.0;
-#pragma unroll 8
-      for (int kk = 0; kk < NB; ++kk) v += La[r][kk] * Xb[kk][c];
-      acc[q] += v;
-    }
+    update_tile(W, n, i0, j0, n, ti == tj, s.A, ti == tj ? s.A : s.T);
+  } else {
+    const int u = b - st.syrk, ti = u / st.ctiles, tj = u % st.ctiles;
+    const int i0 = start + ti * FT, j0 = tj * FT;
+    load_panel(W, n, k0, i0, s.T);
+    load_rows(X, n, k0, j0, start, s.B);
     __syncthreads();
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int t = threadIdx.x + q * 256;
-    S[t / NB][t % NB] = acc[q];
-  }
-  // diagonal inverse of block bi
-  for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
-    const int r = t / NB, c = t % NB;
-    La[r][c] = (r < ni && c < ni) ? X[(long long)(i0 + r) * n + i0 + c] : 0.0;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int t = threadIdx.x + q * 256;
-    const int r = t / NB, c = t % NB;
-    if (r >= ni) continue;
-    double v = 0.0;
-    for (int kk = 0; kk <= r; ++kk) v += La[r][kk] * S[kk][c];
-    X[(long long)(i0 + r) * n + j0 + c] = -v;
+    tri_times(s.Li, s.T, s.A);
+    __syncthreads();
+    tri_times(s.Li, s.B, s.T);
+    __syncthreads();
+    update_tile(X, n, i0, j0, start, false, s.A, s.T);
   }
 }
 
@@ -219,28 +320,22 @@ void dense_symmetrize(double* A, int n, cudaStream_t s) {
   TF_LAUNCH_CHECK("symmetrize_kernel");
 }
 
-void dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s) {
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    potrf_diag_kernel<<<1, 256, 0, s>>>(A, n, k0, info_dev);
-    TF_LAUNCH_CHECK("potrf_diag_kernel");
-    const int below = n - k0 - NB;
-    if (below <= 0) break;
-    trsm_panel_kernel<<<grid_for(below, 128, 4096), 128, 0, s>>>(A, n, k0);
-    TF_LAUNCH_CHECK("trsm_panel_kernel");
-    const int tiles = (below + TILE - 1) / TILE;
-    syrk_update_kernel<<<tiles * (tiles + 1) / 2, 256, 0, s>>>(A, n, k0);
-    TF_LAUNCH_CHECK("syrk_update_kernel");
-  }
-}
+size_t dense_factor_work(int n) { return sizeof(double) * FB * FB * (size_t)((n + FB - 1) / FB); }
 
-void dense_trinv(const double* L, double* X, int n, cudaStream_t s) {
+void dense_cholesky_inverse(double* A, double* X, int n, int* info_dev, double* work, cudaStream_t s) {
+  const int smem = static_cast<int>(sizeof(FactorShared));
+  TF_CUDA_CHECK(cudaFuncSetAttribute(factor_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   TF_CUDA_CHECK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, s));
-  const int blocks = (n + NB - 1) / NB;
-  trinv_diag_kernel<<<blocks, 64, 0, s>>>(L, X, n);
-  TF_LAUNCH_CHECK("trinv_diag_kernel");
-  for (int bi = 1; bi < blocks; ++bi) {
-    trinv_row_kernel<<<bi, 256, 0, s>>>(L, X, n, bi);
-    TF_LAUNCH_CHECK("trinv_row_kernel");
+  const int nblk = (n + FB - 1) / FB;
+  for (int k = 0; k <= nblk; ++k) {
+    if (k < nblk) {
+      factor_diag_kernel<<<1, F_THREADS, 0, s>>>(A, n, k * FB, work + (size_t)k * FB * FB, info_dev);
+      TF_LAUNCH_CHECK("factor_diag_kernel");
+    }
+    const FactorStep st(n, k);
+    if (st.lead + st.finish == 0) continue;
+    factor_step_kernel<<<st.lead + st.finish, F_THREADS, smem, s>>>(A, X, work, n, k);
+    TF_LAUNCH_CHECK("factor_step_kernel");
   }
 }
 
@@ -350,7 +445,7 @@ __global__ void csr_to_dense_kernel(int n, const int32_t* __restrict__ indptr, c
 
 struct tf_chol {
   int n = 0;
-  tfb::DevBuf A, X, tmp, info, work;
+  tfb::DevBuf A, X, tmp, info, work, fwork;
   bool factored = false;
   std::string err;
 };
@@ -405,12 +500,12 @@ extern "C" int tf_chol_factor_csr(tf_chol* h, const int32_t* indptr_dev, const i
     TF_LAUNCH_CHECK("csr_to_dense_kernel");
     tfb::dense_symmetrize(h->A.as<double>(), n, s);
     TF_CUDA_CHECK(cudaMemsetAsync(h->info.p, 0, sizeof(int), s));
-    tfb::dense_cholesky(h->A.as<double>(), n, h->info.as<int>(), s);
+    if (h->fwork.bytes < tfb::dense_factor_work(n)) h->fwork.alloc(tfb::dense_factor_work(n));
+    tfb::dense_cholesky_inverse(h->A.as<double>(), h->X.as<double>(), n, h->info.as<int>(), h->fwork.as<double>(), s);
     int info = 0;
     TF_CUDA_CHECK(cudaMemcpyAsync(&info, h->info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
     if (info != 0) throw tfb::Error(tfb::TF_NUMERIC, "matrix is not positive definite (pivot " + std::to_string(info) + ")");
-    tfb::dense_trinv(h->A.as<double>(), h->X.as<double>(), n, s);
     h->factored = true;
   });
 }

@@ -150,6 +150,7 @@ struct tf_handle {
   DevBuf mass64, lumped64;  // padded element masses and lumped nodal masses of the last tf_mass_apply
   DevBuf tc_err;            // int: set by the tensor-core finest-level kernel when an MMA wait timed out
   DevBuf trimul_work;       // split-K partials of the coarsest triangular products
+  DevBuf factor_work;       // inverted diagonal blocks of the coarsest factorisation
   GalerkinParam W{};
   DevBuf Q, K0dev, k0diag;
   DevBuf moduli_un, moduli64, modulif;
@@ -731,16 +732,16 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     dense_symmetrize(A.as<double>(), static_cast<int>(nl), st);
     int* info = reinterpret_cast<int*>(h->scal.as<double>() + 8);
     TF_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int), st));
-    dense_cholesky(A.as<double>(), static_cast<int>(nl), info, st);
+    hy.X.ensure(sizeof(double) * nl * nl);
+    const size_t fwork = dense_factor_work(static_cast<int>(nl));
+    if (h->factor_work.bytes < fwork) h->factor_work.alloc(fwork);
+    dense_cholesky_inverse(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), info, h->factor_work.as<double>(), st);
     int hinfo = 0;
     TF_CUDA_CHECK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
     TF_CUDA_CHECK(cudaStreamSynchronize(st));
     if (hinfo != 0)
       throw Error(TF_NUMERIC, "coarsest Galerkin matrix is not positive definite (pivot " + std::to_string(hinfo) +
                                   "); the supports do not remove every rigid-body mode");
-    hy.X.ensure(sizeof(double) * nl * nl);
-    dense_trinv(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), st);
-    TF_CUDA_CHECK(cudaStreamSynchronize(st));
   }
   if (range) cudaEventRecord(range->second, st);
   hy.setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
