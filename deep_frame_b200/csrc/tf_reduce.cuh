@@ -66,4 +66,57 @@ __device__ __forceinline__ bool last_block_combine(double& a, double& b, double*
   return true;
 }
 
+// Three values (op 0 = sum, 1 = max), block-wide; result valid in thread 0.
+template <int OP0, int OP1, int OP2>
+__device__ __forceinline__ void block_reduce3(double& a, double& b, double& c) {
+  __shared__ double sa[RED_THREADS / 32], sb[RED_THREADS / 32], sc[RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  a = OP0 ? warp_max(a) : warp_sum(a);
+  b = OP1 ? warp_max(b) : warp_sum(b);
+  c = OP2 ? warp_max(c) : warp_sum(c);
+  if (lane == 0) { sa[warp] = a; sb[warp] = b; sc[warp] = c; }
+  __syncthreads();
+  if (warp == 0) {
+    a = lane < RED_THREADS / 32 ? sa[lane] : 0.0;
+    b = lane < RED_THREADS / 32 ? sb[lane] : 0.0;
+    c = lane < RED_THREADS / 32 ? sc[lane] : 0.0;
+    a = OP0 ? warp_max(a) : warp_sum(a);
+    b = OP1 ? warp_max(b) : warp_sum(b);
+    c = OP2 ? warp_max(c) : warp_sum(c);
+  }
+  __syncthreads();
+}
+
+// last_block_combine for three values; partials stored as [col][block][4].
+template <int OP0, int OP1, int OP2>
+__device__ __forceinline__ bool last_block_combine3(double& a, double& b, double& c, double* partial, unsigned* count, int col) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    double* p = partial + 4 * ((long long)col * gridDim.x + blockIdx.x);
+    p[0] = a;
+    p[1] = b;
+    p[2] = c;
+    __threadfence();
+    const unsigned t = atomicAdd(&count[col], 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  if (threadIdx.x != 0) return false;
+  __threadfence();
+  double ta = 0.0, tb = 0.0, tc = 0.0;
+  const double* p = partial + 4 * (long long)col * gridDim.x;
+  for (unsigned q = 0; q < gridDim.x; ++q) {
+    const double pa = __ldcg(p + 4 * q), pb = __ldcg(p + 4 * q + 1), pc = __ldcg(p + 4 * q + 2);
+    ta = OP0 ? fmax(ta, pa) : ta + pa;
+    tb = OP1 ? fmax(tb, pb) : tb + pb;
+    tc = OP2 ? fmax(tc, pc) : tc + pc;
+  }
+  count[col] = 0;
+  a = ta;
+  b = tb;
+  c = tc;
+  return true;
+}
+
 }  // namespace tfb

@@ -13,6 +13,7 @@ struct PcgState {
   double* scale;
   double* rzo;
   double* beta;
+  double* wscale;          // scale the preconditioner output w was formed with: z = wscale * w
   int* active;
   int* cand;
   int* iters;
@@ -446,24 +447,34 @@ __global__ void pcg_alpha_kernel(const double* __restrict__ p, const double* __r
   if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) st.alpha[col] = st.rho[col] / a;
 }
 
-// x += alpha p; r -= alpha q; rel = ||r|| / ||b||; candidate when rel < tol (topology_multigrid.py:424-430)
+// x += alpha p; r -= alpha q; rel = ||r|| / ||b||; candidate when rel < tol (topology_multigrid.py:424-430).
+// The same pass forms the next preconditioner inputs, scale = max|r| (clamped at 1e-300) and
+// rzo = r . z_old (topology_multigrid.py:320, :446), with z_old = wscale * w rebuilt from the
+// work-precision preconditioner output: z itself is never stored.
+template <typename T>
 __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
-                                  const double* __restrict__ q, long long n, PcgState st, double tol, int step) {
+                                  const double* __restrict__ q, const T* __restrict__ w, long long n, PcgState st, double tol,
+                                  int step) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   const double al = st.alpha[col];
-  double a = 0.0, z = 0.0;
+  const double zs = st.wscale[col];
+  double a = 0.0, mx = 0.0, d = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     x[off + t] += al * p[off + t];
     const double rv = r[off + t] - al * q[off + t];
     r[off + t] = rv;
     a += rv * rv;
+    mx = fmax(mx, fabs(rv));
+    d += rv * (static_cast<double>(w[off + t]) * zs);
   }
-  block_reduce2<0, 0>(a, z);
-  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) {
+  block_reduce3<0, 1, 0>(a, mx, d);
+  if (last_block_combine3<0, 1, 0>(a, mx, d, st.partial, st.count, col)) {
     const double rel = sqrt(a) / st.bnorm[col];
     st.rel[col] = rel;
+    st.scale[col] = fmax(mx, 1e-300);
+    st.rzo[col] = d;
     atomicMax(&st.hist[step - 1], static_cast<unsigned long long>(__double_as_longlong(rel)));
     if (rel < tol) { st.cand[col] = 1; atomicExch(&st.flags[0], 1); }
   }
@@ -490,15 +501,26 @@ __global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, double* _
   }
 }
 
-// r <- t for non-converged columns; retire converged ones; count the active columns.
-__global__ void pcg_retire_kernel(const double* __restrict__ t_res, double* __restrict__ r, long long n, PcgState st, int step) {
+// Columns that continue from the true residual (cand 3): r <- t, and the preconditioner inputs
+// scale = max|t| and rzo = t . z_old are formed again from the new r.
+template <typename T>
+__global__ void pcg_retire_kernel(const double* __restrict__ t_res, double* __restrict__ r, const T* __restrict__ w, long long n,
+                                  PcgState st) {
   const int col = blockIdx.y;
-  if (!st.active[col]) return;
-  const int c = st.cand[col];
-  if (c == 3) {
-    const long long off = (long long)col * n;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-      r[off + t] = t_res[off + t];
+  if (!st.active[col] || st.cand[col] != 3) return;
+  const long long off = (long long)col * n;
+  const double zs = st.wscale[col];
+  double mx = 0.0, d = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double v = t_res[off + t];
+    r[off + t] = v;
+    mx = fmax(mx, fabs(v));
+    d += v * (static_cast<double>(w[off + t]) * zs);
+  }
+  block_reduce2<1, 0>(mx, d);
+  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) {
+    st.scale[col] = fmax(mx, 1e-300);
+    st.rzo[col] = d;
   }
 }
 
@@ -526,22 +548,16 @@ __global__ void pcg_flags_kernel(PcgState st, int step) {
   }
 }
 
-// scale = max|r| (clamped at 1e-300) and rzo = r . z_old (topology_multigrid.py:320, :446)
-__global__ void pcg_prep_kernel(const double* __restrict__ r, const double* __restrict__ z, long long n, PcgState st, int want_rzo) {
+// scale = max|r| (clamped at 1e-300) before the first preconditioner application (topology_multigrid.py:320)
+__global__ void pcg_prep_kernel(const double* __restrict__ r, long long n, PcgState st) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   double mx = 0.0, d = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const double rv = r[off + t];
-    mx = fmax(mx, fabs(rv));
-    if (want_rzo) d += rv * z[off + t];
-  }
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    mx = fmax(mx, fabs(r[off + t]));
   block_reduce2<1, 0>(mx, d);
-  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) {
-    st.scale[col] = fmax(mx, 1e-300);
-    st.rzo[col] = d;
-  }
+  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) st.scale[col] = fmax(mx, 1e-300);
 }
 
 template <typename T>
@@ -554,7 +570,8 @@ __global__ void pcg_to_work_kernel(const double* __restrict__ r, long long n, Pc
     w[off + t] = static_cast<T>(r[off + t] * s);
 }
 
-// z = scale * x_work; rz = r . z; beta = (rz - rzo) / rho (flexible Polak-Ribiere, topology_multigrid.py:445-448)
+// rz = r . z with z = scale * w (w: the work-precision preconditioner output); beta = (rz - rzo) / rho
+// (flexible Polak-Ribiere, topology_multigrid.py:445-448).  z is written out only when asked for (z != nullptr).
 template <typename T>
 __global__ void pcg_from_work_kernel(const T* __restrict__ w, const double* __restrict__ r, double* __restrict__ z, long long n,
                                      PcgState st, int initial) {
@@ -565,28 +582,28 @@ __global__ void pcg_from_work_kernel(const T* __restrict__ w, const double* __re
   double d = 0.0, zz = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const double v = static_cast<double>(w[off + t]) * s;
-    z[off + t] = v;
+    if (z) z[off + t] = v;
     d += r[off + t] * v;
   }
   block_reduce2<0, 0>(d, zz);
   if (last_block_combine<0, 0>(d, zz, st.partial, st.count, col)) {
-    if (initial) {
-      st.beta[col] = 0.0;
-    } else {
-      st.beta[col] = (d - st.rzo[col]) / st.rho[col];
-    }
+    st.beta[col] = initial ? 0.0 : (d - st.rzo[col]) / st.rho[col];
     st.rho[col] = d;
+    st.wscale[col] = s;
   }
 }
 
-// p = z + beta p
-__global__ void pcg_direction_kernel(const double* __restrict__ z, double* __restrict__ p, long long n, PcgState st, int initial) {
+// p = z + beta p, z = wscale * w
+template <typename T>
+__global__ void pcg_direction_kernel(const T* __restrict__ w, double* __restrict__ p, long long n, PcgState st, int initial) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
-  const double be = st.beta[col];
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    p[off + t] = initial ? z[off + t] : z[off + t] + be * p[off + t];
+  const double be = st.beta[col], s = st.wscale[col];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double z = static_cast<double>(w[off + t]) * s;
+    p[off + t] = initial ? z : z + be * p[off + t];
+  }
 }
 
 // ------------------------------------------------------- layout copies ----

@@ -189,7 +189,7 @@ bool work_is_double(const tf_handle* h) { return h->s.precision == TF_PRECISION_
 // ------------------------------------------------------------ buffers -------
 
 void ensure_scratch(tf_handle* h, int ncol) {
-  const size_t need = (size_t)std::max(ncol, 1) * PCG_BLOCKS * 2 * sizeof(double);
+  const size_t need = (size_t)std::max(ncol, 1) * PCG_BLOCKS * 4 * sizeof(double);
   if (h->partial.bytes < need) {
     h->partial.alloc(need);
     h->count.alloc(sizeof(unsigned) * std::max(ncol, 1));
@@ -258,6 +258,7 @@ PcgState pcg_state(tf_handle* h, int ncol) {
   st.scale = d + 4 * c;
   st.rzo = d + 5 * c;
   st.beta = d + 6 * c;
+  st.wscale = d + 7 * c;
   int* i = h->pcg_i.as<int>();
   st.active = i + 0 * c;
   st.cand = i + 1 * c;
@@ -774,24 +775,30 @@ void ensure_coarse_work(tf_handle* h, Hierarchy& hy, int ncol) {
 
 // ----------------------------------------------------------------- PCG ------
 
+// z = M r for the active columns: r scaled by its column max into the work precision, one cycle,
+// and the new search direction p.  Before the first application (initial) the scale is formed here;
+// afterwards pcg_update_kernel / pcg_retire_kernel have formed it.  z is stored only with store_z.
 template <typename T>
-void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int initial, cudaStream_t s) {
+void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int initial, bool store_z, cudaStream_t s) {
   const long long n = 3 * h->geo[0].nnode;
   VBufs<T>& vb = vbufs<T>(h);
   dim3 gr(grid_for(n, RED_THREADS, PCG_BLOCKS), ncol);
   {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  pcg_prep_kernel<<<gr, RED_THREADS, 0, s>>>(h->vr.as<double>(), h->vz.as<double>(), n, st, initial ? 0 : 1);
-  TF_LAUNCH_CHECK("pcg_prep_kernel");
+  if (initial) {
+    pcg_prep_kernel<<<gr, RED_THREADS, 0, s>>>(h->vr.as<double>(), n, st);
+    TF_LAUNCH_CHECK("pcg_prep_kernel");
+  }
   pcg_to_work_kernel<T><<<cols_grid(n, ncol), 256, 0, s>>>(h->vr.as<double>(), n, st, vb.b[0].template as<T>());
   TF_LAUNCH_CHECK("pcg_to_work_kernel");
   }
   vcycle<T>(h, hy, vb, 0, ncol, st.active, s);
   {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  pcg_from_work_kernel<T><<<gr, RED_THREADS, 0, s>>>(vb.x[0].template as<T>(), h->vr.as<double>(), h->vz.as<double>(), n, st, initial);
+  pcg_from_work_kernel<T><<<gr, RED_THREADS, 0, s>>>(vb.x[0].template as<T>(), h->vr.as<double>(),
+                                                    store_z ? h->vz.as<double>() : nullptr, n, st, initial);
   TF_LAUNCH_CHECK("pcg_from_work_kernel");
-  pcg_direction_kernel<<<cols_grid(n, ncol), 256, 0, s>>>(h->vz.as<double>(), h->vp.as<double>(), n, st, initial);
+  pcg_direction_kernel<T><<<cols_grid(n, ncol), 256, 0, s>>>(vb.x[0].template as<T>(), h->vp.as<double>(), n, st, initial);
   TF_LAUNCH_CHECK("pcg_direction_kernel");
   }
 }
@@ -847,7 +854,7 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
     TF_LAUNCH_CHECK("zero_cols_kernel");
     TF_CUDA_CHECK(cudaMemcpyAsync(h->vr.p, h->vb.p, sizeof(double) * n * ncol, cudaMemcpyDeviceToDevice, s));
   }
-  precondition<T>(h, hy, ncol, st, 1, s);
+  precondition<T>(h, hy, ncol, st, 1, false, s);
   int step = 0;
   int n_active = 0;
   for (int c = 0; c < ncol; ++c) n_active += run[c];
@@ -858,8 +865,8 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
   pcg_alpha_kernel<<<gr, RED_THREADS, 0, s>>>(h->vp.as<double>(), h->vq.as<double>(), n, st);
     TF_LAUNCH_CHECK("pcg_alpha_kernel");
     ++step;
-    pcg_update_kernel<<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), h->vr.as<double>(), h->vp.as<double>(), h->vq.as<double>(),
-                                                 n, st, tol, step);
+    pcg_update_kernel<T><<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), h->vr.as<double>(), h->vp.as<double>(),
+                                                    h->vq.as<double>(), vbufs<T>(h).x[0].template as<T>(), n, st, tol, step);
     TF_LAUNCH_CHECK("pcg_update_kernel");
   }
     fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vq.as<double>(), MODE_RESID, ncol, st.active, st.flags, s);
@@ -867,7 +874,7 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
   pcg_truecheck_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, tol, step);
     TF_LAUNCH_CHECK("pcg_truecheck_kernel");
-    pcg_retire_kernel<<<ge, 256, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, step);
+    pcg_retire_kernel<T><<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), vbufs<T>(h).x[0].template as<T>(), n, st);
     TF_LAUNCH_CHECK("pcg_retire_kernel");
     pcg_flags_kernel<<<1, 256, 0, s>>>(st, step);
     TF_LAUNCH_CHECK("pcg_flags_kernel");
@@ -876,7 +883,7 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
     n_active = h->host_flags[0];
     if (n_active == 0) break;
-    precondition<T>(h, hy, ncol, st, 0, s);
+    precondition<T>(h, hy, ncol, st, 0, false, s);
   }
   PcgResult res;
   res.steps = step;
@@ -1339,10 +1346,10 @@ extern "C" int tf_precondition(tf_handle* h, uint64_t key, const double* r_dev, 
     TF_LAUNCH_CHECK("pad_kernel");
     if (work_is_double(h)) {
       ensure_vbufs<double>(h, nrhs);
-      precondition<double>(h, hy, nrhs, st, 1, s);
+      precondition<double>(h, hy, nrhs, st, 1, true, s);
     } else {
       ensure_vbufs<float>(h, nrhs);
-      precondition<float>(h, hy, nrhs, st, 1, s);
+      precondition<float>(h, hy, nrhs, st, 1, true, s);
     }
     unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vz.as<double>(), h->un, h->geo[0], z_dev, nun, nullptr);
     TF_LAUNCH_CHECK("unpad_kernel");
