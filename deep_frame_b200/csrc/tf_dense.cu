@@ -13,20 +13,21 @@
 namespace tfb {
 
 namespace {
-// Blocked Cholesky factorisation fused with the inversion of its factor.  Per 32-wide panel k
-// (rows / columns k0 = 32 k .. k0 + 31) two launches: factor_diag_kernel (one CTA) factors the
-// diagonal block W_kk = L_kk L_kk^T, final after the previous panel's update, and stores
-// Linv_kk = L_kk^-1 in `work`; factor_step_kernel then runs three kinds of CTA:
+// Blocked Cholesky factorisation fused with the inversion of its factor, one launch per 32-wide
+// panel.  Launch k (panel rows / columns k0 = 32 k .. k0 + 31) reads Linv_kk, the inverse of the
+// factor of the diagonal block W_kk = L_kk L_kk^T, from `work` and runs three kinds of CTA:
 //  * trailing tiles (ti >= tj, 64 x 64): L_i = W_ik Linv_kk^T for the tile's two row ranges, then
-//    W_ij -= L_i L_j^T (the Schur complement; W is the input matrix and is overwritten);
+//    W_ij -= L_i L_j^T (the Schur complement; W is the input matrix and is overwritten).  Tile
+//    (0, 0) holds the next diagonal block, final after this update, so that CTA then factors and
+//    inverts it for launch k + 1 while the other tiles run (look-ahead);
 //  * inverse tiles (a row tile below the panel x 64 columns j < k0 + 32): X_k = Linv_kk R_k for
 //    those columns, then R_ij -= L_i X_k.  R lives in the output buffer X; it starts as the identity
 //    and, when panel k runs, block row k of R is the right-hand side of L_kk X_k = R_k;
 //  * finishing tiles: block row k - 1 of R is complete after panel k - 1 and is replaced in place by
 //    X_{k-1} = Linv_{k-1} R_{k-1}.
 // The three kinds read and write disjoint parts of W, X and `work`, so a launch needs no other
-// synchronisation; a last launch finishes the last block row.  L itself is never stored: the
-// coarsest solve only uses X = L^-1 (x = X^T X b).
+// synchronisation.  A one-CTA launch factors block 0 first; a last launch finishes the last block
+// row.  L itself is never stored: the coarsest solve only uses X = L^-1 (x = X^T X b).
 constexpr int FB = 32;       // panel width
 constexpr int FT = 64;       // update tile
 constexpr int FP = FT + 1;   // shared-memory pitch of the K-major operand tiles
@@ -63,10 +64,8 @@ struct FactorStep {
 
 // Factor and invert the diagonal block at (k0, k0) (rows beyond n padded with the identity) and
 // store Linv in Dk; a non-positive pivot is replaced by 1 and reported as 1 + its global index in
-// *info (when *info is still 0).  One CTA; the elimination itself is one warp.
-__global__ void __launch_bounds__(F_THREADS, 1) factor_diag_kernel(const double* __restrict__ W, int n, int k0,
-                                                                   double* __restrict__ Dk, int* __restrict__ info) {
-  __shared__ DiagShared s;
+// *info (when *info is still 0).  Called by every thread of one CTA; the elimination is one warp.
+__device__ void factor_diag(const double* W, int n, int k0, DiagShared& s, double* __restrict__ Dk, int* __restrict__ info) {
   const int nb = min(FB, n - k0);
   {
     double v[FB * FB / F_THREADS];
@@ -142,6 +141,13 @@ __global__ void __launch_bounds__(F_THREADS, 1) factor_diag_kernel(const double*
     const int e = threadIdx.x + q * F_THREADS;
     Dk[e] = s.Li[e / FB][e % FB];
   }
+}
+
+// the factor of diagonal block 0, before the first panel launch
+__global__ void __launch_bounds__(F_THREADS) factor_first_kernel(const double* __restrict__ W, int n, double* __restrict__ D,
+                                                                 int* __restrict__ info) {
+  __shared__ DiagShared s;
+  factor_diag(W, n, 0, s, D, info);
 }
 
 // s.Li <- the 32 x 32 block Dk
@@ -249,7 +255,7 @@ __device__ void update_tile(double* __restrict__ C, int n, int i0, int j0, int c
 }
 
 __global__ void __launch_bounds__(F_THREADS, 2) factor_step_kernel(double* __restrict__ W, double* __restrict__ X,
-                                                                   const double* __restrict__ D, int n, int k) {
+                                                                   double* __restrict__ D, int n, int k, int* __restrict__ info) {
   extern __shared__ __align__(16) unsigned char f_smem[];
   FactorShared& s = *reinterpret_cast<FactorShared*>(f_smem);
   const FactorStep st(n, k);
@@ -288,6 +294,11 @@ __global__ void __launch_bounds__(F_THREADS, 2) factor_step_kernel(double* __res
     }
     __syncthreads();
     update_tile(W, n, i0, j0, n, ti == tj, s.A, ti == tj ? s.A : s.T);
+    if (b == 0) {
+      // tile (0, 0) holds diagonal block k + 1, final now: factor it for the next launch
+      __syncthreads();
+      factor_diag(W, n, start, *reinterpret_cast<DiagShared*>(f_smem), D + (long long)(k + 1) * FB * FB, info);
+    }
   } else {
     const int u = b - st.syrk, ti = u / st.ctiles, tj = u % st.ctiles;
     const int i0 = start + ti * FT, j0 = tj * FT;
@@ -323,18 +334,17 @@ void dense_symmetrize(double* A, int n, cudaStream_t s) {
 size_t dense_factor_work(int n) { return sizeof(double) * FB * FB * (size_t)((n + FB - 1) / FB); }
 
 void dense_cholesky_inverse(double* A, double* X, int n, int* info_dev, double* work, cudaStream_t s) {
+  static_assert(sizeof(DiagShared) <= sizeof(FactorShared), "the look-ahead factor reuses the update tiles' shared memory");
   const int smem = static_cast<int>(sizeof(FactorShared));
   TF_CUDA_CHECK(cudaFuncSetAttribute(factor_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   TF_CUDA_CHECK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, s));
+  factor_first_kernel<<<1, F_THREADS, 0, s>>>(A, n, work, info_dev);
+  TF_LAUNCH_CHECK("factor_first_kernel");
   const int nblk = (n + FB - 1) / FB;
   for (int k = 0; k <= nblk; ++k) {
-    if (k < nblk) {
-      factor_diag_kernel<<<1, F_THREADS, 0, s>>>(A, n, k * FB, work + (size_t)k * FB * FB, info_dev);
-      TF_LAUNCH_CHECK("factor_diag_kernel");
-    }
     const FactorStep st(n, k);
     if (st.lead + st.finish == 0) continue;
-    factor_step_kernel<<<st.lead + st.finish, F_THREADS, smem, s>>>(A, X, work, n, k);
+    factor_step_kernel<<<st.lead + st.finish, F_THREADS, smem, s>>>(A, X, work, n, k, info_dev);
     TF_LAUNCH_CHECK("factor_step_kernel");
   }
 }

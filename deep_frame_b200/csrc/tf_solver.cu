@@ -177,8 +177,14 @@ struct tf_handle {
   unsigned long long k0_version = 0;
   Timers timers;
   std::string err;
+  // the coarsest factorisation runs on `side` while the power iterations run on the caller's stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_fork = nullptr, side_join = nullptr;
   ~tf_handle() {
     if (host_flags) cudaFreeHost(host_flags);
+    if (side_fork) cudaEventDestroy(side_fork);
+    if (side_join) cudaEventDestroy(side_join);
+    if (side) cudaStreamDestroy(side);
   }
 };
 
@@ -696,11 +702,9 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
                                                                            dbl ? nullptr : c.stencilw.as<float>());
     TF_LAUNCH_CHECK("stencil_assemble_kernel");
   }
-  // lambda_max(D^-1 A) of every smoothed level, in the work precision
+  // Dense coarsest factor of the live dofs.  It depends on nothing the power iterations below
+  // produce, so it runs on the handle's side stream while they run on `st`.
   if (dbl) ensure_vbufs<double>(h, 1); else ensure_vbufs<float>(h, 1);
-  for (int l = 0; l + 1 < h->nlev; ++l)
-    hy.lv[l].lambda_max = dbl ? power_lambda<double>(h, hy, l, st) : power_lambda<float>(h, hy, l, st);
-  // dense coarsest factor of the live dofs
   Level& cl = hy.lv[h->nlev - 1];
   std::vector<uint8_t> cmask(cl.g.nnode);
   TF_CUDA_CHECK(cudaMemcpyAsync(cmask.data(), cl.mask.p, cmask.size(), cudaMemcpyDeviceToHost, st));
@@ -718,6 +722,7 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     throw Error(TF_INVALID, "coarsest grid has " + std::to_string(nl) + " live dofs; the dense coarsest factor allows at most " +
                                 std::to_string(DENSE_LIMIT) + " (raise max_levels or lower coarsest_dofs)");
   hy.n_live = static_cast<int>(nl);
+  int* info = reinterpret_cast<int*>(h->scal.as<double>() + 8);
   if (nl > 0) {
     hy.live.ensure(sizeof(long long) * nl);
     TF_CUDA_CHECK(cudaMemcpyAsync(hy.live.p, live.data(), sizeof(long long) * nl, cudaMemcpyHostToDevice, st));
@@ -731,12 +736,25 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
                                                                 hy.live.as<long long>(), static_cast<int>(nl), A.as<double>());
     TF_LAUNCH_CHECK("coarsest_assemble_kernel");
     dense_symmetrize(A.as<double>(), static_cast<int>(nl), st);
-    int* info = reinterpret_cast<int*>(h->scal.as<double>() + 8);
     TF_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int), st));
     hy.X.ensure(sizeof(double) * nl * nl);
     const size_t fwork = dense_factor_work(static_cast<int>(nl));
     if (h->factor_work.bytes < fwork) h->factor_work.alloc(fwork);
-    dense_cholesky_inverse(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), info, h->factor_work.as<double>(), st);
+    if (!h->side) {
+      TF_CUDA_CHECK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+      TF_CUDA_CHECK(cudaEventCreateWithFlags(&h->side_fork, cudaEventDisableTiming));
+      TF_CUDA_CHECK(cudaEventCreateWithFlags(&h->side_join, cudaEventDisableTiming));
+    }
+    TF_CUDA_CHECK(cudaEventRecord(h->side_fork, st));
+    TF_CUDA_CHECK(cudaStreamWaitEvent(h->side, h->side_fork, 0));
+    dense_cholesky_inverse(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), info, h->factor_work.as<double>(), h->side);
+    TF_CUDA_CHECK(cudaEventRecord(h->side_join, h->side));
+  }
+  // lambda_max(D^-1 A) of every smoothed level, in the work precision
+  for (int l = 0; l + 1 < h->nlev; ++l)
+    hy.lv[l].lambda_max = dbl ? power_lambda<double>(h, hy, l, st) : power_lambda<float>(h, hy, l, st);
+  if (nl > 0) {
+    TF_CUDA_CHECK(cudaStreamWaitEvent(st, h->side_join, 0));
     int hinfo = 0;
     TF_CUDA_CHECK(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
     TF_CUDA_CHECK(cudaStreamSynchronize(st));
