@@ -253,6 +253,53 @@ __device__ __forceinline__ void epilogue(const LevelArgs<T>& a, int mode, long l
   }
 }
 
+// Per-column epilogue inputs besides A u (b; res and x for the Chebyshev update), loaded before the
+// operator so that their latency overlaps its arithmetic.  The other inputs (the direction u and
+// the inverse diagonal, the same for every column) are read afterwards.
+template <typename T>
+struct EpiPre {
+  T v[2][3];
+};
+
+template <typename T>
+__device__ __forceinline__ void epilogue_load(const LevelArgs<T>& a, int mode, long long col_off, long long node, EpiPre<T>& in) {
+  const long long d0 = col_off + 3 * node;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (mode == MODE_RESID || mode == MODE_JACOBI) {
+      in.v[0][q] = a.b[d0 + q];
+    } else if (mode == MODE_CHEB) {
+      in.v[0][q] = a.res[d0 + q];
+      in.v[1][q] = a.x[d0 + q];
+    }
+  }
+}
+
+// epilogue() from prefetched inputs (the same arithmetic)
+template <typename T>
+__device__ __forceinline__ void epilogue_pre(const LevelArgs<T>& a, int mode, long long col_off, long long node, unsigned m,
+                                             const T av[3], const EpiPre<T>& in) {
+  const long long d0 = col_off + 3 * node;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const bool live = (m >> q) & 1u;
+    const long long d = d0 + q;
+    if (mode == MODE_APPLY) {
+      a.y[d] = live ? av[q] : T(0);
+    } else if (mode == MODE_RESID) {
+      a.y[d] = live ? (in.v[0][q] - av[q]) : T(0);
+    } else if (mode == MODE_JACOBI) {
+      a.y[d] = a.u[d] + a.s * a.inv[3 * node + q] * (in.v[0][q] - (live ? av[q] : T(0)));
+    } else {  // MODE_CHEB
+      const T r = in.v[0][q] - (live ? av[q] : T(0));
+      const T dn = a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r;
+      a.res[d] = r;
+      a.y[d] = dn;
+      a.x[d] = in.v[1][q] + dn;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Shared-memory tiled level operators.  A CTA owns a tile of TX x TY x tz
 // output nodes (tz <= TZMAX chosen per grid so that the z extent is covered
@@ -460,16 +507,40 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
     while (next < c_end && a.active && !a.active[next]) ++next;
     if (next < c_end) fetch(next);
     if (owner) {
-      T av[NPT][3];
-      fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
       const long long off = (long long)c * a.colstride;
+      if constexpr (sizeof(T) == 4) {
+        // work-precision smoother: the epilogue inputs are fetched before the operator
+        EpiPre<T> ep[NPT];
+        unsigned mq[NPT];
 #pragma unroll
-      for (int q = 0; q < NPT; ++q) {
-        const int i = x0 + lx * NPT + q;
-        if (i >= g.nx) continue;
-        const long long n = ((long long)i * g.ny + j) * g.nz + k;
-        const unsigned m = a.mask ? a.mask[n] : 7u;
-        epilogue(a, mode, off, n, m, av[q]);
+        for (int q = 0; q < NPT; ++q) {
+          const int i = x0 + lx * NPT + q;
+          mq[q] = 0u;
+          if (i >= g.nx) continue;
+          const long long n = ((long long)i * g.ny + j) * g.nz + k;
+          mq[q] = a.mask ? a.mask[n] : 7u;
+          epilogue_load(a, mode, off, n, ep[q]);
+        }
+        T av[NPT][3];
+        fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+          const int i = x0 + lx * NPT + q;
+          if (i >= g.nx) continue;
+          const long long n = ((long long)i * g.ny + j) * g.nz + k;
+          epilogue_pre(a, mode, off, n, mq[q], av[q], ep[q]);
+        }
+      } else {
+        T av[NPT][3];
+        fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+          const int i = x0 + lx * NPT + q;
+          if (i >= g.nx) continue;
+          const long long n = ((long long)i * g.ny + j) * g.nz + k;
+          const unsigned m = a.mask ? a.mask[n] : 7u;
+          epilogue(a, mode, off, n, m, av[q]);
+        }
       }
     }
     if (next >= c_end) break;
