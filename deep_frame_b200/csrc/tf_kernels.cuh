@@ -670,6 +670,12 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const Le
   const long long n = ((long long)i * g.ny + j) * g.nz + k;
   const long long nst = g.nnode;
   const T* sp = a.E + n;
+  // the columns' epilogue inputs are fetched before the stencil arithmetic (their latency overlaps it)
+  const unsigned m = a.mask ? a.mask[n] : 7u;
+  EpiPre<T> ep[CB];
+#pragma unroll
+  for (int c = 0; c < CB; ++c)
+    if (c < nc && (!a.active || a.active[c0 + c])) epilogue_load(a, mode, off + c * a.colstride, n, ep[c]);
   T out[CB][3];
 #pragma unroll
   for (int c = 0; c < CB; ++c) { out[c][0] = T(0); out[c][1] = T(0); out[c][2] = T(0); }
@@ -695,10 +701,9 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const Le
       }
     }
   }
-  const unsigned m = a.mask ? a.mask[n] : 7u;
 #pragma unroll
   for (int c = 0; c < CB; ++c) {
-    if (c < nc && (!a.active || a.active[c0 + c])) epilogue(a, mode, off + c * a.colstride, n, m, out[c]);
+    if (c < nc && (!a.active || a.active[c0 + c])) epilogue_pre(a, mode, off + c * a.colstride, n, m, out[c], ep[c]);
   }
 }
 
