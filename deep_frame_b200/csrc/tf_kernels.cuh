@@ -68,11 +68,15 @@ template <int SLOT> struct K0Const<double, SLOT, true> {
 };
 
 
+// Node counts stay below 2^31 (tf_create checks it), so 32-bit division suffices: a 64-bit one is
+// a long instruction sequence per call.
 __device__ __forceinline__ void node_coords(long long n, const Geo& g, int& i, int& j, int& k) {
-  k = static_cast<int>(n % g.nz);
-  long long r = n / g.nz;
-  j = static_cast<int>(r % g.ny);
-  i = static_cast<int>(r / g.ny);
+  const unsigned u = static_cast<unsigned>(n), nz = static_cast<unsigned>(g.nz), ny = static_cast<unsigned>(g.ny);
+  const unsigned r = u / nz;
+  k = static_cast<int>(u - r * nz);
+  const unsigned ii = r / ny;
+  j = static_cast<int>(r - ii * ny);
+  i = static_cast<int>(ii);
 }
 
 template <typename T>
@@ -343,6 +347,44 @@ __device__ __forceinline__ void stage_tile(T* __restrict__ s, const Geo& g, cons
       load_masked(u, mask, ((long long)gx * g.ny + gy) * g.nz + gz, v0, v1, v2);
     T* d = s + 3 * ((cx * HY + cy) * HZ + cz);
     d[0] = v0; d[1] = v1; d[2] = v2;
+  }
+}
+
+// Stage the masked input tiles of nc <= CB columns in one pass over the halo: the mask is read once
+// per node and the columns' loads are issued together, independent of the mask load (the mask is
+// applied when storing).
+template <typename T, int CB>
+__device__ __forceinline__ void stage_tiles(T* __restrict__ s, const Geo& g, const T* __restrict__ u, long long colstride, int nc,
+                                            const uint8_t* __restrict__ mask, int x0, int y0, int z0, int tz) {
+  const int hz = tz + 2;
+  const int count = HX * HY * hz;
+  for (int t = threadIdx.x; t < count; t += blockDim.x) {
+    const int cz = t % hz, r = t / hz, cy = r % HY, cx = r / HY;
+    const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
+    const bool in = (unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz;
+    const long long node = in ? ((long long)gx * g.ny + gy) * g.nz + gz : 0;
+    const unsigned m = in ? (mask ? mask[node] : 7u) : 0u;
+    T v[CB][3];
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+      v[c][0] = v[c][1] = v[c][2] = T(0);
+      if (in && c < nc) {
+        const T* p = u + c * colstride + 3 * node;
+        v[c][0] = p[0];
+        v[c][1] = p[1];
+        v[c][2] = p[2];
+      }
+    }
+    const int so = 3 * ((cx * HY + cy) * HZ + cz);
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+      if (c < nc) {
+        T* d = s + c * HALO * 3 + so;
+        d[0] = (m & 1u) ? v[c][0] : T(0);
+        d[1] = (m & 2u) ? v[c][1] : T(0);
+        d[2] = (m & 4u) ? v[c][2] : T(0);
+      }
+    }
   }
 }
 
@@ -659,10 +701,7 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const Le
   const int tz = tm.tz;
   const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
   const long long off = (long long)c0 * a.colstride;
-#pragma unroll
-  for (int c = 0; c < CB; ++c) {
-    if (c < nc) stage_tile(su + c * HALO * 3, g, a.u + off + c * a.colstride, a.mask, x0, y0, z0, tz);
-  }
+  stage_tiles<T, CB>(su, g, a.u + off, a.colstride, nc, a.mask, x0, y0, z0, tz);
   __syncthreads();
   const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
   const int i = x0 + lx, j = y0 + ly, k = z0 + lz;

@@ -1072,6 +1072,7 @@ extern "C" int tf_create(const tf_grid* grid, const double* ke, const double* me
     for (int l = 0; l < count; ++l)
       h->geo.push_back(make_geo(h->padded[0] >> l, h->padded[1] >> l, h->padded[2] >> l));
     h->un = make_geo(h->shape[0], h->shape[1], h->shape[2]);
+    require(h->geo[0].nnode < (1LL << 31), "grid too large: the padded grid must have fewer than 2^31 nodes");
     // trilinear interpolation weights W[child][fine corner][coarse corner] (topology_multigrid.py:19-27)
     static const int C[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
     for (int c = 0; c < 8; ++c) {
