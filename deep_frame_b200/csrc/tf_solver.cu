@@ -151,6 +151,7 @@ struct tf_handle {
   DevBuf tc_err;            // int: set by the tensor-core finest-level kernel when an MMA wait timed out
   DevBuf trimul_work;       // split-K partials of the coarsest triangular products
   DevBuf factor_work;       // inverted diagonal blocks of the coarsest factorisation
+  DevBuf solve_small;       // per-solve column norms and column lists (grows, never shrinks)
   GalerkinParam W{};
   DevBuf Q, K0dev, k0diag;
   DevBuf moduli_un, moduli64, modulif;
@@ -1211,11 +1212,11 @@ int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, do
     std::vector<double> norms(nrhs, 0.0);
     if (nrhs > 0) {
       ensure_scratch(h, nrhs);
-      DevBuf dn(sizeof(double) * nrhs);
+      if (h->solve_small.bytes < sizeof(double) * nrhs) h->solve_small.alloc(sizeof(double) * nrhs);
       colnorm_kernel<<<dim3(grid_for(nun, RED_THREADS, PCG_BLOCKS), nrhs), RED_THREADS, 0, s>>>(
-          f_dev, nun, dn.as<double>(), h->partial.as<double>(), h->count.as<unsigned>());
+          f_dev, nun, h->solve_small.as<double>(), h->partial.as<double>(), h->count.as<unsigned>());
       TF_LAUNCH_CHECK("colnorm_kernel");
-      TF_CUDA_CHECK(cudaMemcpyAsync(norms.data(), dn.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
+      TF_CUDA_CHECK(cudaMemcpyAsync(norms.data(), h->solve_small.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
       TF_CUDA_CHECK(cudaStreamSynchronize(s));
     }
     double mx = 0.0;
@@ -1230,9 +1231,10 @@ int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, do
     std::vector<double> history;
     int batches = 0, retried = 0, steps = 0;
     if (!dead.empty()) {
-      DevBuf dcols(sizeof(int) * dead.size());
-      TF_CUDA_CHECK(cudaMemcpyAsync(dcols.p, dead.data(), sizeof(int) * dead.size(), cudaMemcpyHostToDevice, s));
-      zero_flat_cols_kernel<<<dim3(grid_for(nun, 256), (unsigned)dead.size()), 256, 0, s>>>(u_dev, nun, dcols.as<int>());
+      // solve_small is reused in stream order: the norms above were read back before this copy
+      if (h->solve_small.bytes < sizeof(int) * dead.size()) h->solve_small.alloc(sizeof(int) * dead.size());
+      TF_CUDA_CHECK(cudaMemcpyAsync(h->solve_small.p, dead.data(), sizeof(int) * dead.size(), cudaMemcpyHostToDevice, s));
+      zero_flat_cols_kernel<<<dim3(grid_for(nun, 256), (unsigned)dead.size()), 256, 0, s>>>(u_dev, nun, h->solve_small.as<int>());
       TF_LAUNCH_CHECK("zero_flat_cols_kernel");
       TF_CUDA_CHECK(cudaStreamSynchronize(s));
     }
@@ -1264,9 +1266,10 @@ int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, do
         // restart from the previous iterate where it improved on zero (topology_multigrid.py:393)
         std::vector<int> reset(nc, 0);
         for (int c = 0; c < nc; ++c) reset[c] = failed[c] && !(r.rel[c] < 1.0);
-        DevBuf dreset(sizeof(int) * nc);
-        TF_CUDA_CHECK(cudaMemcpyAsync(dreset.p, reset.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
-        zero_cols_kernel<double><<<cols_grid(n, nc), 256, 0, s>>>(h->vx.as<double>(), n, dreset.as<int>());
+        // solve_small is reused in stream order (every user of it runs on stream s)
+        if (h->solve_small.bytes < sizeof(int) * nc) h->solve_small.alloc(sizeof(int) * nc);
+        TF_CUDA_CHECK(cudaMemcpyAsync(h->solve_small.p, reset.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
+        zero_cols_kernel<double><<<cols_grid(n, nc), 256, 0, s>>>(h->vx.as<double>(), n, h->solve_small.as<int>());
         TF_LAUNCH_CHECK("zero_cols_kernel");
         PcgResult again = pcg_precise(h, hy, nc, failed, s);
         for (int c = 0; c < nc; ++c)
