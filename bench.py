@@ -533,7 +533,7 @@ def main():
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
                        "outer": "fp64 PCG", "vcycle": args.precision + (" (finest apply: tcgen05 TF32)" if result["smoother"].get("tensor_cores") else ""), "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
                        "pcg_iterations": result["iterations_max"], "smoother": result["smoother"],
-                       "smoother_choice": "autotuned (fastest of 8 schedules / depths / finest-apply units, all to the same tolerance)" if result["tuning"] else "reference default",
+                       "smoother_choice": f"autotuned (fastest of {len(result['tuning'])} schedules / depths / finest-apply units, all to the same tolerance)" if result["tuning"] else "reference default",
                        "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
                        "parallelism": f"rhs-sharded x{result['world']}"},
             "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),

@@ -15,8 +15,15 @@ CANDIDATES = (
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5},
     {"smoother": "chebyshev", "chebyshev_degree": 3, "growth": 1.0},
     {"smoother": "jacobi", "sweeps": 2, "growth": 2.0},
+    # lighter smoothing on the Galerkin levels (fewer sweeps per cycle, possibly more PCG iterations)
+    {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.0},
+    {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.25},
+    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0},
+    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 1.5},
+    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 3.0},
     # one more level (a coarsest grid of a few hundred dofs: cheaper dense factor, longer V-cycle)
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5, "coarsest_dofs": 1200},
+    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "coarsest_dofs": 1200},
     # the same schedules with the finest-level V-cycle apply on the tensor cores (TF32 operands)
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5, "tensor_cores": True},
     {"smoother": "chebyshev", "chebyshev_degree": 3, "growth": 2.0, "tensor_cores": True},

@@ -349,28 +349,29 @@ void dense_cholesky_inverse(double* A, double* X, int n, int* info_dev, double* 
   }
 }
 
-// Split-K form of C = op(X) B: CTA (row block rb, K chunk kc, column group) multiplies 32 rows of op(X)
-// restricted to K chunk kc (256 wide) with up to 48 columns of B and stores the partial tile; chunks
+// Split-K form of C = op(X) B: CTA (row block rb, K chunk kc, column group) multiplies 64 rows of op(X)
+// restricted to K chunk kc (128 wide) with up to 48 columns of B and stores the partial tile; chunks
 // that lie entirely in the zero triangle of op(X) are skipped.  trimul_sum_kernel adds the partials of
-// every row in chunk order (deterministic) into C.  Balanced over 148 SMs for the coarsest sizes
+// every row in chunk order (deterministic) into C.  Each of the 128 threads holds a 4 x 6 register
+// tile (10 shared-memory loads per 24 FMA); the split keeps ~150 CTAs busy at the coarsest sizes
 // (a few thousand unknowns), where a whole-K row tile would leave most SMs idle.
-constexpr int TM_RB = 32, TM_KCH = 256, TM_KS = 32, TM_CW = 48;
+constexpr int TM_RB = 64, TM_KCH = 128, TM_KS = 32, TM_CW = 48, TM_THREADS = 128;
 
 __device__ __forceinline__ bool trimul_chunk_live(int i0, int kc, int transpose) {
   return transpose ? (kc + 1) * TM_KCH - 1 >= i0 : kc * TM_KCH <= i0 + TM_RB - 1;
 }
 
-__global__ void __launch_bounds__(256) trimul_split_kernel(const double* __restrict__ X, const double* __restrict__ B,
-                                                           double* __restrict__ P, int n, int ncol, int transpose) {
+__global__ void __launch_bounds__(TM_THREADS) trimul_split_kernel(const double* __restrict__ X, const double* __restrict__ B,
+                                                                  double* __restrict__ P, int n, int ncol, int transpose) {
   __shared__ double Xs[TM_RB][TM_KS + 1];
   __shared__ double Bs[TM_CW][TM_KS + 1];
   const int i0 = blockIdx.x * TM_RB, kc = blockIdx.y, c0 = blockIdx.z * TM_CW;
   if (!trimul_chunk_live(i0, kc, transpose)) return;
-  const int t = threadIdx.x, r = t % TM_RB, cg = t / TM_RB;   // 8 column groups of 6
+  const int t = threadIdx.x, cg = t % 8, rg = t / 8;   // 16 row groups of 4 x 8 column groups of 6
   const int k_lo = kc * TM_KCH, k_hi = min(n, k_lo + TM_KCH);
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  double acc[4][6] = {};
   for (int k0 = k_lo; k0 < k_hi; k0 += TM_KS) {
-    for (int e = t; e < TM_RB * TM_KS; e += 256) {
+    for (int e = t; e < TM_RB * TM_KS; e += TM_THREADS) {
       // contiguous global reads: k fastest for X rows, row fastest for X^T
       const int rr = transpose ? e % TM_RB : e / TM_KS, kk = transpose ? e / TM_RB : e % TM_KS;
       const int i = i0 + rr, k = k0 + kk;
@@ -378,25 +379,34 @@ __global__ void __launch_bounds__(256) trimul_split_kernel(const double* __restr
       if (i < n && k < k_hi) v = transpose ? X[(long long)k * n + i] : X[(long long)i * n + k];
       Xs[rr][kk] = v;
     }
-    for (int e = t; e < TM_CW * TM_KS; e += 256) {
+    for (int e = t; e < TM_CW * TM_KS; e += TM_THREADS) {
       const int cc = e / TM_KS, kk = e % TM_KS, col = c0 + cc, k = k0 + kk;
       Bs[cc][kk] = (col < ncol && k < k_hi) ? B[(long long)col * n + k] : 0.0;
     }
     __syncthreads();
-#pragma unroll 8
+#pragma unroll 4
     for (int kk = 0; kk < TM_KS; ++kk) {
-      const double a = Xs[r][kk];
+      double a[4], b[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) acc[q] = fma(a, Bs[cg * 6 + q][kk], acc[q]);
+      for (int p = 0; p < 4; ++p) a[p] = Xs[rg * 4 + p][kk];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) b[q] = Bs[cg * 6 + q][kk];
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
     }
     __syncthreads();
   }
-  const int i = i0 + r;
-  if (i >= n) return;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const int col = c0 + cg * 6 + q;
-    if (col < ncol) P[((long long)kc * ncol + col) * n + i] = acc[q];
+  for (int p = 0; p < 4; ++p) {
+    const int i = i0 + rg * 4 + p;
+    if (i >= n) continue;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int col = c0 + cg * 6 + q;
+      if (col < ncol) P[((long long)kc * ncol + col) * n + i] = acc[p][q];
+    }
   }
 }
 
@@ -422,7 +432,7 @@ void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, 
                   cudaStream_t s) {
   const int nchunks = (n + TM_KCH - 1) / TM_KCH;
   dim3 grid((n + TM_RB - 1) / TM_RB, nchunks, (ncol + TM_CW - 1) / TM_CW);
-  trimul_split_kernel<<<grid, 256, 0, s>>>(X, B, work, n, ncol, transpose);
+  trimul_split_kernel<<<grid, TM_THREADS, 0, s>>>(X, B, work, n, ncol, transpose);
   TF_LAUNCH_CHECK("trimul_split_kernel");
   trimul_sum_kernel<<<grid_for((long long)n * ncol, 256), 256, 0, s>>>(work, C, n, ncol, nchunks, transpose, active);
   TF_LAUNCH_CHECK("trimul_sum_kernel");
