@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tensor-cores", action="store_true", help="FP32 finest-level V-cycle apply on tcgen05 (TF32)")
+    ap.add_argument("--schedule", default=None, metavar="DEGREE,GROWTH",
+                    help="use this Chebyshev smoother schedule instead of autotuning (e.g. 1,2)")
     ap.add_argument("--instances", type=int, default=0,
                     help="solve N independent seeded plates of uneven size and RHS count concurrently and report solves/s")
     ap.add_argument("--learned", action="store_true", help="train the learned initial guess and report PCG with / without it")
@@ -55,6 +57,11 @@ def parse():
                     help="SIMP: start every PCG from the previous design's solution (no value), or from the energy-optimal "
                          "combination of the last M designs' solutions (--warm-start M)")
     return ap.parse_args()
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one 42-column finest-level FP32 launch of
+# the 96 x 96 x 16 plate, by epilogue mode, from ncu captures of that launch
+FINE_TRAFFIC = {"cheb": 434e6, "resid": 220.5e6}
 
 
 def peaks():
@@ -114,14 +121,14 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_problem(config, precision, device, tensor_cores=False):
+def build_problem(config, precision, device, tensor_cores=False, smoother=None):
     from deep_frame_b200 import problems
     from deep_frame_b200.covariance import InterfaceCovariance
     from deep_frame_b200.elasticity import HexElasticity
     spec = problems.CONFIGS[config]
     domain, density, cov = problems.plate(spec["shape"], 0)
     system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": spec["tolerance"], "device": str(device),
-                                              "tensor_cores": tensor_cores})
+                                              "tensor_cores": tensor_cores, **(smoother or {})})
     model = InterfaceCovariance(system, cov, domain["interfaces"])
     return spec, system, model, density
 
@@ -141,13 +148,17 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    spec, system, model, density = build_problem(args.config, args.precision, device, args.tensor_cores)
+    fixed = None
+    if args.schedule:
+        degree, growth = args.schedule.split(",")
+        fixed = {"smoother": "chebyshev", "chebyshev_degree": int(degree), "growth": float(growth)}
+    spec, system, model, density = build_problem(args.config, args.precision, device, args.tensor_cores, fixed)
     moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
     moduli = torch.as_tensor(moduli_host, device=device)
     scale = torch.as_tensor(-derivative, device=device)
     groups = model.groups()
     tuned, tuning = None, None
-    if not args.no_autotune:
+    if not args.no_autotune and not args.schedule:
         # measured smoother choice (outside the timed region); every candidate solves to the same tolerance
         from deep_frame_b200.autotune import CANDIDATES, tune_smoother
         choice = [None]
@@ -178,10 +189,12 @@ def ours(args):
     launches0 = int(_lib.load().tf_launch_count())
     with Clocks(local) as clocks:
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed")   # lets a profiler select the timed steps' launches
         start.record()
         for _ in range(args.steps):
             rows, flex = step()
         stop.record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
     launches = int(_lib.load().tf_launch_count()) - launches0
     if world > 1:
@@ -505,16 +518,26 @@ def main():
         return
     hbm, bf16, source = peaks()
     ms = result["ms"]
-    # algorithmic bytes of one launch of the dominant kernel: every node reads its 3 input values and
-    # writes 3 outputs per column (+ the element moduli once per column launch)
+    # algorithmic bytes of one launch of the dominant kernel, per node and column: the words its mode
+    # must read and write (+ the element moduli, once per launch: a CTA stages them for its columns).  PCG operator: u read, y
+    # written (6).  Work-precision finest level with Chebyshev degree d: per V-cycle 2 residual applies
+    # (u, b read, y written: 9) and 2 (d - 1) Chebyshev steps (u, res, x read; y, res, x written: 18).
     dominant = result["dominant"]
     word = 8 if dominant == "fine_fp64" or args.precision == "float64" else 4
     nodes, cols = result["nodes"], result["cols"]
     per_launch_cols = cols / max(1, len(result["columns"]))
-    traffic_alg = nodes * per_launch_cols * (6 * word) + nodes * per_launch_cols * word
+    words = 6.0
+    sm = result["smoother"]
+    if dominant == "fine_work" and sm.get("smoother", "chebyshev") == "chebyshev":
+        d = int(sm.get("chebyshev_degree", 3))
+        words = (2 * 9 + 2 * (d - 1) * 18) / (2 * d)
+    traffic_alg = nodes * per_launch_cols * (words * word) + nodes * word
     # DRAM bytes of one finest-level FP32 launch on this workload, from an ncu capture of that
     # launch (dram__bytes_read.sum + dram__bytes_write.sum); None for other kernels
-    traffic = {"fine_work": 434e6}.get(dominant) if args.config == CONFIG and args.precision == "float32" else None
+    traffic = None
+    if args.config == CONFIG and args.precision == "float32" and dominant == "fine_work" and sm.get("smoother", "chebyshev") == "chebyshev":
+        # ncu captures on this workload: a residual apply (degree 1 schedules) and a Chebyshev step
+        traffic = FINE_TRAFFIC.get("resid" if int(sm.get("chebyshev_degree", 3)) == 1 else "cheb")
     roof = None
     if "dominant_per_launch_ms" in result:
         achieved = traffic_alg / (result["dominant_per_launch_ms"] * 1e-3) / 1e9
@@ -533,7 +556,8 @@ def main():
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
                        "outer": "fp64 PCG", "vcycle": args.precision + (" (finest apply: tcgen05 TF32)" if result["smoother"].get("tensor_cores") else ""), "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
                        "pcg_iterations": result["iterations_max"], "smoother": result["smoother"],
-                       "smoother_choice": f"autotuned (fastest of {len(result['tuning'])} schedules / depths / finest-apply units, all to the same tolerance)" if result["tuning"] else "reference default",
+                       "smoother_choice": (f"autotuned (fastest of {len(result['tuning'])} schedules / depths / finest-apply units, all to the same tolerance)"
+                                           if result["tuning"] else ("fixed by --schedule" if args.schedule else "reference default")),
                        "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
                        "parallelism": f"rhs-sharded x{result['world']}"},
             "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),
