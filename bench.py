@@ -341,7 +341,10 @@ def simp(args):
     config = args.config if args.config != CONFIG else "plate_128x128x24"
     spec = problems.CONFIGS[config]
     domain, _, cov = problems.plate(spec["shape"], 0)
-    smoother = {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5}
+    smoother = {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0}   # the plate's autotuned schedule
+    if args.schedule:
+        degree, growth = args.schedule.split(",")
+        smoother = {"smoother": "chebyshev", "chebyshev_degree": int(degree), "growth": float(growth)}
     precisions = [args.precision] + (["float64"] if args.simp_compare and args.precision != "float64" else [])
     runs, physical = {}, {}
     for precision in precisions:
@@ -398,7 +401,7 @@ def instances(args):
     for i in range(args.instances):
         shape = sizes[int(rng.integers(len(sizes)))]
         specs.append((shape, int(rng.integers(6, 43)), i))
-    settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5}
+    settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0}
     work = []
     for shape, rhs, seed in specs:
         domain, density, cov = problems.plate(shape, seed)
