@@ -55,6 +55,37 @@ def test_direct_solver_rejects_indefinite_matrix(cuda):
     solver.close()
 
 
+@pytest.mark.parametrize("n", [1, 5, 31, 32, 33, 64, 97, 300])
+def test_direct_solver_sizes_around_panel_edges(cuda, n):
+    """The fused blocked factorisation and inversion (32-wide panels, 64 x 64 update tiles, a last
+    partial panel padded with the identity) against NumPy, two right-hand sides."""
+    from scipy.sparse import csr_matrix
+    from deep_frame_b200.direct import CudaDirectSolver
+    rng = np.random.default_rng(n)
+    m = rng.standard_normal((n, n)) / np.sqrt(n)
+    a = m @ m.T + 0.5 * np.eye(n)
+    rhs = rng.standard_normal((n, 2))
+    solver = CudaDirectSolver(csr_matrix(a), rhs)
+    x = solver.solve(csr_matrix(a), rhs)
+    want = np.linalg.solve(a, rhs)
+    assert np.linalg.norm(x - want) <= 1e-10 * np.linalg.norm(want)
+    assert solver.close() == []
+
+
+def test_direct_solver_reports_first_bad_pivot_beyond_first_panel(cuda):
+    """A diagonally dominant matrix with one negative diagonal entry at row 40 (second panel): the
+    factorisation stops being positive definite there and reports pivot 41 (1-based)."""
+    from scipy.sparse import csr_matrix
+    from deep_frame_b200.direct import CudaDirectSolver
+    n = 70
+    a = np.full((n, n), 0.01) + np.eye(n) * 4.0
+    a[40, 40] = -1.0
+    solver = CudaDirectSolver(csr_matrix(a), np.ones((n, 1)))
+    with pytest.raises(RuntimeError, match=r"pivot 41\)"):
+        solver.solve(csr_matrix(a), np.ones((n, 1)))
+    solver.close()
+
+
 def test_multigrid_system_solve_matches_direct_system_solve(cuda):
     direct, density = _system((16, 8, 8), 3)
     mg, _ = _system((16, 8, 8), 3, "multigrid", {"tolerance": 1e-12, "coarsest_dofs": 200, "precision": "float64"})
