@@ -77,8 +77,12 @@ Geo make_geo(long long ex, long long ey, long long ez) {
   return g;
 }
 
+// Column-batched elementwise launches: blockIdx.y = column, grid-stride loops along x.  The CTAs along
+// x are capped so that all columns together make about 16 CTAs per SM: with many columns, fewer and
+// longer-running CTAs stream the vectors faster than one short CTA per few hundred elements.
 inline dim3 cols_grid(long long n, int ncol, int block = 256, int cap = 1184) {
-  return dim3(grid_for(n, block, cap), ncol);
+  const int per_col = std::max(1, std::min(cap, (148 * 16 + std::max(ncol, 1) - 1) / std::max(ncol, 1)));
+  return dim3(grid_for(n, block, per_col), ncol);
 }
 
 // Optional CUDA-event timing of kernel classes on the launching stream.
