@@ -142,71 +142,6 @@ __device__ __forceinline__ void fine_node(const K0Param<T>& K, const Geo& g, con
   }
 }
 
-// ---------------------------------------------------------------------------
-// Coarse-level (Galerkin block) operator at one node for CB columns at once:
-// out[c] = sum_e B_e[c_n(e) rows, :] (mask*u_c)_e.  Each block value loaded is
-// reused for CB columns.  Blocks are stored entry-major ([576][nelem]), so the
-// threads of a warp (consecutive nodes along z) read consecutive elements and
-// every block load is one coalesced transaction.
-// ---------------------------------------------------------------------------
-template <typename T, int CB>
-__device__ __forceinline__ void block_node(const Geo& g, const T* __restrict__ B, const uint8_t* __restrict__ mask,
-                                           const T* __restrict__ u, long long colstride, int ncol,
-                                           int i, int j, int k, T out[CB][3]) {
-#pragma unroll
-  for (int c = 0; c < CB; ++c) { out[c][0] = T(0); out[c][1] = T(0); out[c][2] = T(0); }
-  long long ebase[8];
-  bool evalid[8];
-#pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    const int ei = i - 1 + (e >> 2), ej = j - 1 + ((e >> 1) & 1), ek = k - 1 + (e & 1);
-    evalid[e] = (unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez;
-    ebase[e] = evalid[e] ? (((long long)ei * g.ey + ej) * g.ez + ek) : 0;
-  }
-#pragma unroll
-  for (int di = -1; di <= 1; ++di) {
-#pragma unroll
-    for (int dj = -1; dj <= 1; ++dj) {
-#pragma unroll
-      for (int dk = -1; dk <= 1; ++dk) {
-        const int ni = i + di, nj = j + dj, nk = k + dk;
-        if (!((unsigned)ni < (unsigned)g.nx && (unsigned)nj < (unsigned)g.ny && (unsigned)nk < (unsigned)g.nz)) continue;
-        const long long node = ((long long)ni * g.ny + nj) * g.nz + nk;
-        T uv[CB][3];
-#pragma unroll
-        for (int c = 0; c < CB; ++c) {
-          if (c < ncol) load_masked(u + c * colstride, mask, node, uv[c][0], uv[c][1], uv[c][2]);
-          else { uv[c][0] = uv[c][1] = uv[c][2] = T(0); }
-        }
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
-          const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
-          if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
-          if (!evalid[e]) continue;
-          const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
-          const int cm = corner_id(cx, cy, cz);
-          const long long est = (long long)g.ex * g.ey * g.ez;
-          const T* bp = B + ebase[e] + (long long)((3 * cn) * 24 + 3 * cm) * est;
-          T b[9];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            b[3 * a + 0] = bp[(a * 24 + 0) * est];
-            b[3 * a + 1] = bp[(a * 24 + 1) * est];
-            b[3 * a + 2] = bp[(a * 24 + 2) * est];
-          }
-#pragma unroll
-          for (int c = 0; c < CB; ++c) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-              out[c][a] += b[3 * a] * uv[c][0] + b[3 * a + 1] * uv[c][1] + b[3 * a + 2] * uv[c][2];
-          }
-        }
-      }
-    }
-  }
-}
-
 // Epilogue modes of the level operators.
 enum ApplyMode : int {
   MODE_APPLY = 0,   // y = mask * A u
@@ -331,23 +266,6 @@ __host__ inline TileMap tile_map(const Geo& g) {
   m.tiles_y = (g.ny + TY - 1) / TY;
   m.tiles_z = (g.nz + m.tz - 1) / m.tz;
   return m;
-}
-
-// Stage the masked input tile of one column (3 values per node) into s[HALO][3].
-template <typename T>
-__device__ __forceinline__ void stage_tile(T* __restrict__ s, const Geo& g, const T* __restrict__ u, const uint8_t* __restrict__ mask,
-                                           int x0, int y0, int z0, int tz) {
-  const int hz = tz + 2;
-  const int count = HX * HY * hz;
-  for (int t = threadIdx.x; t < count; t += blockDim.x) {
-    const int cz = t % hz, r = t / hz, cy = r % HY, cx = r / HY;
-    const int gx = x0 - 1 + cx, gy = y0 - 1 + cy, gz = z0 - 1 + cz;
-    T v0 = T(0), v1 = T(0), v2 = T(0);
-    if ((unsigned)gx < (unsigned)g.nx && (unsigned)gy < (unsigned)g.ny && (unsigned)gz < (unsigned)g.nz)
-      load_masked(u, mask, ((long long)gx * g.ny + gy) * g.nz + gz, v0, v1, v2);
-    T* d = s + 3 * ((cx * HY + cy) * HZ + cz);
-    d[0] = v0; d[1] = v1; d[2] = v2;
-  }
 }
 
 // Stage the masked input tiles of nc <= CB columns in one pass over the halo: the mask is read once
@@ -596,90 +514,6 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
 template <typename T, int TZ, int NPT>
 constexpr size_t fine_smem_bytes() {
   return sizeof(T) * (3 * (FTXT * NPT + 2) * (TY + 2) * FineTile<T, TZ>::P + (FTXT * NPT + 1) * (TY + 1) * (TZ + 1));
-}
-
-// Galerkin levels: CB columns per CTA share every block value loaded.
-template <typename T, int CB>
-__global__ void __launch_bounds__(TX * TY * TZMAX) block_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* su = reinterpret_cast<T*>(smem_raw);   // [CB][HALO][3]
-  const int c0 = blockIdx.y * CB;
-  if (a.gate && !*a.gate) return;
-  const int nc = min(CB, a.ncol - c0);
-  bool any = false;
-  for (int c = 0; c < nc; ++c) any |= (!a.active || a.active[c0 + c]);
-  if (!any) return;
-  const Geo& g = a.g;
-  const int b = blockIdx.x;
-  const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
-  const int tz = tm.tz;
-  const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
-  const long long off = (long long)c0 * a.colstride;
-#pragma unroll
-  for (int c = 0; c < CB; ++c) {
-    if (c < nc) stage_tile(su + c * HALO * 3, g, a.u + off + c * a.colstride, a.mask, x0, y0, z0, tz);
-  }
-  __syncthreads();
-  const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
-  const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
-  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
-  const long long est = (long long)g.ex * g.ey * g.ez;
-  long long ebase[8];
-  bool evalid[8];
-#pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    const int ei = i - 1 + (e >> 2), ej = j - 1 + ((e >> 1) & 1), ek = k - 1 + (e & 1);
-    evalid[e] = (unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez;
-    ebase[e] = evalid[e] ? (((long long)ei * g.ey + ej) * g.ez + ek) : 0;
-  }
-  T out[CB][3];
-#pragma unroll
-  for (int c = 0; c < CB; ++c) { out[c][0] = T(0); out[c][1] = T(0); out[c][2] = T(0); }
-  const int cbase = 3 * (((lx + 1) * HY + (ly + 1)) * HZ + (lz + 1));
-#pragma unroll
-  for (int di = -1; di <= 1; ++di) {
-#pragma unroll
-    for (int dj = -1; dj <= 1; ++dj) {
-#pragma unroll
-      for (int dk = -1; dk <= 1; ++dk) {
-        const int noff = cbase + 3 * ((di * HY + dj) * HZ + dk);
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
-          const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
-          if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
-          const int cn = corner_id(1 - ox, 1 - oy, 1 - oz);
-          const int cm = corner_id(cx, cy, cz);
-          T bv[9];
-          if (evalid[e]) {
-            const T* bp = a.E + ebase[e] + (long long)((3 * cn) * 24 + 3 * cm) * est;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-              bv[3 * q + 0] = bp[(q * 24 + 0) * est];
-              bv[3 * q + 1] = bp[(q * 24 + 1) * est];
-              bv[3 * q + 2] = bp[(q * 24 + 2) * est];
-            }
-          } else {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) bv[q] = T(0);
-          }
-#pragma unroll
-          for (int c = 0; c < CB; ++c) {
-            const T* p = su + c * HALO * 3 + noff;
-            const T u0 = p[0], u1 = p[1], u2 = p[2];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) out[c][q] = fma(bv[3 * q + 2], u2, fma(bv[3 * q + 1], u1, fma(bv[3 * q], u0, out[c][q])));
-          }
-        }
-      }
-    }
-  }
-  const long long n = ((long long)i * g.ny + j) * g.nz + k;
-  const unsigned m = a.mask ? a.mask[n] : 7u;
-#pragma unroll
-  for (int c = 0; c < CB; ++c) {
-    if (c < nc && (!a.active || a.active[c0 + c])) epilogue(a, mode, off + c * a.colstride, n, m, out[c]);
-  }
 }
 
 // Galerkin levels as assembled 27-point stencils: S[(d * 9 + 3 q + r)][node] is the 3 x 3 coupling of

@@ -19,7 +19,7 @@ struct PcgState {
   int* iters;
   int* flags;              // [0] any candidate this step, [1] number of active columns
   unsigned long long* hist;  // bit patterns of non-negative doubles, one per step
-  double* partial;         // [ncol][blocks][2]
+  double* partial;         // [ncol][blocks][2] (two-value reductions) or [4] (three-value)
   unsigned* count;         // [ncol]
   int ncol;
 };
