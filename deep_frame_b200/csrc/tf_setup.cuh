@@ -405,18 +405,22 @@ __global__ void jacobi_first_kernel(long long ndof, const T* __restrict__ inv, c
     x[off + t] = s * inv[t] * b[off + t];
 }
 
-// Chebyshev start from a zero guess: res = b, d = inv * res / theta, x = d.
+// Chebyshev start from a zero guess: res = b, d = inv * res / theta, x = d (with has_x: x += d, res
+// kept).  Without write_rd only x is written: a one-sweep smoother reads neither res nor d again.
 template <typename T>
 __global__ void cheb_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ res,
-                                  T* __restrict__ d, T* __restrict__ x, T inv_theta, int has_x, const int* __restrict__ active) {
+                                  T* __restrict__ d, T* __restrict__ x, T inv_theta, int has_x, int write_rd,
+                                  const int* __restrict__ active) {
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const long long off = (long long)col * ndof;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x) {
     const T r = has_x ? res[off + t] : b[off + t];
     const T dv = inv[t] * r * inv_theta;
-    res[off + t] = r;
-    d[off + t] = dv;
+    if (write_rd) {
+      res[off + t] = r;
+      d[off + t] = dv;
+    }
     x[off + t] = has_x ? x[off + t] + dv : dv;
   }
 }

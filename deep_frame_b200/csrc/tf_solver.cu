@@ -545,9 +545,10 @@ void smooth(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, bool first, int nc
     a.y = vb.res[l].template as<T>();
     launch_level<T>(h, l, a, MODE_RESID, st);
   }
+  // with one sweep nothing reads res or d afterwards (the V-cycle's next residual apply rewrites res)
   cheb_first_kernel<T><<<ge, 256, 0, st>>>(nd, a.inv, vb.b[l].template as<T>(), vb.res[l].template as<T>(),
                                            vb.d[l].template as<T>(), vb.x[l].template as<T>(), static_cast<T>(1.0 / theta),
-                                           first ? 0 : 1, active);
+                                           first ? 0 : 1, count > 1 ? 1 : 0, active);
   TF_LAUNCH_CHECK("cheb_first_kernel");
   for (int k = 1; k < count; ++k) {
     const double rn = 1.0 / (2.0 * sigma - rho);
