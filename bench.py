@@ -32,6 +32,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "42-RHS hex8 solve s @1e-8 resid; SIMP iter/s: learned+mixed vs plain FP64"
 CONFIG = "plate_96x96x16"
+PLATES = ("plate_96x96x16", "plate_128x128x24", "plate_192x192x32", "plate_352x352x48")
 
 
 def parse():
@@ -40,7 +41,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--config", default=CONFIG, choices=PLATES,
+                    help="covariance plate workload (the 48 x 24 x 24 cantilever is a parity case of the tests, not a bench line)")
     ap.add_argument("--precision", default="float32")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
