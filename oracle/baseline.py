@@ -18,10 +18,10 @@ over groups.  Per-column cost falls as a batched block grows, so when share > bl
 scaling overstates the CPU time somewhat; with at least as many workers per group as columns
 (share = 1 <= block) nothing is scaled.
 """
-import math
 import multiprocessing as mp
 import os
 import time
+from concurrent.futures import ProcessPoolExecutor
 
 import numpy as np
 
@@ -29,40 +29,56 @@ import numpy as np
 _THREAD_VARS = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS")
 
 
+def _read(path):
+    try:
+        with open(path) as f:
+            return f.read().strip()
+    except OSError:
+        return None
+
+
 def host_cores():
-    """Cores this process may use: its CPU affinity, capped by a cgroup v2 CPU quota if one is set."""
+    """Cores this process may use: its CPU affinity, capped by a cgroup CPU quota if one is set
+    (``cpu.max`` of cgroup v2, else ``cpu.cfs_quota_us`` / ``cpu.cfs_period_us`` of cgroup v1)."""
     cores = len(os.sched_getaffinity(0))
     try:
-        with open("/sys/fs/cgroup/cpu.max") as f:
-            quota, period = f.read().split()[:2]
-        if quota != "max":
-            cores = min(cores, max(1, int(int(quota) // int(period))))
-    except (OSError, ValueError):
+        v2 = _read("/sys/fs/cgroup/cpu.max")
+        if v2 is not None:
+            quota, period = v2.split()[:2]
+            if quota != "max":
+                cores = min(cores, max(1, int(quota) // int(period)))
+        else:
+            quota, period = _read("/sys/fs/cgroup/cpu/cpu.cfs_quota_us"), _read("/sys/fs/cgroup/cpu/cpu.cfs_period_us")
+            if quota is not None and period is not None and int(quota) > 0:
+                cores = min(cores, max(1, int(quota) // int(period)))
+    except ValueError:
         pass
     return cores
 
 
 def available_bytes():
     """Host memory this process may still use, in bytes: MemAvailable of /proc/meminfo, capped by
-    the room left under a cgroup v2 memory limit if one is set (None where neither is readable)."""
+    the room left under a cgroup memory limit if one is set (v2 ``memory.max`` - ``memory.current``,
+    else v1 ``memory.limit_in_bytes`` - ``memory.usage_in_bytes``); None where nothing is readable."""
     avail = None
-    try:
-        with open("/proc/meminfo") as f:
-            for line in f:
-                if line.startswith("MemAvailable:"):
-                    avail = int(line.split()[1]) * 1024
-                    break
-    except (OSError, ValueError):
-        pass
-    try:
-        with open("/sys/fs/cgroup/memory.max") as f:
-            limit = f.read().strip()
-        if limit != "max":
-            with open("/sys/fs/cgroup/memory.current") as f:
-                room = int(limit) - int(f.read().strip())
+    info = _read("/proc/meminfo")
+    if info:
+        for line in info.splitlines():
+            if line.startswith("MemAvailable:"):
+                avail = int(line.split()[1]) * 1024
+                break
+    for limit_path, used_path in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                                  ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        limit, used = _read(limit_path), _read(used_path)
+        if limit is None or used is None:
+            continue
+        try:
+            room = int(limit) - int(used)
+        except ValueError:          # "max": no limit
+            break
+        if int(limit) < (1 << 60):  # v1 reports "no limit" as a huge number
             avail = room if avail is None else min(avail, room)
-    except (OSError, ValueError):
-        pass
+        break
     return avail
 
 
@@ -122,25 +138,28 @@ def _solve_block(task):
 class ParallelBaseline:
     """Spawn-started pool of single-threaded oracle workers, reused across samples.
 
-    ``spawn`` keeps the workers independent of any CUDA context the parent holds."""
+    ``spawn`` keeps the workers independent of any CUDA context the parent holds.  A worker that
+    dies (killed for memory, say) breaks the pool: the sample raises ``BrokenProcessPool`` instead
+    of waiting for a task that will never finish."""
 
     def __init__(self, workers):
         self.workers = int(workers)
-        saved = {k: os.environ.get(k) for k in _THREAD_VARS}
+        # the thread caps must be in the environment when the workers start (they start on the first
+        # submit), so they stay set while the pool lives and are restored by close()
+        self._saved = {k: os.environ.get(k) for k in _THREAD_VARS}
         for k in _THREAD_VARS:
             os.environ[k] = "1"
-        try:
-            self.pool = mp.get_context("spawn").Pool(self.workers)
-        finally:
-            for k, v in saved.items():
+        self.pool = ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn"))
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.shutdown(wait=True, cancel_futures=True)
+            self.pool = None
+            for k, v in self._saved.items():
                 if v is None:
                     os.environ.pop(k, None)
                 else:
                     os.environ[k] = v
-
-    def close(self):
-        self.pool.close()
-        self.pool.join()
 
     def __enter__(self):
         return self
@@ -163,7 +182,7 @@ class ParallelBaseline:
                 owner.append((g, share))
                 start += share
         t0 = time.perf_counter()
-        results = self.pool.map(_solve_block, tasks, chunksize=1)
+        results = list(self.pool.map(_solve_block, tasks))
         wall = time.perf_counter() - t0
         estimate = 0.0
         per_group = []
