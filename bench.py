@@ -497,7 +497,7 @@ def learned_guess(args):
         cases["plate_%dx%dx%d" % shape] = learned.compare(net, dom, cv, moduli, multigrid=settings)
     policy = learned.GuessPolicy(net)
     for row in cases.values():
-        policy.judge(row["network"]["mean_iterations"], row["zero"]["mean_iterations"])
+        policy.assess(row["network"]["mean_iterations"], row["zero"]["mean_iterations"])
     line = {"metric": "PCG iterations / seconds to 1e-8 with and without the learned initial guess", "unit": "iterations",
             "n_gpus": 1, "data": "synthetic (SIMP trajectory snapshots of seeded plates)",
             "config": {"network": "3-level conv encoder/decoder, channels (8, 16, 32), 9 conv layers, FP32, hand-written kernels",

@@ -970,10 +970,10 @@ int guard(tf_handle* h, F&& f) {
 
 void validate_settings(const tf_settings& s) {
   require(s.precision >= TF_PRECISION_FLOAT64 && s.precision <= TF_PRECISION_FLOAT16, "invalid precision");
-  require(s.precision <= TF_PRECISION_FLOAT32, "bfloat16/float16 work precision is not available in this build");
+  require(s.precision <= TF_PRECISION_FLOAT32, "bfloat16/float16 work precision is not available in this library");
   require(s.smoother == TF_SMOOTHER_JACOBI || s.smoother == TF_SMOOTHER_CHEBYSHEV, "invalid smoother");
   require(s.cycle == TF_CYCLE_V || s.cycle == TF_CYCLE_W, "invalid cycle");
-  require(s.coarse == TF_COARSE_GALERKIN, "only Galerkin coarse operators are available in this build");
+  require(s.coarse == TF_COARSE_GALERKIN, "only Galerkin coarse operators are available in this library");
   require(s.sweeps >= 1 && s.chebyshev_degree >= 1, "sweeps and chebyshev_degree must be positive");
   require(s.max_levels >= 2 && s.max_levels <= 16, "max_levels must be in [2, 16]");
   require(s.power_iterations >= 1, "power_iterations must be positive");

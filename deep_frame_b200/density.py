@@ -10,7 +10,7 @@ cells, ``filtered``, ``project`` (single and robust tanh projections),
 and the whole OC multiplier search run in libtfb200.so; host-array methods keep
 the reference's NumPy signatures and the ``*_device`` methods take and return
 CUDA tensors.  Corridor blends and prop-disc volume weights of the reference
-are not part of this build.
+are not part of this library.
 """
 import ctypes
 
@@ -115,7 +115,7 @@ class DensityMap:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.settings = settings
         if settings.get("corridor") is not None or settings.get("prop_discs") is not None:
-            raise NotImplementedError("corridor blends and prop-disc volume weights are not part of this build")
+            raise NotImplementedError("corridor blends and prop-disc volume weights are not part of this library")
         self.beta = settings["beta_schedule"][0] if settings.get("beta_schedule") else settings["projection_beta"]
         self.robust = settings.get("projection", "single") == "robust"
         eta, delta = settings["projection_eta"], settings.get("robust_delta", 0.25)

@@ -4,7 +4,7 @@ The network maps, per load column, the node fields (load f scaled by max|f|, log
 stiffness, live mask) to the shape of the displacement u (the target is u / rms(u)); the scale of
 the guess is then fixed by one operator apply, x0 = alpha y with alpha = (y . f) / (y . K y), the
 energy-optimal multiple of the prediction.  It is trained on (density, load, displacement) snapshots
-the solver itself produces along SIMP trajectories and judged by the iterations GMG-PCG needs from
+the solver itself produces along SIMP trajectories and assessed by the iterations GMG-PCG needs from
 its guess to the same tolerance; ``GuessPolicy`` drops it whenever it does not reduce them.
 
 Layers (channel-major FP32 node grids, every kernel in libtfb200.so, deterministic):
@@ -210,7 +210,7 @@ class GuessPolicy:
     def __init__(self, net):
         self.net, self.enabled, self.record = net, True, []
 
-    def judge(self, iterations_with, iterations_without):
+    def assess(self, iterations_with, iterations_without):
         self.record.append((int(iterations_with), int(iterations_without)))
         if iterations_with >= iterations_without:
             self.enabled = False

@@ -15,7 +15,7 @@ back through the filter on the device; the OC multiplier search runs on the
 device (``tf_oc_update``).  Robust runs use beta continuation with the
 reference's level rules and the relaxed dilated-volume target.  Modal
 constraints, corridor blends and prop-disc volume weights are not part of
-this build and are rejected as invalid settings.
+this library and are rejected as invalid settings.
 """
 from copy import deepcopy
 from time import perf_counter
@@ -126,7 +126,7 @@ def _settings(settings):
         raise ValueError("Invalid beta continuation settings")
     for name, what in (("modal", "modal constraints"), ("corridor", "corridor blends"), ("prop_discs", "prop-disc volume weights")):
         if result[name] is not None:
-            raise ValueError(f"{what} are not part of this build")
+            raise ValueError(f"{what} are not part of this library")
     return result
 
 

@@ -72,5 +72,5 @@ def test_trajectory_training_and_guess_pipeline(cuda):
     result = learned.compare(net, domain, cov, snapshots[3][0], multigrid=settings)
     assert result["zero"]["mean_iterations"] > 0 and result["network"]["mean_iterations"] > 0
     policy = learned.GuessPolicy(net)
-    kept = policy.judge(result["network"]["mean_iterations"], result["zero"]["mean_iterations"])
+    kept = policy.assess(result["network"]["mean_iterations"], result["zero"]["mean_iterations"])
     assert kept == (result["network"]["mean_iterations"] < result["zero"]["mean_iterations"])
