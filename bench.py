@@ -74,6 +74,29 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+# CUDA-core lanes per SM of sm_100 (FP32 FMA and FP64 FMA) and its SM count: the nominal non-tensor
+# peaks are lanes x 2 flop x SMs x SM clock.  No measured figure exists for these pipes.
+FMA_LANES = {"fp32": 128, "fp64": 64}
+SMS = 148
+
+
+def fma_roof(precision, flops_per_launch, per_launch_ms, sm_mhz=None, sm_max_mhz=1965.0):
+    """Compute side of the dominant kernel's roofline: its algorithmic flops per launch over the
+    launch time, against the nominal CUDA-core FMA peak at the maximum SM clock and, when clocks
+    were sampled, at the median SM clock seen under load."""
+    achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
+    lanes = FMA_LANES[precision]
+    peak_max = lanes * 2 * SMS * sm_max_mhz * 1e6 / 1e12
+    out = {"bound": "fma", "pipe": precision, "achieved": round(achieved, 2), "unit": "TFLOP/s",
+           "peak": round(peak_max, 1), "frac": round(achieved / peak_max, 4), "peak_source": "nominal at the maximum SM clock",
+           "flops_per_launch": int(flops_per_launch)}
+    if sm_mhz:
+        peak_seen = lanes * 2 * SMS * sm_mhz * 1e6 / 1e12
+        out["peak_at_sampled_clock"] = round(peak_seen, 1)
+        out["frac_at_sampled_clock"] = round(achieved / peak_seen, 4)
+    return out
+
+
 class Clocks:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -555,6 +578,10 @@ def main():
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "traffic": traffic, "kernel": dominant, "peak_source": source,
                 "per_launch_ms": round(result["dominant_per_launch_ms"], 4), "algorithmic_bytes_per_launch": int(traffic_alg)}
+        # the same launch against the CUDA-core FMA pipe that bounds it: 576 FMA (1152 flop) per node and column
+        clk = result["clocks"] or {}
+        roof["compute"] = fma_roof("fp64" if word == 8 else "fp32", 1152.0 * nodes * per_launch_cols, result["dominant_per_launch_ms"],
+                                   clk.get("sm_mhz"), clk.get("sm_max_mhz") or 1965.0)
     cpu = None
     if not args.no_cpu and result["world"] == 1:
         try:
