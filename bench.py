@@ -248,7 +248,8 @@ def ours(args):
               "world": world, "rank": rank, "columns": [len(g["local"]) for g in measure.groups], "ndof": system.ndof,
               "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in timed),
               "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores", "coarsest_dofs")},
-              "tuning": tuning, "tr": rows[0]["value"], "lambda_max": rows[1]["value"]}
+              "tuning": tuning, "tr": rows[0]["value"], "lambda_max": rows[1]["value"],
+              "grad_mean": rows[0]["gradient"].cpu().numpy(), "grad_worst": rows[1]["gradient"].cpu().numpy()}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     result["dominant"] = dominant
     if breakdown[dominant]["launches"]:
@@ -533,6 +534,24 @@ def learned_guess(args):
     print(json.dumps(line))
 
 
+def oracle_errors(config, result):
+    """Relative errors of the step's tr, lambda_max and sensitivity fields against the FP64 oracle
+    values of the same workload (tests/golden/<workload>.npz, from tests/golden/make_plate_oracle.py:
+    the oracle's GMG-PCG to a 1e-10 true relative residual); None when no such file exists."""
+    path = ROOT / "tests" / "golden" / f"{config}.npz"
+    if not path.exists():
+        return None
+    ref = np.load(path)
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a) - b) / np.linalg.norm(b))
+
+    return {"oracle": f"FP64 GMG-PCG to {float(ref['tolerance']):g} (tests/golden/{path.name})",
+            "tr_rel": rel(result["tr"], ref["tr"]), "lambda_max_rel": rel(result["lambda_max"], ref["lambda_max"]),
+            "grad_mean_rel": rel(result["grad_mean"], ref["grad_mean"]), "grad_worst_rel": rel(result["grad_worst"], ref["grad_worst"]),
+            "bars": {"tr": 1e-6, "lambda_max": 1e-6, "sensitivities": 1e-5}}
+
+
 def main():
     args = parse()
     if args.learned:
@@ -609,6 +628,9 @@ def main():
         line["e2e_solve_api"] = {"value": round(a["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": a["h2d_bytes_per_step"],
                                  "d2h_bytes_per_step": a["d2h_bytes_per_step"], "call": "GeometricMultigrid.update + .solve per half with host NumPy forces and solutions"}
     line["results"] = {"tr_K_inv_sigma": result["tr"], "lambda_max": result["lambda_max"]}
+    parity = oracle_errors(args.config, result)
+    if parity:
+        line["results"]["vs_fp64_oracle"] = parity
     print(json.dumps(line))
 
 

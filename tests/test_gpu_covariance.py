@@ -64,3 +64,27 @@ def test_gram_is_reproducible_and_exact(cuda):
     assert np.array_equal(results[0], results[1])
     expected = a.cpu().numpy() @ b.cpu().numpy().T
     assert np.max(np.abs(results[0] - expected)) < 1e-9 * np.max(np.abs(expected))
+
+
+@pytest.mark.parametrize("precision", ["float32", "float64"])
+def test_benchmark_plate_matches_fp64_oracle(cuda, precision):
+    """The benchmark workload itself (96 x 96 x 16 plate, seed 0, 2 x 42 columns solved to the
+    benchmark's 1e-8) against the FP64 oracle of tests/golden/plate_96x96x16.npz (the oracle's
+    GMG-PCG to 1e-10; made by tests/golden/make_plate_oracle.py): tr and lambda_max within 1e-6
+    relative, both sensitivity fields within 1e-5 relative (2-norm)."""
+    from pathlib import Path
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    ref = np.load(Path(__file__).resolve().parent / "golden" / "plate_96x96x16.npz")
+    domain, density, cov = problems.plate((96, 96, 16), 0)
+    system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": 1e-8})
+    model = InterfaceCovariance(system, cov, domain["interfaces"])
+    rows = {row["name"]: row for row in model.measure_device(density, 3.0, 1e-9)}
+    assert rows["load_mean"]["value"] == pytest.approx(float(ref["tr"]), rel=1e-6)
+    assert rows["load_worst"]["value"] == pytest.approx(float(ref["lambda_max"]), rel=1e-6)
+    assert rows["load_worst"]["info"]["ks_n_mm"] == pytest.approx(float(ref["ks"]), rel=1e-6)
+    for name, key in (("load_mean", "grad_mean"), ("load_worst", "grad_worst")):
+        got = rows[name]["gradient"].cpu().numpy()
+        assert np.linalg.norm(got - ref[key]) < 1e-5 * np.linalg.norm(ref[key]), name
+    system.close()

@@ -130,3 +130,14 @@ def test_oracle_covariance_matches_reference_measure():
     assert np.linalg.norm(res["grad_mean"] - g["grad_mean"]) < 1e-8 * np.linalg.norm(g["grad_mean"])
     assert np.linalg.norm(res["grad_worst"] - g["grad_worst"]) < 1e-8 * np.linalg.norm(g["grad_worst"])
     assert np.allclose(ocov.directions(g["sigma"]), g["directions"], atol=1e-12 * np.abs(g["directions"]).max())
+
+
+def test_benchmark_plate_fixture_is_converged():
+    """tests/golden/plate_96x96x16.npz (tests/golden/make_plate_oracle.py): every one of the 84
+    columns reached the fixture's FP64 tolerance, and the measures are consistent (tr >= lambda_max,
+    KS >= lambda_max, sensitivities of energies with a positive SIMP slope are <= 0)."""
+    g = golden("plate_96x96x16")
+    assert g["relative"].shape == (84,) and np.all(g["relative"] < g["tolerance"]) and g["tolerance"] <= 1e-10
+    assert float(g["tr"]) > float(g["lambda_max"]) > 0 and float(g["ks"]) >= float(g["lambda_max"])
+    for key in ("grad_mean", "grad_worst"):
+        assert g[key].shape == (96 * 96 * 16,) and np.all(np.isfinite(g[key])) and np.all(g[key] <= 0)
