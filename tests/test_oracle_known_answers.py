@@ -1,0 +1,126 @@
+"""Known answers the oracle must reproduce, after the reference's own physics tests.  No GPU.
+
+* Euler-Bernoulli tip deflection (8 %) and first bending frequency (5 %) of a slender clamped
+  hex8 beam (reference tests/test_topology_optimization.py:56-68);
+* compliance sensitivity through SIMP, the cone filter and the projection against central
+  finite differences, relative 2e-5, and the volume derivative (:70-89);
+* tr(K^-1 Sigma) and the KS aggregate of the covariance eigenvalues against central finite
+  differences in the physical densities, relative 1e-5 (reference
+  tests/test_topology_problem.py:510-528).
+
+The device results are held to the oracle elsewhere (the tests marked gpu), so these close the
+chain from the kernels to the physics.
+"""
+import numpy as np
+import pytest
+from scipy.sparse.linalg import eigsh, splu
+
+from oracle import covariance as ocov
+from oracle import hex8, operator as op
+from oracle.density import DensityMapOracle
+
+
+def clamped_beam(shape):
+    nodes = tuple(n + 1 for n in shape)
+    i = np.indices(nodes).reshape(3, -1)
+    clamp = np.flatnonzero(i[0] == 0)
+    tip = np.flatnonzero(i[0] == shape[0])
+    fixed = (3 * clamp[:, None] + np.arange(3)).ravel()
+    free = np.setdiff1d(np.arange(3 * int(np.prod(nodes))), fixed)
+    return tip, free
+
+
+def test_cantilever_deflection_and_frequency_against_euler_bernoulli():
+    shape, spacing = (24, 4, 4), (2.0, 1.5, 1.5)
+    young, rho = 4430.0, 1.09e-9
+    k0, m0, _ = hex8.element_matrices(spacing, 0.3)
+    nelem = int(np.prod(shape))
+    stiffness = op.assemble(shape, k0, np.full(nelem, young)).tocsc()
+    mass = op.assemble(shape, m0, np.full(nelem, rho)).tocsc()
+    tip, free = clamped_beam(shape)
+    force = np.zeros(stiffness.shape[0])
+    force[3 * tip + 2] = -1.0 / len(tip)                  # 1 N in -z spread over the end face
+    u = np.zeros_like(force)
+    u[free] = splu(stiffness[free][:, free]).solve(force[free])
+    deflection = -np.mean(u[3 * tip + 2])
+    length, width, height = np.asarray(shape) * spacing
+    second_moment = width * height ** 3 / 12
+    assert deflection == pytest.approx(length ** 3 / (3 * young * second_moment), rel=0.08)
+    omega2 = eigsh(stiffness[free][:, free], k=1, M=mass[free][:, free], sigma=0, which="LM")[0][0]
+    expected = 1.875104068711961 ** 2 / (2 * np.pi * length ** 2) * np.sqrt(young * second_moment / (rho * width * height))
+    assert np.sqrt(omega2) / (2 * np.pi) == pytest.approx(expected, rel=0.05)
+
+
+def test_filtered_projected_compliance_sensitivity_matches_finite_difference():
+    shape, spacing = (5, 3, 3), (2.0, 2.0, 2.0)
+    young, p, eps = 4430.0, 3.0, 1e-9
+    preserve = np.zeros(shape, dtype=bool)
+    preserve[0] = True
+    preserve[-1] = True
+    mapping = DensityMapOracle(shape, spacing, 3.1, np.ones(shape, dtype=bool), preserve, beta=2.0)
+    k0 = hex8.element_matrices(spacing, 0.3)[0]
+    tip, free = clamped_beam(shape)
+    force = np.zeros(3 * int(np.prod(np.asarray(shape) + 1)))
+    force[3 * tip + 2] = -1.0 / len(tip)
+
+    def compliance(design, gradient=False):
+        physical, projection = mapping.physical(design)
+        moduli, slope = hex8.simp(physical, p, eps, young)
+        k = op.assemble(shape, k0, moduli).tocsc()
+        u = np.zeros_like(force)
+        u[free] = splu(k[free][:, free]).solve(force[free])
+        value = float(force @ u)
+        if not gradient:
+            return value
+        return value, mapping.pullback(-slope * op.element_energy(shape, k0, u), projection), projection
+
+    design = np.full(mapping.n, 0.65)
+    design[mapping.preserve.ravel()] = 1.0
+    _, derivative, projection = compliance(design, gradient=True)
+    volume_derivative = mapping.pullback(np.ones(mapping.n), projection)
+    direction = np.random.default_rng(42).normal(size=mapping.n)
+    direction[~mapping.free.ravel()] = 0.0
+    direction /= np.linalg.norm(direction)
+    step = 1e-5
+    fd = (compliance(design + step * direction) - compliance(design - step * direction)) / (2 * step)
+    assert derivative @ direction == pytest.approx(fd, rel=2e-5, abs=1e-10)
+    plus, minus = mapping.physical(design + step * direction)[0], mapping.physical(design - step * direction)[0]
+    assert volume_derivative @ direction == pytest.approx((plus.sum() - minus.sum()) / (2 * step), rel=1e-7)
+
+
+def test_covariance_trace_and_ks_gradients_match_finite_differences():
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    shape = (16, 12, 4)
+    domain, density, cov = problems.plate(shape, 3)
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, cov, domain["interfaces"])
+    index = {name: k for k, name in enumerate(model.cases)}
+    halves = []
+    for members in system.groups.values():
+        forces = np.zeros((system.ndof, model.rank))
+        for case, part in members:
+            forces[:, index[case["name"]]] = part["force"]
+        halves.append((forces, members[0][1]["fixed"]))
+
+    def measure(physical):
+        moduli, slope = system.moduli(physical, 3.0, 1e-9)
+        k = op.assemble(shape, system.ke, moduli).tocsc()
+        parts = []
+        for forces, fixed in halves:
+            live = op.live_dofs(shape, moduli, fixed)
+            u = np.zeros_like(forces)
+            u[live] = splu(k[live][:, live].tocsc()).solve(forces[live])
+            parts.append((forces, u))
+        # KS with a fixed scale (the constraint limit), as the reference's load_worst constraint uses
+        return ocov.measure(parts, model.factor, shape, system.ke, slope, ks=5.0, limit_worst=40.0)
+
+    rng = np.random.default_rng(5)
+    physical = rng.uniform(0.3, 0.7, int(np.prod(shape)))
+    direction = rng.standard_normal(physical.size)
+    step = 1e-5
+    at, plus, minus = measure(physical), measure(physical + step * direction), measure(physical - step * direction)
+    assert at["grad_mean"] @ direction == pytest.approx((plus["load_mean"] - minus["load_mean"]) / (2 * step), rel=1e-5)
+    assert at["grad_worst"] @ direction == pytest.approx((plus["ks"] - minus["ks"]) / (2 * step), rel=1e-5)
+    assert at["ks"] >= at["load_worst"]
