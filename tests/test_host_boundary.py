@@ -1,0 +1,70 @@
+"""Host side of the drop-in boundary on a machine without a CUDA device.  No GPU.
+
+The reference pins "no CPU fallback" (tests/test_topology_optimization.py:406-416): when the GPU
+solver cannot run, the OC driver reports status "failed" with the error and an empty history
+instead of solving on the CPU, and unknown solver names are "invalid" (:400-404).  The same
+holds here, and every device entry point fails loudly before any work.
+"""
+import numpy as np
+import pytest
+import torch
+
+from deep_frame_b200 import _lib
+
+no_cuda = pytest.mark.skipif(torch.cuda.is_available(), reason="checks the path of a host without a CUDA device")
+
+
+def beam_domain(shape=(5, 3, 3), spacing=2.0):
+    extent = np.array(shape) * spacing
+    return {"grid": {"shape": list(shape), "spacing_mm": [spacing] * 3, "origin_mm": [0.0] * 3, "order": "C", "axis_order": "xyz"},
+            "allowed": np.ones(shape, bool), "preserve": np.zeros(shape, bool), "forbidden": np.zeros(shape, bool),
+            "material": {"young_modulus_mpa": 4430.0, "poisson_ratio": 0.3, "density_g_cm3": 1.09}, "point_masses": [],
+            "load_cases": [{"name": "tip", "analysis": "static",
+                            "fixed_regions": [{"kind": "box", "min_mm": [-0.01] * 3, "max_mm": [0.01, extent[1] + 0.01, extent[2] + 0.01]}],
+                            "loads": [{"region": {"kind": "box", "min_mm": [extent[0] - 0.01, -0.01, -0.01], "max_mm": (extent + 0.01).tolist()},
+                                       "force_n": [0.0, 0.0, -1.0]}]}]}
+
+
+@no_cuda
+def test_oc_driver_fails_without_cpu_fallback():
+    from deep_frame_b200.topology_optimization import optimize_topology
+    result = optimize_topology(beam_domain(), {"volume_fraction": 0.65, "filter_radius_mm": 3.1})
+    assert result["status"] == "failed"
+    assert result["history"] == [] and len(result["diagnostics"]) == 1 and result["diagnostics"][0]
+
+
+def test_unknown_linear_solver_is_invalid():
+    from deep_frame_b200.topology_optimization import _settings, optimize_topology
+    with pytest.raises(ValueError, match="linear_solver"):
+        _settings({"linear_solver": "fake_gpu"})
+    result = optimize_topology(beam_domain(), {"linear_solver": "fake_gpu"})
+    assert result["status"] == "invalid" and "linear_solver" in result["diagnostics"][0]
+
+
+@no_cuda
+def test_multigrid_refuses_to_run_on_the_cpu():
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    from deep_frame_b200.elements import hexahedron_matrices
+    ke = hexahedron_matrices((1.0, 1.0, 1.0), 0.3)[0]
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        GeometricMultigrid((4, 4, 4), (1.0, 1.0, 1.0), ke, {"device": "cpu"})
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        GeometricMultigrid((4, 4, 4), (1.0, 1.0, 1.0), ke)
+
+
+def test_multigrid_settings_are_validated_and_translated():
+    from deep_frame_b200.topology_multigrid import MULTIGRID, _native_settings
+    native = _native_settings(dict(MULTIGRID, smoother="jacobi", cycle="W", sweeps=3, tolerance=1e-9, batch=12, tensor_cores=True))
+    assert native.smoother == _lib.SMOOTHER["jacobi"] and native.cycle == _lib.CYCLE["W"]
+    assert native.sweeps == 3 and native.tolerance == 1e-9 and native.batch == 12 and native.tensor_cores == 1
+    assert native.coarsest_dofs == MULTIGRID["coarsest_dofs"] and native.chebyshev_degree == MULTIGRID["chebyshev_degree"]
+    for bad in ({"precision": "int8"}, {"smoother": "gauss_seidel"}, {"cycle": "F"}, {"coarse": "algebraic"}):
+        with pytest.raises(ValueError, match="Invalid multigrid settings"):
+            _native_settings(dict(MULTIGRID, **bad))
+
+
+def test_missing_library_raises_instead_of_falling_back(monkeypatch, tmp_path):
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIBRARY", tmp_path / "libtfb200.so")
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        _lib.load()
