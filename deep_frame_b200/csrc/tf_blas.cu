@@ -68,8 +68,10 @@ __global__ void gram_reduce_kernel(const double* __restrict__ partial, int pairs
 
 extern "C" int tf_gram(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
                        double* scratch_dev, void* stream) {
-  if (ra < 1 || rb < 1 || ra > GRAM_MAX || rb > GRAM_MAX || n < 1 || !a_dev || !b_dev || !out_dev || !scratch_dev)
+  if (ra < 1 || rb < 1 || ra > GRAM_MAX || rb > GRAM_MAX || n < 1 || !a_dev || !b_dev || !out_dev || !scratch_dev) {
+    record_unhandled_error("tf_gram: need 1 <= ra, rb <= 64, n >= 1 and non-NULL pointers");
     return TF_INVALID;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = static_cast<int>(std::min<long long>(GRAM_BLOCKS, (n + KC - 1) / KC));
   gram_partial_kernel<<<blocks, 256, 0, s>>>(a_dev, ra, b_dev, rb, n, scratch_dev);

@@ -40,6 +40,8 @@ extern std::atomic<long long> g_launch_count;
 
 // Store the message tf_last_error(NULL) returns (entry points without a handle).
 void record_unhandled_error(const std::string& message);
+// This thread's last such message (also what tf_filter/mma/chol_last_error(NULL) return).
+const char* unhandled_error();
 
 inline void require(bool ok, const std::string& m) {
   if (!ok) throw Error(TF_INVALID, m);

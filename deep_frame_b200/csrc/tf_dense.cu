@@ -552,4 +552,4 @@ extern "C" int tf_chol_destroy(tf_chol* h) {
   return tfb::TF_OK;
 }
 
-extern "C" const char* tf_chol_last_error(const tf_chol* h) { return h ? h->err.c_str() : ""; }
+extern "C" const char* tf_chol_last_error(const tf_chol* h) { return h ? h->err.c_str() : tfb::unhandled_error(); }

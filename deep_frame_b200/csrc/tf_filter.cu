@@ -392,7 +392,7 @@ extern "C" int tf_filter_destroy(tf_filter* h) {
   return TF_OK;
 }
 
-extern "C" const char* tf_filter_last_error(const tf_filter* h) { return h ? h->err.c_str() : ""; }
+extern "C" const char* tf_filter_last_error(const tf_filter* h) { return h ? h->err.c_str() : unhandled_error(); }
 
 namespace {
 void ensure_reduction(tf_filter* h, cudaStream_t s) {

@@ -367,7 +367,7 @@ extern "C" int tf_mma_destroy(tf_mma* h) {
   return TF_OK;
 }
 
-extern "C" const char* tf_mma_last_error(const tf_mma* h) { return h ? h->err.c_str() : ""; }
+extern "C" const char* tf_mma_last_error(const tf_mma* h) { return h ? h->err.c_str() : unhandled_error(); }
 
 extern "C" int tf_mma_step(tf_mma* h, int32_t iteration, const double* xval, const double* xmin, const double* xmax,
                            const double* xold1, const double* xold2, const double* df0dx, const double* fval, const double* dfdx,

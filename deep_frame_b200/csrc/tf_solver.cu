@@ -995,6 +995,7 @@ void validate_settings(const tf_settings& s) {
 namespace tfb {
 // Message for tf_last_error(NULL) from entry points that take no handle.
 void record_unhandled_error(const std::string& message) { g_last_create_error = message; }
+const char* unhandled_error() { return g_last_create_error.c_str(); }
 }  // namespace tfb
 
 extern "C" int tf_default_settings(tf_settings* s) {

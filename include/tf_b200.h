@@ -230,6 +230,7 @@ TF_API int tf_oc_update(tf_filter* f, const double* design_dev, const double* ob
                         double move_limit, double beta, double eta, int32_t robust, double* candidate_dev, tf_oc_report* report,
                         void* stream);
 TF_API int tf_filter_destroy(tf_filter* f);
+/* NULL: the message of this thread's last failed call without a handle (as tf_last_error(NULL)). */
 TF_API const char* tf_filter_last_error(const tf_filter* f);
 
 /* ------------------------------------------------------------------------------------
@@ -287,6 +288,7 @@ TF_API int tf_mma_step(tf_mma* h, int32_t iteration, const double* xval, const d
                        const tf_mma_settings* settings, double* xnew, double* y_out, double* z_out, double* lam_out,
                        int32_t* newton_iterations, void* stream);
 TF_API int tf_mma_destroy(tf_mma* h);
+/* NULL: the message of this thread's last failed call without a handle (as tf_last_error(NULL)). */
 TF_API const char* tf_mma_last_error(const tf_mma* h);
 
 /* ------------------------------------------------------------------------------------
@@ -301,6 +303,7 @@ TF_API int tf_chol_factor_csr(tf_chol* h, const int32_t* indptr_dev, const int32
                               void* stream);
 TF_API int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, double* x_dev, void* stream);
 TF_API int tf_chol_destroy(tf_chol* h);
+/* NULL: the message of this thread's last failed call without a handle (as tf_last_error(NULL)). */
 TF_API const char* tf_chol_last_error(const tf_chol* h);
 
 /* CUDA-event timing of the kernel classes this handle launches, recorded on the launching

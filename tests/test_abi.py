@@ -52,3 +52,43 @@ def test_host_only_entry_points(library):
     assert lib.tf_create(None, None, None, None, ctypes.byref(handle)) == 1
     assert b"must not be NULL" in lib.tf_last_error(None)
     assert lib.tf_destroy(None) == 0
+
+
+def test_handleless_failures_carry_a_message(library):
+    """Entry points without a handle (and the create calls, whose handle stays NULL on failure)
+    return TF_STATUS_INVALID with a message that every *_last_error(NULL) getter returns."""
+    import numpy as np
+    from deep_frame_b200 import _lib
+    lib = _lib.load()
+    P = ctypes.c_void_p
+    out = P()
+    assert lib.tf_mma_create(0, 10, ctypes.byref(out)) == 1 and out.value is None
+    assert b"constraints" in lib.tf_mma_last_error(None) and lib.tf_last_error(None) == lib.tf_mma_last_error(None)
+    assert lib.tf_chol_create(0, ctypes.byref(out)) == 1 and b"unknowns" in lib.tf_chol_last_error(None)
+    shape, spacing = (ctypes.c_int64 * 3)(4, 4, 4), (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    allowed = np.ones(64, np.uint8)
+    assert lib.tf_filter_create(shape, spacing, -1.0, allowed.ctypes.data_as(P), None, ctypes.byref(out)) == 1
+    assert b"radius" in lib.tf_filter_last_error(None)
+    assert lib.tf_gram(None, -1, None, 2, 10, None, None, None) == 1 and lib.tf_last_error(None).startswith(b"tf_gram:")
+    assert lib.tf_simp(None, 10, 3.0, 1e-9, 1.0, None, None, None, None, None) == 1
+    assert lib.tf_last_error(None).startswith(b"tf_simp:")
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the path of a host without a CUDA device")
+def test_create_without_a_device_reports_a_cuda_error(library):
+    """On a host without a usable GPU the create calls fail with TF_STATUS_CUDA, a message and a
+    NULL handle: no crash and no CPU fallback."""
+    import numpy as np
+    from deep_frame_b200 import _lib
+    from deep_frame_b200.elements import hexahedron_matrices
+    lib = _lib.load()
+    grid = _lib.TfGrid()
+    for d in range(3):
+        grid.shape[d], grid.spacing[d] = 4, 1.0
+    ke = np.ascontiguousarray(hexahedron_matrices((1.0, 1.0, 1.0), 0.3)[0])
+    settings = _lib.default_settings()
+    handle = ctypes.c_void_p()
+    assert lib.tf_create(ctypes.byref(grid), ke.ctypes.data_as(ctypes.c_void_p), None, ctypes.byref(settings), ctypes.byref(handle)) == 2
+    assert handle.value is None and lib.tf_last_error(None)
+    assert lib.tf_mma_create(1, 10, ctypes.byref(handle)) == 2 and handle.value is None and lib.tf_mma_last_error(None)
+    assert lib.tf_chol_create(10, ctypes.byref(handle)) == 2 and handle.value is None and lib.tf_chol_last_error(None)
