@@ -82,3 +82,42 @@ def test_clock_summary_reads_reasons():
     s = c.summary()
     assert s["sm_mhz"] == 1900.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 3
     assert s["reasons"] == ["sw_power_cap"]
+
+
+def test_gpu_arm_line_from_a_device_result(monkeypatch, capsys):
+    """main() assembles the contract line from what ours() measured (a canned device result here,
+    shaped like the plate's) plus the CPU leg: every required key, the roofline arithmetic and
+    the errors against the FP64 oracle fixture."""
+    import numpy as np
+    ref = np.load(ROOT / "tests" / "golden" / "plate_96x96x16.npz")
+    nodes, cols = 159953, 84
+    result = {"rank": 0, "world": 1, "ms": 93.6, "dominant": "fine_work", "nodes": nodes, "cols": cols, "columns": [42, 42],
+              "smoother": {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "tensor_cores": False},
+              "dominant_per_launch_ms": 0.2832, "clocks": {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 5},
+              "ndof": 479859, "levels": 4, "coarsest_dofs": 1521, "iterations_max": [18, 18], "tuning": None,
+              "launches_per_step": 2075.0, "breakdown": {"fine_work": {"ms": 20.4, "launches": 72}}, "converged": True,
+              "e2e": {"ms": 95.8, "h2d_bytes_per_step": 2359296, "d2h_bytes_per_step": 2359312},
+              "solve_api": {"ms": 267.2, "h2d_bytes_per_step": 1, "d2h_bytes_per_step": 1},
+              "tr": float(ref["tr"]) * (1 + 1e-10), "lambda_max": float(ref["lambda_max"]),
+              "grad_mean": ref["grad_mean"], "grad_worst": ref["grad_worst"] * (1 + 1e-9)}
+    monkeypatch.setattr(bench, "ours", lambda args: (result, SimpleNamespace(), None, None))
+    monkeypatch.setattr(bench, "cpu_samples", lambda system, density, **k: [(32.08, {"workers": 16, "text": "canned"})])
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "5", "--warmup", "3", "--schedule", "1,2"])
+    bench.main()
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+                "vs_baseline", "dtype", "data", "config", "clocks", "gpu_launches", "roofline", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["value"] == pytest.approx(0.0936) and line["n_gpus"] == 1 and line["gpu_launches"] == 10375
+    assert line["config"]["workload"] == "plate_96x96x16" and line["config"]["smoother_choice"] == "fixed by --schedule"
+    roof = line["roofline"]
+    # degree-1 schedule: every finest launch a residual apply, 9 words per node and column + the moduli
+    algorithmic = nodes * 42 * 36 + nodes * 4
+    assert roof["algorithmic_bytes_per_launch"] == algorithmic and roof["traffic"] == bench.FINE_TRAFFIC["resid"]
+    assert roof["achieved"] == pytest.approx(algorithmic / 0.2832e-3 / 1e9, abs=0.1) and roof["frac"] == pytest.approx(roof["achieved"] / roof["peak"], abs=1e-4)
+    assert roof["compute"]["flops_per_launch"] == int(1152 * nodes * 42)
+    assert line["cpu_baseline"] == {"value": 32.08, "unit": "s", "cores": 16, "kind": "port", "sample": "canned"}
+    assert line["e2e"]["value"] == pytest.approx(0.0958) and line["e2e"]["h2d_bytes_per_step"] == 2359296
+    errors = line["results"]["vs_fp64_oracle"]
+    assert errors["tr_rel"] == pytest.approx(1e-10, rel=1e-3) and errors["lambda_max_rel"] == 0.0
+    assert errors["grad_mean_rel"] == 0.0 and errors["grad_worst_rel"] == pytest.approx(1e-9, rel=1e-3)
