@@ -294,6 +294,24 @@ def ours(args):
         result["solve_api"] = {"ms": e0.elapsed_time(e1) / args.steps,
                                "h2d_bytes_per_step": int(moduli_host.nbytes + sum(f.nbytes for _, f in host_forces)),
                                "d2h_bytes_per_step": int(sum(f.nbytes for _, f in host_forces))}
+        # (3) the reference-facing measure call itself: InterfaceCovariance.measure_device with a host density,
+        # both sensitivity fields read back to the host
+        try:
+            def measure_api_step():
+                r = model.measure_device(host_density, 3.0, 1e-9)
+                return r[0]["gradient"].cpu().numpy(), r[1]["gradient"].cpu().numpy()
+
+            measure_api_step()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(args.steps):
+                grads = measure_api_step()
+            e1.record()
+            torch.cuda.synchronize()
+            result["measure_api"] = {"ms": e0.elapsed_time(e1) / args.steps, "h2d_bytes_per_step": int(moduli_host.nbytes),
+                                     "d2h_bytes_per_step": int(grads[0].nbytes + grads[1].nbytes + model.rank * model.rank * 8)}
+        except (RuntimeError, ValueError) as exc:
+            result["measure_api"] = {"error": f"{type(exc).__name__}: {exc}"}
     if world > 1:
         dist.destroy_process_group()
     return result, system, model, density
@@ -627,6 +645,12 @@ def main():
         a = result["solve_api"]
         line["e2e_solve_api"] = {"value": round(a["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": a["h2d_bytes_per_step"],
                                  "d2h_bytes_per_step": a["d2h_bytes_per_step"], "call": "GeometricMultigrid.update + .solve per half with host NumPy forces and solutions"}
+        m = result.get("measure_api")
+        if m is not None:
+            line["e2e_measure_api"] = ({"error": m["error"]} if "error" in m else
+                                       {"value": round(m["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": m["h2d_bytes_per_step"],
+                                        "d2h_bytes_per_step": m["d2h_bytes_per_step"],
+                                        "call": "InterfaceCovariance.measure_device(host density), both sensitivity fields to the host"})
     line["results"] = {"tr_K_inv_sigma": result["tr"], "lambda_max": result["lambda_max"]}
     parity = oracle_errors(args.config, result)
     if parity:

@@ -98,6 +98,7 @@ def test_gpu_arm_line_from_a_device_result(monkeypatch, capsys):
               "launches_per_step": 2075.0, "breakdown": {"fine_work": {"ms": 20.4, "launches": 72}}, "converged": True,
               "e2e": {"ms": 95.8, "h2d_bytes_per_step": 2359296, "d2h_bytes_per_step": 2359312},
               "solve_api": {"ms": 267.2, "h2d_bytes_per_step": 1, "d2h_bytes_per_step": 1},
+              "measure_api": {"ms": 97.0, "h2d_bytes_per_step": 1179648, "d2h_bytes_per_step": 2373480},
               "tr": float(ref["tr"]) * (1 + 1e-10), "lambda_max": float(ref["lambda_max"]),
               "grad_mean": ref["grad_mean"], "grad_worst": ref["grad_worst"] * (1 + 1e-9)}
     monkeypatch.setattr(bench, "ours", lambda args: (result, SimpleNamespace(), None, None))
@@ -118,6 +119,7 @@ def test_gpu_arm_line_from_a_device_result(monkeypatch, capsys):
     assert roof["compute"]["flops_per_launch"] == int(1152 * nodes * 42)
     assert line["cpu_baseline"] == {"value": 32.08, "unit": "s", "cores": 16, "kind": "port", "sample": "canned"}
     assert line["e2e"]["value"] == pytest.approx(0.0958) and line["e2e"]["h2d_bytes_per_step"] == 2359296
+    assert line["e2e_measure_api"]["value"] == pytest.approx(0.097) and line["e2e_measure_api"]["call"].startswith("InterfaceCovariance")
     errors = line["results"]["vs_fp64_oracle"]
     assert errors["tr_rel"] == pytest.approx(1e-10, rel=1e-3) and errors["lambda_max_rel"] == 0.0
     assert errors["grad_mean_rel"] == 0.0 and errors["grad_worst_rel"] == pytest.approx(1e-9, rel=1e-3)
