@@ -10,6 +10,7 @@ direct solves, CPU torch for the reference's matrix-free operator and its
 density filter, and the reference's InterfaceCovariance for tr / lambda_max.
 Nothing under tests/ reads the reference at test time; only these .npz files.
 """
+import json
 import shutil
 import sys
 import tempfile
@@ -159,6 +160,17 @@ def covariance(topt, tprob):
            "ks": rows["load_worst"]["info"]["ks_n_mm"], "grad_mean": rows["load_mean"]["gradient"],
            "grad_worst": rows["load_worst"]["gradient"], "ke": system.ke, "penalization": 3.0, "min_stiffness_ratio": 1e-6,
            "young": system.young, **forces, **parts}
+    # the inputs themselves, so the product's own set-up (wrench forces, mirror parts, fixed sets) can be
+    # rebuilt from them and compared with the reference's
+    keep = ("grid", "symmetry", "material", "load_cases", "interfaces", "point_masses")
+    out["domain_json"] = json.dumps({k: domain[k] for k in keep})
+    for name in ("allowed", "preserve", "forbidden"):
+        out[f"domain_{name}"] = np.asarray(domain[name])
+    settings = problem["covariance"]
+    out["covariance_json"] = json.dumps({"support": settings["support"], "sigma": np.asarray(settings["sigma"]).tolist(),
+                                         "labels": settings["labels"], "prefix": settings["prefix"], "ks": settings["ks"],
+                                         "ks_cutoff": settings["ks_cutoff"],
+                                         "limits": {k: settings["limits"][k] for k in ("mean_n_mm", "worst_n_mm")}})
     np.savez_compressed(OUT / "covariance.npz", **out)
     tp.close()
 

@@ -141,3 +141,31 @@ def test_benchmark_plate_fixture_is_converged():
     assert float(g["tr"]) > float(g["lambda_max"]) > 0 and float(g["ks"]) >= float(g["lambda_max"])
     for key in ("grad_mean", "grad_worst"):
         assert g[key].shape == (96 * 96 * 16,) and np.all(np.isfinite(g[key])) and np.all(g[key] <= 0)
+
+
+def test_product_covariance_setup_matches_reference():
+    """The product's host set-up of the covariance model, rebuilt from the reference's own domain and
+    settings (stored in the fixture): the same unit-wrench load directions split into the same
+    mirror parts with the same fixed dofs (topology_problem.py:584-638 of the reference)."""
+    import json
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    g = golden("covariance")
+    domain = json.loads(str(g["domain_json"]))
+    for name in ("allowed", "preserve", "forbidden"):
+        domain[name] = g[f"domain_{name}"]
+    settings = json.loads(str(g["covariance_json"]))
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, settings, domain["interfaces"])
+    assert model.rank == int(g["rank"]) and model.factor == float(g["factor"])
+    assert np.allclose(model.directions, g["directions"], rtol=0, atol=1e-12 * np.abs(g["directions"]).max())
+    scale = max(np.abs(g[key]).max() for key in g.files if key.startswith("force_"))
+    for k, parts in enumerate(model.forces):
+        for sign, force in parts.items():
+            key = f"force_{k}_{'p' if sign > 0 else 'm'}"
+            assert key in g.files, key
+            assert np.allclose(force, g[key], rtol=0, atol=1e-12 * scale), key
+    assert sum(len(p) for p in model.forces) == sum(key.startswith("force_") for key in g.files)
+    fixed = {members[0][1]["sign"]: members[0][1]["fixed"] for members in system.groups.values()}
+    for sign, label in ((1, "p"), (-1, "m")):
+        assert np.array_equal(np.sort(fixed[sign]), np.sort(g[f"fixed_{label}"]))
