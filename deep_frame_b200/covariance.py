@@ -70,22 +70,27 @@ class InterfaceCovariance:
         return [(dofs(direct), nodal[:len(direct), :, j].ravel(), dofs(mirror), (nodal[len(direct):, :, j] * flip).ravel()) for j in range(6)]
 
     # ------------------------------------------------------------- device --
+    def group_members(self):
+        """Per fixture group holding covariance directions: (key, direction indices k, their parts).
+
+        A group can also hold other static load cases of the domain (the reference registers the
+        directions on the support case's fixture, topology_problem.py:599-611); only the covariance
+        directions enter F, so only their parts are kept, in registration order."""
+        index = {name: k for k, name in enumerate(self.cases)}
+        out = []
+        for key, members in self.system.groups.items():
+            mine = [(index[case["name"]], part) for case, part in members if case["name"] in index]
+            if mine:
+                out.append((key, np.asarray([k for k, _ in mine]), [part for _, part in mine]))
+        return out
+
     def groups(self):
         """Per fixture group: (key, case indices k, device force block [m, ndof])."""
         if self._groups is None:
             mg = self.system._multigrid()
             torch = mg.torch
-            index = {name: k for k, name in enumerate(self.cases)}
-            groups = []
-            for key, members in self.system.groups.items():
-                ks = [index[case["name"]] for case, _ in members if case["name"] in index]
-                if not ks:
-                    continue
-                if len(ks) != len(members):
-                    raise ValueError("covariance cases share a fixture group with other load cases")
-                forces = torch.as_tensor(np.stack([part["force"] for _, part in members]), dtype=torch.float64, device=mg.device)
-                groups.append((key, np.asarray(ks), forces))
-            self._groups = groups
+            self._groups = [(key, ks, torch.as_tensor(np.stack([part["force"] for part in parts]), dtype=torch.float64, device=mg.device))
+                            for key, ks, parts in self.group_members()]
         return self._groups
 
     def measure_device(self, physical_density, penalization=3.0, min_stiffness_ratio=1e-6, gradients=True):

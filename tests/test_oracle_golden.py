@@ -169,3 +169,27 @@ def test_product_covariance_setup_matches_reference():
     fixed = {members[0][1]["sign"]: members[0][1]["fixed"] for members in system.groups.values()}
     for sign, label in ((1, "p"), (-1, "m")):
         assert np.array_equal(np.sort(fixed[sign]), np.sort(g[f"fixed_{label}"]))
+
+
+def test_covariance_groups_skip_other_load_cases_of_the_fixture():
+    """In the reference's covariance cantilever the static "tip" case shares the support fixture
+    with the covariance directions; the device force blocks take the directions' parts only."""
+    import json
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    g = golden("covariance")
+    domain = json.loads(str(g["domain_json"]))
+    for name in ("allowed", "preserve", "forbidden"):
+        domain[name] = g[f"domain_{name}"]
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, json.loads(str(g["covariance_json"])), domain["interfaces"])
+    assert any(case["name"] == "tip" for members in system.groups.values() for case, _ in members)
+    chosen = model.group_members()
+    seen = set()
+    for key, ks, parts in chosen:
+        assert len(ks) == len(parts) >= 1
+        for k, part in zip(ks, parts):
+            expected = g[f"force_{k}_{'p' if part['sign'] > 0 else 'm'}"]
+            assert np.allclose(part["force"], expected, rtol=0, atol=1e-12 * np.abs(expected).max())
+            seen.add((int(k), part["sign"]))
+    assert len(seen) == sum(key.startswith("force_") for key in g.files)
