@@ -294,13 +294,51 @@ def inertia_relief(topt):
     np.savez_compressed(OUT / "inertia_relief.npz", **out)
 
 
+def setup_checksums(forces, fixed, ndof):
+    """Compact fingerprints of a covariance set-up: per (direction, sign) force the 2-norm, the sum and
+    the dot product with a seeded random vector; per sign the sorted fixed dofs' count, sum and
+    weighted sum.  Shared by the fixture writer and the test that rebuilds the set-up."""
+    probe = np.random.default_rng(7).standard_normal(ndof)
+    out = {}
+    for k, parts in enumerate(forces):
+        for sign, f in parts.items():
+            tag = f"{k}_{'p' if sign > 0 else 'm'}"
+            out[f"force_{tag}"] = np.array([np.linalg.norm(f), f.sum(), f @ probe])
+    for sign, dofs in fixed.items():
+        d = np.sort(np.asarray(dofs, dtype=np.int64))
+        out[f"fixed_{'p' if sign > 0 else 'm'}"] = np.array([len(d), d.sum(), (d.astype(float) * probe[d]).sum()])
+    return out
+
+
+def plate_setup(topt, tprob):
+    """The reference's host set-up of the benchmark plate (96 x 96 x 16, seed 0): its InterfaceCovariance
+    directions and every direction's mirror parts, fingerprinted (the full 84 force vectors would be
+    320 MB)."""
+    sys.path.insert(0, str(OUT.parents[1]))
+    from deep_frame_b200 import problems
+    domain, _, cov = problems.plate((96, 96, 16), 0)
+    # the reference's HexElasticity wants a static case at construction; one on the same stack fixture
+    # (loaded on the battery deck) joins the covariance directions' fixture group without changing them
+    stack = domain["load_cases"][0]["fixed_regions"]
+    battery = domain["interfaces"]["battery"]["regions"][0]
+    domain = dict(domain, load_cases=domain["load_cases"] + [{"name": "probe", "analysis": "static", "fixed_regions": stack,
+                                                              "loads": [{"region": battery, "force_n": [0.0, 0.0, -1.0]}]}])
+    system = topt.HexElasticity(domain)
+    settings = {"support": cov["support"], "sigma": cov["sigma"], "labels": cov["labels"], "prefix": "sigma_"}
+    model = tprob.InterfaceCovariance(system, settings, domain["interfaces"])
+    fixed = {members[0][1]["sign"]: members[0][1]["fixed"] for members in system.groups.values()}
+    out = setup_checksums(model.forces, fixed, system.ndof)
+    out.update(rank=model.rank, factor=model.factor, directions=model.directions, ndof=system.ndof)
+    np.savez_compressed(OUT / "plate_setup.npz", **out)
+
+
 def main(source):
     """Regenerate every fixture; ``--only NAME[,NAME]`` limits it to the named generators."""
     topt, tmg, tprob = load_reference(source)
     steps = {"hex8": lambda: hex8(topt), "operator": lambda: operator(topt, tmg, tprob),
              "cantilever_small": lambda: direct(topt, (16, 8, 8), 0, "cantilever_small"), "filter": lambda: density_filter(topt),
              "covariance": lambda: covariance(topt, tprob), "oc": lambda: optimality_criteria(topt),
-             "inertia_relief": lambda: inertia_relief(topt),
+             "inertia_relief": lambda: inertia_relief(topt), "plate_setup": lambda: plate_setup(topt, tprob),
              "cantilever_48x24x24": lambda: direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")}
     only = next((arg.split("=", 1)[1] for arg in sys.argv if arg.startswith("--only=")), None)
     for name, step in steps.items():

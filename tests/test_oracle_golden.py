@@ -193,3 +193,27 @@ def test_covariance_groups_skip_other_load_cases_of_the_fixture():
             assert np.allclose(part["force"], expected, rtol=0, atol=1e-12 * np.abs(expected).max())
             seen.add((int(k), part["sign"]))
     assert len(seen) == sum(key.startswith("force_") for key in g.files)
+
+
+def test_benchmark_plate_setup_matches_reference():
+    """The benchmark plate's 42 load directions and their mirror parts as the product sets them up
+    equal the reference's own InterfaceCovariance on the same seeded domain (tests/golden/plate_setup.npz,
+    fingerprints per direction and sign: 2-norm, sum, dot with a seeded random vector; fixed sets)."""
+    import importlib.util
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    make_golden = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(make_golden)
+    g = golden("plate_setup")
+    domain, _, cov = problems.plate((96, 96, 16), 0)
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, cov, domain["interfaces"])
+    assert system.ndof == int(g["ndof"]) and model.rank == int(g["rank"]) and model.factor == float(g["factor"])
+    assert np.allclose(model.directions, g["directions"], rtol=0, atol=1e-12 * np.abs(g["directions"]).max())
+    fixed = {members[0][1]["sign"]: members[0][1]["fixed"] for members in system.groups.values()}
+    mine = make_golden.setup_checksums(model.forces, fixed, system.ndof)
+    assert set(mine) == {key for key in g.files if key.startswith(("force_", "fixed_"))}
+    for key, value in mine.items():
+        assert np.allclose(value, g[key], rtol=1e-12, atol=1e-12 * max(1.0, np.abs(g[key]).max())), key
