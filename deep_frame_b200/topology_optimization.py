@@ -208,6 +208,10 @@ def optimize_topology(domain, settings, *, progress_callback=None, device="cuda"
         import torch
         settings = _settings(settings)
         validate_masks(domain)
+        # the reference's HexElasticity refuses a domain without a static case (topology_optimization.py:440-441);
+        # this library's HexElasticity accepts one (a covariance-only plate), so the OC driver checks it here
+        if not any(case.get("analysis") == "static" for case in domain.get("load_cases", [])):
+            raise ValueError("Topology optimization requires at least one static case")
         mapping = DensityMap(domain, settings, device)
         grid_shape = tuple(domain["grid"]["shape"])
         target = settings["volume_fraction"] * int(np.count_nonzero(mapping.allowed))

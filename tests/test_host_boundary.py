@@ -68,3 +68,14 @@ def test_missing_library_raises_instead_of_falling_back(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIBRARY", tmp_path / "libtfb200.so")
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.load()
+
+
+def test_oc_driver_needs_a_static_case():
+    """A domain with only a modal case is invalid for the OC driver, as in the reference
+    (topology_optimization.py:440-441), and is reported before any device work."""
+    from deep_frame_b200.topology_optimization import optimize_topology
+    domain = beam_domain()
+    domain["load_cases"] = [{"name": "modes", "analysis": "modal", "fixed_regions": domain["load_cases"][0]["fixed_regions"]}]
+    result = optimize_topology(domain, {"volume_fraction": 0.65, "filter_radius_mm": 3.1})
+    assert result["status"] == "invalid" and result["diagnostics"] == ["Topology optimization requires at least one static case"]
+    assert result["history"] == []
