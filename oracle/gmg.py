@@ -22,6 +22,7 @@ import numpy as np
 from scipy.sparse import coo_matrix, csr_matrix, diags, kron, identity
 from scipy.sparse.linalg import splu
 
+from .hex8 import CORNERS, grid_numbering
 from .operator import assemble, live_dofs
 
 DEFAULTS = {"coarsest_dofs": 8000, "max_levels": 8, "smoother": "chebyshev", "sweeps": 2, "damping": 1.0,
@@ -52,6 +53,43 @@ def prolongation(coarse_shape):
     """Dof prolongation for node-major, component-minor vectors of a grid of coarse_shape elements."""
     px, py, pz = (prolongation_1d(n) for n in coarse_shape)
     return kron(kron(kron(px, py), pz), identity(3)).tocsr()
+
+
+def local_interpolation():
+    """[8 children, 24 fine dofs, 24 coarse dofs]: the trilinear weight of every coarse-element corner
+    at every corner of each of its 8 children (children in C order of their offsets), per component
+    (the reference's ``_interpolation``, topology_multigrid.py:19-27)."""
+    offsets = np.array(list(np.ndindex(2, 2, 2)), dtype=float)
+    at = (offsets[:, None, :] + CORNERS[None, :, :]) / 2.0                        # [child, fine corner, xyz]
+    weight = np.prod(np.where(CORNERS[None, None, :, :] == 1, at[:, :, None, :], 1.0 - at[:, :, None, :]), axis=3)
+    return np.einsum("cfk,ij->cfikj", weight, np.eye(3)).reshape(8, 24, 24)
+
+
+def fine_blocks(shape, k0, moduli, mask):
+    """[nelem, 24, 24] element matrices E_e K0 gated on both sides by the fine live mask (the children
+    of the first Galerkin level, topology_multigrid.py:131-135)."""
+    _, dofs = grid_numbering(shape)
+    m = np.asarray(mask, dtype=float)[dofs]                                       # [nelem, 24]
+    return np.asarray(moduli, dtype=float).ravel()[:, None, None] * m[:, :, None] * m[:, None, :] * np.asarray(k0)[None]
+
+
+def galerkin_blocks(shape, children):
+    """Coarse element blocks sum_c P_c^T B_c P_c over the 8 children of every coarse element,
+    symmetrised (topology_multigrid.py:173-178); ``shape`` is the children's grid, even in every axis."""
+    cx, cy, cz = (n // 2 for n in shape)
+    index = np.arange(int(np.prod(shape))).reshape(cx, 2, cy, 2, cz, 2).transpose(0, 2, 4, 1, 3, 5).reshape(-1, 8)
+    local = local_interpolation()
+    blocks = np.einsum("cia,ecij,cjb->eab", local, children[index], local, optimize=True)
+    return (blocks + blocks.transpose(0, 2, 1)) / 2
+
+
+def assemble_blocks(shape, blocks):
+    """Sparse matrix of per-element [24, 24] blocks on a grid of ``shape`` elements."""
+    _, dofs = grid_numbering(shape)
+    ndof = 3 * int(np.prod(np.asarray(shape) + 1))
+    rows = np.repeat(dofs, 24, axis=1).ravel()
+    cols = np.tile(dofs, (1, 24)).ravel()
+    return coo_matrix((blocks.reshape(-1), (rows, cols)), shape=(ndof, ndof)).tocsr()
 
 
 class MultigridOracle:

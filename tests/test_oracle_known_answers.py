@@ -124,3 +124,26 @@ def test_covariance_trace_and_ks_gradients_match_finite_differences():
     assert at["grad_mean"] @ direction == pytest.approx((plus["load_mean"] - minus["load_mean"]) / (2 * step), rel=1e-5)
     assert at["grad_worst"] @ direction == pytest.approx((plus["ks"] - minus["ks"]) / (2 * step), rel=1e-5)
     assert at["ks"] >= at["load_worst"]
+
+
+def test_galerkin_element_blocks_equal_the_sparse_triple_product():
+    """The reference builds each Galerkin level from element blocks, sum over the 8 children of
+    P_c^T B_c P_c (topology_multigrid.py:145-208); the oracle uses P^T A P with the sparse
+    prolongation.  They are the same operator, on the first level (children masked on both sides
+    by the fine live mask) and on the next (children unmasked): the reference's
+    tests/test_topology_multigrid.py:41-53 checks the same identity."""
+    from oracle.gmg import MultigridOracle, assemble_blocks, fine_blocks, galerkin_blocks
+    shape = (8, 8, 8)
+    rng = np.random.default_rng(11)
+    moduli = rng.uniform(0.05, 1.0, int(np.prod(shape)))
+    moduli[rng.uniform(size=moduli.size) < 0.1] = 0.0                             # some void cells
+    nodes = np.indices(tuple(n + 1 for n in shape)).reshape(3, -1)
+    fixed = (3 * np.flatnonzero(nodes[0] == 0)[:, None] + np.arange(3)).ravel()
+    k0 = hex8.element_matrices((1.0, 1.0, 1.0), 0.3)[0]
+    mg = MultigridOracle(shape, k0, moduli, fixed, {"coarsest_dofs": 100})
+    assert mg.levels == 3 and mg.padded == shape
+    level1 = galerkin_blocks(shape, fine_blocks(shape, k0, moduli, mg.mask[0]))
+    level2 = galerkin_blocks((4, 4, 4), level1)
+    for level, (grid, blocks) in enumerate((((4, 4, 4), level1), ((2, 2, 2), level2)), start=1):
+        difference = assemble_blocks(grid, blocks) - mg.A[level]
+        assert abs(difference).max() < 1e-12 * abs(mg.A[level]).max(), level
