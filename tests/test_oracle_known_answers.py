@@ -147,3 +147,47 @@ def test_galerkin_element_blocks_equal_the_sparse_triple_product():
     for level, (grid, blocks) in enumerate((((4, 4, 4), level1), ((2, 2, 2), level2)), start=1):
         difference = assemble_blocks(grid, blocks) - mg.A[level]
         assert abs(difference).max() < 1e-12 * abs(mg.A[level]).max(), level
+
+
+def test_half_plate_equals_the_full_plate():
+    """The mirror-symmetric half model (x >= 0, symmetric and antisymmetric fixture groups, factor 2)
+    gives the tr(K^-1 Sigma) and lambda_max of the full plate with mirrored densities, both set up by
+    the product's host code and solved directly; the reference checks the same on its cantilever
+    (tests/test_topology_problem.py:479-508, relative 1e-8)."""
+    import copy
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    shape = (16, 12, 4)
+    half, density, cov = problems.plate(shape, 2)
+    full = copy.deepcopy(half)
+    full.pop("symmetry")
+    full["grid"]["shape"] = [2 * shape[0], shape[1], shape[2]]
+    full["grid"]["origin_mm"] = [-float(shape[0]), 0.0, 0.0]
+    for name in ("allowed", "preserve", "forbidden"):
+        full[name] = np.concatenate([half[name][::-1], half[name]], axis=0)
+    density_full = np.concatenate([density.reshape(shape)[::-1], density.reshape(shape)], axis=0).ravel()
+
+    def measure(domain, rho):
+        grid = tuple(domain["grid"]["shape"])
+        system = HexElasticity(domain)
+        model = InterfaceCovariance(system, cov, domain["interfaces"])
+        moduli, slope = system.moduli(rho, 3.0, 1e-9)
+        k = op.assemble(grid, system.ke, moduli).tocsc()
+        index = {name: j for j, name in enumerate(model.cases)}
+        parts = []
+        for members in system.groups.values():
+            forces = np.zeros((system.ndof, model.rank))
+            for case, part in members:
+                forces[:, index[case["name"]]] = part["force"]
+            live = op.live_dofs(grid, moduli, members[0][1]["fixed"])
+            u = np.zeros_like(forces)
+            u[live] = splu(k[live][:, live].tocsc()).solve(forces[live])
+            parts.append((forces, u))
+        return model, ocov.measure(parts, model.factor, grid, system.ke, slope)
+
+    half_model, half_values = measure(half, density)
+    full_model, full_values = measure(full, density_full)
+    assert half_model.factor == 2.0 and full_model.factor == 1.0 and len(half_model.system.groups) == 2
+    assert half_values["load_mean"] == pytest.approx(full_values["load_mean"], rel=1e-8)
+    assert half_values["load_worst"] == pytest.approx(full_values["load_worst"], rel=1e-8)
