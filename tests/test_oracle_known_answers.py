@@ -191,3 +191,29 @@ def test_half_plate_equals_the_full_plate():
     assert half_model.factor == 2.0 and full_model.factor == 1.0 and len(half_model.system.groups) == 2
     assert half_values["load_mean"] == pytest.approx(full_values["load_mean"], rel=1e-8)
     assert half_values["load_worst"] == pytest.approx(full_values["load_worst"], rel=1e-8)
+
+
+def test_rank_one_covariance_has_trace_equal_to_lambda_max():
+    """With a rank-one Sigma = s s^T there is one load direction, so F is 1 x 1 and
+    tr(K^-1 Sigma) = lambda_max (reference tests/test_topology_problem.py:510-516)."""
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    shape = (16, 12, 4)
+    domain, density, cov = problems.plate(shape, 1)
+    s = np.random.default_rng(4).standard_normal(42)
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, dict(cov, sigma=np.outer(s, s)), domain["interfaces"])
+    assert model.rank == 1 and np.allclose(model.directions @ model.directions.T, np.outer(s, s))
+    moduli, slope = system.moduli(density, 3.0, 1e-9)
+    k = op.assemble(shape, system.ke, moduli).tocsc()
+    parts = []
+    for members in system.groups.values():
+        forces = np.column_stack([part["force"] for _, part in members])
+        live = op.live_dofs(shape, moduli, members[0][1]["fixed"])
+        u = np.zeros_like(forces)
+        u[live] = splu(k[live][:, live].tocsc()).solve(forces[live])
+        parts.append((forces, u))
+    values = ocov.measure(parts, model.factor, shape, system.ke, slope)
+    assert values["load_mean"] == pytest.approx(values["load_worst"], rel=1e-12)
+    assert np.allclose(values["grad_mean"], values["grad_worst"], rtol=1e-10, atol=1e-14 * np.abs(values["grad_mean"]).max())
