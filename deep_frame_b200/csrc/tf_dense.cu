@@ -545,9 +545,13 @@ extern "C" int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, doub
 }
 
 extern "C" int tf_chol_destroy(tf_chol* h) {
-  if (h) {
-    cudaDeviceSynchronize();
-    delete h;
+  if (!h) return tfb::TF_OK;
+  // an error the device reports here (from earlier work) is returned, and the handle is freed regardless
+  const cudaError_t e = cudaDeviceSynchronize();
+  delete h;
+  if (e != cudaSuccess) {
+    tfb::record_unhandled_error(std::string("tf_chol_destroy: ") + cudaGetErrorString(e));
+    return tfb::TF_CUDA;
   }
   return tfb::TF_OK;
 }

@@ -1533,8 +1533,13 @@ extern "C" int tf_timers(tf_handle* h, int32_t enable, double* ms, int64_t* coun
 
 extern "C" int tf_destroy(tf_handle* h) {
   if (!h) return TF_OK;
-  cudaDeviceSynchronize();
+  // an error the device reports here (from earlier work) is returned, and the handle is freed regardless
+  const cudaError_t e = cudaDeviceSynchronize();
   delete h;
+  if (e != cudaSuccess) {
+    g_last_create_error = std::string("tf_destroy: ") + cudaGetErrorString(e);
+    return TF_CUDA;
+  }
   return TF_OK;
 }
 

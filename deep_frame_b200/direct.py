@@ -116,7 +116,10 @@ class CudaDirectSolver:
         except Exception as error:
             self.cleanup_errors.append("CUDA cleanup synchronization: " + str(error))
         try:
-            self.lib.tf_chol_destroy(self.handle)
+            status = self.lib.tf_chol_destroy(self.handle)
+            if status:
+                message = (self.lib.tf_chol_last_error(None) or b"").decode(errors="replace")
+                self.cleanup_errors.append(f"tf_chol_destroy failed ({_lib.STATUS.get(status, status)}): {message}")
         except Exception as error:
             self.cleanup_errors.append(str(error))
         self.handle = None

@@ -473,7 +473,10 @@ class GeometricMultigrid:
         errors = []
         if getattr(self, "handle", None):
             try:
-                self.lib.tf_destroy(self.handle)
+                status = self.lib.tf_destroy(self.handle)
+                if status:
+                    message = (self.lib.tf_last_error(None) or b"").decode(errors="replace")
+                    errors.append(f"tf_destroy failed ({_lib.STATUS.get(status, status)}): {message}")
             except Exception as error:  # pragma: no cover - defensive
                 errors.append(str(error))
             self.handle = None

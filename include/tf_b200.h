@@ -302,6 +302,8 @@ TF_API int tf_chol_create(int64_t n, tf_chol** out);
 TF_API int tf_chol_factor_csr(tf_chol* h, const int32_t* indptr_dev, const int32_t* indices_dev, const double* data_dev,
                               void* stream);
 TF_API int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, double* x_dev, void* stream);
+/* Frees the handle in every case; a device error seen while waiting for it returns TF_STATUS_CUDA with
+ * the message in tf_chol_last_error(NULL) (CudaDirectSolver.close, topology_optimization.py:205-239). */
 TF_API int tf_chol_destroy(tf_chol* h);
 /* NULL: the message of this thread's last failed call without a handle (as tf_last_error(NULL)). */
 TF_API const char* tf_chol_last_error(const tf_chol* h);
@@ -319,7 +321,9 @@ TF_API int tf_timers(tf_handle* h, int32_t enable, double* ms, int64_t* counts, 
 TF_API int64_t tf_launch_count(void);
 
 /* Release the handle and every device buffer it owns (GeometricMultigrid.close,
- * topology_multigrid.py:543-548).  Idempotent for NULL. */
+ * topology_multigrid.py:543-548).  Idempotent for NULL.  The handle is freed in every case; an
+ * error the device reports while the destroy waits for it returns TF_STATUS_CUDA with the message
+ * in tf_last_error(NULL), so close() can hand it back as the reference's close does. */
 TF_API int tf_destroy(tf_handle* h);
 
 /* Message of the last failed call on `h` (or, with h NULL, of the last failed tf_create,

@@ -79,3 +79,31 @@ def test_oc_driver_needs_a_static_case():
     result = optimize_topology(domain, {"volume_fraction": 0.65, "filter_radius_mm": 3.1})
     assert result["status"] == "invalid" and result["diagnostics"] == ["Topology optimization requires at least one static case"]
     assert result["history"] == []
+
+
+def test_close_hands_back_device_errors_instead_of_raising():
+    """GeometricMultigrid.close and CudaDirectSolver.close return the errors met while releasing
+    their handles (the reference's close returns its collected error strings,
+    topology_multigrid.py:543-548 and topology_optimization.py:205-239); a stand-in library whose
+    destroy reports a CUDA error plays the device here."""
+    from types import SimpleNamespace
+    from deep_frame_b200.direct import CudaDirectSolver
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    destroyed = []
+    lib = SimpleNamespace(tf_destroy=lambda h: destroyed.append(h) or 2, tf_last_error=lambda h: b"tf_destroy: an illegal memory access was encountered",
+                          tf_chol_destroy=lambda h: destroyed.append(h) or 2, tf_chol_last_error=lambda h: b"tf_chol_destroy: unspecified launch failure")
+    mg = object.__new__(GeometricMultigrid)
+    mg.lib, mg.handle = lib, "multigrid-handle"
+    assert mg.close() == ["tf_destroy failed (cuda): tf_destroy: an illegal memory access was encountered"]
+    assert mg.handle is None and mg.close() == [] and destroyed == ["multigrid-handle"]
+
+    def failing_sync(device):
+        raise RuntimeError("CUDA error: unspecified launch failure")
+
+    solver = object.__new__(CudaDirectSolver)
+    solver.lib, solver.handle, solver.closed, solver.cleanup_errors, solver.device = lib, "chol-handle", False, [], None
+    solver.torch = SimpleNamespace(cuda=SimpleNamespace(synchronize=failing_sync))
+    errors = solver.close()
+    assert errors == ["CUDA cleanup synchronization: CUDA error: unspecified launch failure",
+                      "tf_chol_destroy failed (cuda): tf_chol_destroy: unspecified launch failure"]
+    assert solver.closed and solver.handle is None and solver.close() == errors and destroyed[-1] == "chol-handle"
