@@ -107,3 +107,46 @@ def test_close_hands_back_device_errors_instead_of_raising():
     assert errors == ["CUDA cleanup synchronization: CUDA error: unspecified launch failure",
                       "tf_chol_destroy failed (cuda): tf_chol_destroy: unspecified launch failure"]
     assert solver.closed and solver.handle is None and solver.close() == errors and destroyed[-1] == "chol-handle"
+
+
+def test_cleanup_errors_follow_the_primary_error(monkeypatch):
+    """When an iteration fails and closing the solver fails too, the outcome is "failed" with the
+    original error first and the cleanup error after it (reference
+    tests/test_topology_optimization.py:418-427).  Stand-ins replace the device density map and
+    elasticity system."""
+    import torch
+    from deep_frame_b200 import topology_optimization as topo
+    closed = []
+
+    class Mapping:
+        def __init__(self, domain, settings, device):
+            shape = tuple(domain["grid"]["shape"])
+            self.allowed, self.preserve = np.ones(shape, bool), np.zeros(shape, bool)
+            self.n, self.device, self.beta, self.robust = int(np.prod(shape)), torch.device("cpu"), 1.0, False
+
+        def initial(self, target):
+            return np.full(self.n, target / self.n)
+
+        def _dev(self, values):
+            return torch.as_tensor(values)
+
+        def fields_device(self, design):
+            raise RuntimeError("CUDA solve unavailable in controlled test")
+
+        def close(self):
+            closed.append("mapping")
+
+    class System:
+        def __init__(self, domain, **kwargs):
+            pass
+
+        def close(self):
+            closed.append("system")
+            return ["cleanup failed in controlled test"]
+
+    monkeypatch.setattr(topo, "DensityMap", Mapping)
+    monkeypatch.setattr(topo, "HexElasticity", System)
+    result = topo.optimize_topology(beam_domain(), {"volume_fraction": 0.65, "filter_radius_mm": 3.1})
+    assert result["status"] == "failed" and result["history"] == []
+    assert result["diagnostics"] == ["CUDA solve unavailable in controlled test", "cleanup failed in controlled test"]
+    assert closed == ["system", "mapping"]
