@@ -27,7 +27,7 @@ from .operator import assemble, live_dofs
 
 DEFAULTS = {"coarsest_dofs": 8000, "max_levels": 8, "smoother": "chebyshev", "sweeps": 2, "damping": 1.0,
             "chebyshev_degree": 3, "chebyshev_ratio": 20.0, "growth": 2.0, "cycle": "V", "power_iterations": 20,
-            "tolerance": 1e-8, "max_iterations": 2000, "dead_ratio": 1e-12}
+            "tolerance": 1e-8, "max_iterations": 2000, "dead_ratio": 1e-12, "zero_rhs": 1e-12}
 
 
 def level_count(shape, settings):
@@ -199,9 +199,23 @@ class MultigridOracle:
         return self._cycle(0, r / scale) * scale
 
     def solve(self, forces, max_iterations=None):
-        """Flexible PCG per column; forces [ndof_unpadded, R] -> (u, iterations, relative, history)."""
+        """Flexible PCG per column; forces [ndof_unpadded, R] -> (u, iterations, relative, history).
+
+        Columns whose norm is at most zero_rhs times the largest are not solved: zero solution, 0
+        iterations, relative residual 0 (the reference's solve, topology_multigrid.py:350-351)."""
         forces = np.asarray(forces, dtype=float)
         forces = forces[:, None] if forces.ndim == 1 else forces
+        norms = np.linalg.norm(forces, axis=0)
+        live = np.flatnonzero(norms > self.s["zero_rhs"] * max(norms.max(initial=0.0), 1e-300))
+        u = np.zeros_like(forces)
+        iterations, relative = np.zeros(forces.shape[1], dtype=int), np.zeros(forces.shape[1])
+        history = []
+        if len(live):
+            u[:, live], iterations[live], relative[live], history = self._pcg(forces[:, live], max_iterations)
+        return u, iterations, relative, history
+
+    def _pcg(self, forces, max_iterations=None):
+        """Batched flexible PCG of the live columns (topology_multigrid.py:407-454)."""
         limit = self.s["max_iterations"] if max_iterations is None else max_iterations
         tol = self.s["tolerance"]
         n_p = self.A[0].shape[0]

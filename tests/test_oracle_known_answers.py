@@ -217,3 +217,24 @@ def test_rank_one_covariance_has_trace_equal_to_lambda_max():
     values = ocov.measure(parts, model.factor, shape, system.ke, slope)
     assert values["load_mean"] == pytest.approx(values["load_worst"], rel=1e-12)
     assert np.allclose(values["grad_mean"], values["grad_worst"], rtol=1e-10, atol=1e-14 * np.abs(values["grad_mean"]).max())
+
+
+def test_oracle_skips_zero_load_columns_like_the_reference():
+    """A zero right-hand side column is not solved (zero solution, 0 iterations, residual 0) and the
+    others converge as if alone (reference topology_multigrid.py:350-351 and its
+    tests/test_topology_multigrid.py:178-188)."""
+    from oracle.gmg import MultigridOracle
+    shape = (8, 4, 4)
+    k0 = hex8.element_matrices((1.0, 1.0, 1.0), 0.3)[0]
+    moduli = np.random.default_rng(2).uniform(0.2, 1.0, int(np.prod(shape)))
+    tip, free = clamped_beam(shape)
+    fixed = np.setdiff1d(np.arange(3 * int(np.prod(np.asarray(shape) + 1))), free)
+    force = np.zeros(3 * int(np.prod(np.asarray(shape) + 1)))
+    force[3 * tip + 2] = -1.0 / len(tip)
+    mg = MultigridOracle(shape, k0, moduli, fixed, {"tolerance": 1e-10, "coarsest_dofs": 100})
+    u, iterations, relative, _ = mg.solve(np.column_stack([force, np.zeros_like(force), 2 * force]))
+    alone = mg.solve(force)[0][:, 0]
+    assert iterations[1] == 0 and relative[1] == 0 and not u[:, 1].any()
+    assert iterations[0] > 0 and relative[0] < 1e-10 and relative[2] < 1e-10
+    assert np.allclose(u[:, 0], alone, rtol=0, atol=1e-9 * np.abs(alone).max())
+    assert np.allclose(u[:, 2], 2 * alone, rtol=0, atol=1e-9 * np.abs(alone).max())
