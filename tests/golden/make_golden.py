@@ -332,6 +332,43 @@ def plate_setup(topt, tprob):
     np.savez_compressed(OUT / "plate_setup.npz", **out)
 
 
+def diagnostic_domains():
+    """Two beams for the system summary: the OC test beam (fixture, tip and side loads, modes) and a
+    beam whose load selectors lose nodes to forbidden cells and to the preserve-adjacent interface
+    policy, plus a point selector between nodes that needs the half-voxel expansion."""
+    def beam(shape):
+        extent = np.array(shape, dtype=float)
+        fixture = box([-0.01, -0.01, -0.01], [0.01, extent[1] + 0.01, extent[2] + 0.01])
+        preserve = np.zeros(shape, dtype=bool)
+        preserve[0] = preserve[-1] = True
+        return extent, fixture, {"grid": {"shape": list(shape), "spacing_mm": [1.0, 1.0, 1.0], "origin_mm": [0.0, 0.0, 0.0],
+                                          "order": "C", "axis_order": "xyz"},
+                                 "allowed": np.ones(shape, dtype=bool), "preserve": preserve, "forbidden": np.zeros(shape, dtype=bool),
+                                 "material": {"young_modulus_mpa": 4430.0, "poisson_ratio": 0.3, "density_g_cm3": 1.09}, "point_masses": []}
+    extent, fixture, plain = beam((6, 4, 4))
+    tip = box([extent[0] - 0.01, -0.01, -0.01], (extent + 0.01).tolist())
+    plain["load_cases"] = [{"name": "tip", "analysis": "static", "fixed_regions": [fixture], "loads": [{"region": tip, "force_n": [0.0, 0.0, -1.0]}]},
+                           {"name": "side", "analysis": "static", "fixed_regions": [fixture], "loads": [{"region": tip, "force_n": [0.0, 0.6, 0.0]}]},
+                           {"name": "modes", "analysis": "modal", "fixed_regions": [fixture]}]
+    extent, fixture, filtered = beam((8, 4, 4))
+    filtered["allowed"][3:5, :, 3] = False
+    filtered["forbidden"] = ~filtered["allowed"]
+    top = box([3.99, -0.01, 3.99], [8.01, 4.01, 4.01])
+    point = box([7.49, 1.99, 3.99], [7.51, 2.01, 4.01])
+    filtered["load_cases"] = [{"name": "deck", "analysis": "static", "fixed_regions": [fixture], "loads": [{"region": top, "force_n": [0.0, 0.0, -1.0]}]},
+                              {"name": "point", "analysis": "static", "fixed_regions": [fixture], "loads": [{"region": point, "force_n": [0.0, 1.0, 0.0]}]}]
+    return {"plain": (plain, "allowed_adjacent"), "filtered": (filtered, "preserve_adjacent")}
+
+
+def system_diagnostics(topt):
+    """The reference's HexElasticity.diagnostics() on the diagnostic domains, as JSON."""
+    out = {}
+    for name, (domain, policy) in diagnostic_domains().items():
+        system = topt.HexElasticity(domain, interface_node_policy=policy)
+        out[name] = json.dumps(system.diagnostics())
+    np.savez_compressed(OUT / "diagnostics.npz", **out)
+
+
 def main(source):
     """Regenerate every fixture; ``--only NAME[,NAME]`` limits it to the named generators."""
     topt, tmg, tprob = load_reference(source)
@@ -339,6 +376,7 @@ def main(source):
              "cantilever_small": lambda: direct(topt, (16, 8, 8), 0, "cantilever_small"), "filter": lambda: density_filter(topt),
              "covariance": lambda: covariance(topt, tprob), "oc": lambda: optimality_criteria(topt),
              "inertia_relief": lambda: inertia_relief(topt), "plate_setup": lambda: plate_setup(topt, tprob),
+             "diagnostics": lambda: system_diagnostics(topt),
              "cantilever_48x24x24": lambda: direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")}
     only = next((arg.split("=", 1)[1] for arg in sys.argv if arg.startswith("--only=")), None)
     for name, step in steps.items():

@@ -217,3 +217,25 @@ def test_benchmark_plate_setup_matches_reference():
     assert set(mine) == {key for key in g.files if key.startswith(("force_", "fixed_"))}
     for key, value in mine.items():
         assert np.allclose(value, g[key], rtol=1e-12, atol=1e-12 * max(1.0, np.abs(g[key]).max())), key
+
+
+def test_system_diagnostics_match_reference():
+    """HexElasticity.diagnostics() on the reference's own diagnostic domains (tests/golden/diagnostics.npz,
+    built by make_golden.py) has the reference's keys and values, selector expansions and
+    interface-policy filtering included; only the solver records differ by design (the device
+    multigrid / Cholesky instead of SuperLU / cuDSS)."""
+    import importlib.util
+    import json
+    from deep_frame_b200.elasticity import HexElasticity
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    make_golden = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(make_golden)
+    g = golden("diagnostics")
+    solver_keys = {"linear_solver", "requested_linear_solver", "gpu_symbolic_reanalyses", "gpu_solver_residency",
+                   "gpu_transient_releases", "gpu_solver_details"}
+    for name, (domain, policy) in make_golden.diagnostic_domains().items():
+        expected = json.loads(str(g[name]))
+        got = json.loads(json.dumps(HexElasticity(domain, interface_node_policy=policy).diagnostics(), default=lambda v: v.tolist()))
+        assert set(got) == set(expected), (name, set(got) ^ set(expected))
+        for key in set(expected) - solver_keys:
+            assert got[key] == expected[key], (name, key)
