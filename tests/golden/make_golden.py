@@ -366,7 +366,22 @@ def system_diagnostics(topt):
     for name, (domain, policy) in diagnostic_domains().items():
         system = topt.HexElasticity(domain, interface_node_policy=policy)
         out[name] = json.dumps(system.diagnostics())
+    # and the inertia-relief domains of inertia_relief.npz (their cases carry a relief summary)
+    for name, domain in relief_domains().items():
+        out[name] = json.dumps(topt.HexElasticity(domain).diagnostics())
     np.savez_compressed(OUT / "diagnostics.npz", **out)
+
+
+def relief_domains():
+    """The domains stored in inertia_relief.npz, rebuilt from their JSON text."""
+    relief = np.load(OUT / "inertia_relief.npz")
+    out = {}
+    for name in ("tiny", "relief_full", "relief_half"):
+        domain = json.loads(str(relief[f"{name}_domain"]))
+        for key in ("allowed", "preserve", "forbidden"):
+            domain[key] = np.asarray(domain[key], dtype=bool)
+        out[name] = domain
+    return out
 
 
 def main(source):

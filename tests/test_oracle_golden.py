@@ -233,7 +233,9 @@ def test_system_diagnostics_match_reference():
     g = golden("diagnostics")
     solver_keys = {"linear_solver", "requested_linear_solver", "gpu_symbolic_reanalyses", "gpu_solver_residency",
                    "gpu_transient_releases", "gpu_solver_details"}
-    for name, (domain, policy) in make_golden.diagnostic_domains().items():
+    cases = dict(make_golden.diagnostic_domains(), **{name: (d, "allowed_adjacent") for name, d in make_golden.relief_domains().items()})
+    assert set(cases) == set(g.files)
+    for name, (domain, policy) in cases.items():
         expected = json.loads(str(g[name]))
         got = json.loads(json.dumps(HexElasticity(domain, interface_node_policy=policy).diagnostics(), default=lambda v: v.tolist()))
         assert set(got) == set(expected), (name, set(got) ^ set(expected))
