@@ -69,6 +69,75 @@ class InterfaceCovariance:
         dofs = lambda nodes: (3 * nodes[:, None] + np.arange(3)).ravel()
         return [(dofs(direct), nodal[:len(direct), :, j].ravel(), dofs(mirror), (nodal[len(direct):, :, j] * flip).ravel()) for j in range(6)]
 
+    def _worst_wrench(self, vector):
+        """The six interface wrench components of largest magnitude in Sigma^1/2's image of F's top
+        eigenvector: [["interface/dof", value], ...] (the reference's info row)."""
+        wrench = self.directions @ vector
+        return [["/".join(self.labels[i]), float(wrench[i])] for i in np.argsort(np.abs(wrench))[::-1][:6]]
+
+    def _limits(self):
+        """Constraint limits scaled by the calibration factor (one number, or a dict with a per-support
+        entry; without interface bodies the "rails" entry applies)."""
+        limits = self.settings["limits"]
+        calibration = limits.get("calibration", 1.0)
+        if isinstance(calibration, dict):
+            calibration = calibration.get("rails", calibration)
+        out = {}
+        for key in ("mean_n_mm", "worst_n_mm"):
+            scale = calibration[key] if isinstance(calibration, dict) else calibration
+            out[key] = limits.get(key) and limits[key] * scale
+        return out
+
+    # --------------------------------------------------------------- host --
+    def matrix(self, solutions):
+        """F = factor * sum over mirror signs of P_s^T U_s, symmetrised, from the host solutions that
+        HexElasticity.solve returns (``solutions[case]["fields"][sign]``), and the stacked U_s
+        (the reference's matrix, topology_problem.py:639-646)."""
+        zero = np.zeros(self.system.ndof)
+        signs = sorted({sign for name in self.cases for sign in solutions[name]["fields"]})
+        stacked = {sign: np.stack([solutions[name]["fields"].get(sign, zero) for name in self.cases], axis=1) for sign in signs}
+        loads = {sign: np.stack([parts.get(sign, zero) for parts in self.forces], axis=1) for sign in signs}
+        flexibility = self.factor * sum(loads[sign].T @ stacked[sign] for sign in signs)
+        return (flexibility + flexibility.T) / 2, stacked
+
+    def energy(self, stacked, vector, derivative):
+        """-factor * dE/drho * sum_s (U_s v)_e^T K0 (U_s v)_e per element: the sensitivity of v^T F v
+        (the reference's energy, topology_problem.py:647-652)."""
+        total = np.zeros(self.system.nelem)
+        for field in stacked.values():
+            ue = (field @ vector)[self.system.dofs]
+            total += np.einsum("ei,ij,ej->e", ue, self.system.ke, ue, optimize=True)
+        return -self.factor * np.asarray(derivative) * total
+
+    def measure(self, solutions):
+        """The load_mean / load_worst rows from host solutions (the reference's measure,
+        topology_problem.py:657-684, without interface bodies): tr F, lambda_max F, the KS aggregate
+        over F's eigenvalues and, where a limit is set, the constraint values and gradients."""
+        limits, s = self._limits(), self.settings["ks"]
+        flexibility, stacked = self.matrix(solutions)
+        mean = float(np.trace(flexibility))
+        values, vectors = np.linalg.eigh(flexibility)
+        values, vectors = values[::-1], vectors[:, ::-1]
+        worst = float(values[0])
+        scale = limits["worst_n_mm"] or worst
+        weights = np.exp(s * (values - worst) / scale)
+        ks_value = worst + scale * np.log(weights.sum()) / s
+        weights /= weights.sum()
+        info = {"eigenvalues_n_mm": values[:6].tolist(), "ks_n_mm": float(ks_value), "ks": s, "rank": self.rank,
+                "worst_wrench": self._worst_wrench(vectors[:, 0])}
+        rows = [{"name": "load_mean", "value": mean, "limit": limits["mean_n_mm"], "unit": "N mm", "sense": "<=", "g": None, "gradient": None},
+                {"name": "load_worst", "value": worst, "limit": limits["worst_n_mm"], "unit": "N mm", "sense": "<=", "g": None, "gradient": None,
+                 "info": info}]
+        if limits["mean_n_mm"]:
+            gradient = sum(solutions[name]["derivative"] for name in self.cases)
+            rows[0].update(g=mean / limits["mean_n_mm"] - 1, gradient=gradient / limits["mean_n_mm"])
+        if limits["worst_n_mm"]:
+            derivative = solutions[self.cases[0]]["modulus_derivative"]
+            keep = np.flatnonzero(weights > self.settings["ks_cutoff"])
+            gradient = sum(weights[i] * self.energy(stacked, vectors[:, i], derivative) for i in keep)
+            rows[1].update(g=float(ks_value / limits["worst_n_mm"] - 1), gradient=gradient / limits["worst_n_mm"])
+        return rows
+
     # ------------------------------------------------------------- device --
     def group_members(self):
         """Per fixture group holding covariance directions: (key, direction indices k, their parts).
@@ -129,7 +198,7 @@ class InterfaceCovariance:
             flex[np.ix_(ks, ks)] += self.factor * out.cpu().numpy()
         flex = (flex + flex.T) / 2
         s = self.settings["ks"]
-        limits = self.settings["limits"]
+        limits = self._limits()
         mean = float(np.trace(flex))
         values, vectors = np.linalg.eigh(flex)
         values, vectors = values[::-1], vectors[:, ::-1]
@@ -140,7 +209,8 @@ class InterfaceCovariance:
         weights /= weights.sum()
         rows = [{"name": "load_mean", "value": mean, "limit": limits.get("mean_n_mm"), "unit": "N mm", "sense": "<=", "g": None, "gradient": None},
                 {"name": "load_worst", "value": worst, "limit": limits.get("worst_n_mm"), "unit": "N mm", "sense": "<=", "g": None, "gradient": None,
-                 "info": {"eigenvalues_n_mm": values[:6].tolist(), "ks_n_mm": float(ks_value), "ks": s, "rank": self.rank}}]
+                 "info": {"eigenvalues_n_mm": values[:6].tolist(), "ks_n_mm": float(ks_value), "ks": s, "rank": self.rank,
+                          "worst_wrench": self._worst_wrench(vectors[:, 0])}}]
         if gradients:
             grad_mean = torch.zeros(self.system.nelem, dtype=torch.float64, device=mg.device)
             grad_worst = torch.zeros_like(grad_mean)

@@ -166,6 +166,7 @@ def covariance(topt, tprob):
     out["domain_json"] = json.dumps({k: domain[k] for k in keep})
     for name in ("allowed", "preserve", "forbidden"):
         out[f"domain_{name}"] = np.asarray(domain[name])
+    out["info_json"] = json.dumps(rows["load_worst"]["info"])
     settings = problem["covariance"]
     out["covariance_json"] = json.dumps({"support": settings["support"], "sigma": np.asarray(settings["sigma"]).tolist(),
                                          "labels": settings["labels"], "prefix": settings["prefix"], "ks": settings["ks"],

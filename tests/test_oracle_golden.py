@@ -4,7 +4,7 @@ from pathlib import Path
 
 import numpy as np
 import pytest
-from scipy.sparse.linalg import spsolve
+from scipy.sparse.linalg import splu, spsolve
 
 from oracle import covariance as ocov
 from oracle import density as oden
@@ -241,3 +241,44 @@ def test_system_diagnostics_match_reference():
         assert set(got) == set(expected), (name, set(got) ^ set(expected))
         for key in set(expected) - solver_keys:
             assert got[key] == expected[key], (name, key)
+
+
+def test_host_measure_matches_reference_rows():
+    """InterfaceCovariance.matrix / energy / measure on host solutions in HexElasticity.solve's format
+    (fields per mirror sign, per-case derivative, modulus derivative) reproduce the reference's own
+    rows on its covariance cantilever: tr, lambda_max, KS, both gradients and the info record."""
+    import json
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    g = golden("covariance")
+    domain = json.loads(str(g["domain_json"]))
+    for name in ("allowed", "preserve", "forbidden"):
+        domain[name] = g[f"domain_{name}"]
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, json.loads(str(g["covariance_json"])), domain["interfaces"])
+    shape = tuple(g["shape"])
+    moduli, slope = hex8.simp(g["density"], float(g["penalization"]), float(g["min_stiffness_ratio"]), float(g["young"]))
+    matrix = op.assemble(shape, g["ke"], moduli).tocsc()
+    solutions = {}
+    for members in system.groups.values():
+        live = op.live_dofs(shape, moduli, members[0][1]["fixed"])
+        lu = splu(matrix[live][:, live].tocsc())
+        for case, part in members:
+            u = np.zeros(system.ndof)
+            u[live] = lu.solve(part["force"][live])
+            entry = solutions.setdefault(case["name"], {"fields": {}, "energy": np.zeros(system.nelem)})
+            entry["fields"][part["sign"]] = u
+            entry["energy"] += model.factor * op.element_energy(shape, g["ke"], u)
+    for entry in solutions.values():
+        entry.update(derivative=-slope * entry.pop("energy"), modulus_derivative=slope)
+    rows = {row["name"]: row for row in model.measure(solutions)}
+    assert rows["load_mean"]["value"] == pytest.approx(float(g["load_mean"]), rel=1e-9)
+    assert rows["load_worst"]["value"] == pytest.approx(float(g["load_worst"]), rel=1e-9)
+    assert rows["load_worst"]["info"]["ks_n_mm"] == pytest.approx(float(g["ks"]), rel=1e-9)
+    assert np.linalg.norm(rows["load_mean"]["gradient"] - g["grad_mean"]) < 1e-8 * np.linalg.norm(g["grad_mean"])
+    assert np.linalg.norm(rows["load_worst"]["gradient"] - g["grad_worst"]) < 1e-8 * np.linalg.norm(g["grad_worst"])
+    info, expected = rows["load_worst"]["info"], json.loads(str(g["info_json"]))
+    assert set(info) == set(expected) and info["rank"] == expected["rank"] and info["ks"] == expected["ks"]
+    assert np.allclose(info["eigenvalues_n_mm"], expected["eigenvalues_n_mm"], rtol=1e-9)
+    assert [label for label, _ in info["worst_wrench"]] == [label for label, _ in expected["worst_wrench"]]
+    assert np.allclose([v for _, v in info["worst_wrench"]], [v for _, v in expected["worst_wrench"]], rtol=1e-9, atol=1e-12)
