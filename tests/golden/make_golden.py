@@ -373,6 +373,22 @@ def system_diagnostics(topt):
     np.savez_compressed(OUT / "diagnostics.npz", **out)
 
 
+def solve_metrics(topt):
+    """The reference's metrics records (HexElasticity.solve(..., metrics=True), SuperLU) on the plain
+    diagnostic beam and on the mirrored half relief domain, with the seeded densities used."""
+    out = {}
+    domains = {"plain": diagnostic_domains()["plain"][0], "relief_half": relief_domains()["relief_half"]}
+    for name, domain in domains.items():
+        system = topt.HexElasticity(domain, linear_solver="cpu_superlu")
+        density = np.random.default_rng(5).uniform(0.2, 1.0, system.nelem)
+        result = system.solve(density, metrics=True)
+        keep = ("max_displacement_mm", "max_von_mises_mpa", "loads", "stiffness_n_per_mm")
+        out[f"{name}_density"] = density
+        out[f"{name}_metrics"] = json.dumps({case: {key: entry[key] for key in keep} for case, entry in result.items()})
+        system.close()
+    np.savez_compressed(OUT / "metrics.npz", **out)
+
+
 def relief_domains():
     """The domains stored in inertia_relief.npz, rebuilt from their JSON text."""
     relief = np.load(OUT / "inertia_relief.npz")
@@ -392,7 +408,7 @@ def main(source):
              "cantilever_small": lambda: direct(topt, (16, 8, 8), 0, "cantilever_small"), "filter": lambda: density_filter(topt),
              "covariance": lambda: covariance(topt, tprob), "oc": lambda: optimality_criteria(topt),
              "inertia_relief": lambda: inertia_relief(topt), "plate_setup": lambda: plate_setup(topt, tprob),
-             "diagnostics": lambda: system_diagnostics(topt),
+             "diagnostics": lambda: system_diagnostics(topt), "metrics": lambda: solve_metrics(topt),
              "cantilever_48x24x24": lambda: direct(topt, (48, 24, 24), 0, "cantilever_48x24x24")}
     only = next((arg.split("=", 1)[1] for arg in sys.argv if arg.startswith("--only=")), None)
     for name, step in steps.items():

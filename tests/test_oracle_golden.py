@@ -282,3 +282,44 @@ def test_host_measure_matches_reference_rows():
     assert np.allclose(info["eigenvalues_n_mm"], expected["eigenvalues_n_mm"], rtol=1e-9)
     assert [label for label, _ in info["worst_wrench"]] == [label for label, _ in expected["worst_wrench"]]
     assert np.allclose([v for _, v in info["worst_wrench"]], [v for _, v in expected["worst_wrench"]], rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["plain", "relief_half"])
+def test_solve_metrics_match_reference(name):
+    """The metrics record of HexElasticity.solve(..., metrics=True) (per-load mean and directional
+    displacement, load stiffness, peak displacement, peak von Mises stress) from the product's host
+    code, fed displacements of the oracle's direct solves, equals the reference's own record
+    (tests/golden/metrics.npz, SuperLU) on a full beam and on a mirrored half relief domain."""
+    import importlib.util
+    import json
+    from deep_frame_b200.elasticity import HexElasticity
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    make_golden = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(make_golden)
+    domain = {"plain": make_golden.diagnostic_domains()["plain"][0], "relief_half": make_golden.relief_domains()["relief_half"]}[name]
+    g = golden("metrics")
+    expected = json.loads(str(g[f"{name}_metrics"]))
+    system = HexElasticity(domain)
+    shape = tuple(domain["grid"]["shape"])
+    moduli, _ = system.moduli(g[f"{name}_density"], 3.0, 1e-6)
+    matrix = op.assemble(shape, system.ke, moduli).tocsc()
+    for case in system.cases:
+        if case["name"] not in expected:
+            continue
+        direct, mirror = np.zeros(system.ndof), np.zeros(system.ndof)
+        for part in case["parts"]:
+            live = op.live_dofs(shape, moduli, part["fixed"])
+            u = np.zeros(system.ndof)
+            u[live] = spsolve(matrix[live][:, live].tocsc(), part["force"][live])
+            direct += u
+            mirror += part["sign"] * u
+        got = system._metrics([direct] if system.symmetry is None else [direct, mirror], moduli, case)
+        want = expected[case["name"]]
+        assert got["max_displacement_mm"] == pytest.approx(want["max_displacement_mm"], rel=1e-8)
+        assert got["max_von_mises_mpa"] == pytest.approx(want["max_von_mises_mpa"], rel=1e-8)
+        assert (got["stiffness_n_per_mm"] is None) == (want["stiffness_n_per_mm"] is None)
+        assert len(got["loads"]) == len(want["loads"])
+        for a, b in zip(got["loads"], want["loads"]):
+            assert a["node_count"] == b["node_count"] and np.allclose(a["force_n"], b["force_n"], rtol=1e-12)
+            assert np.allclose(a["mean_displacement_mm"], b["mean_displacement_mm"], rtol=1e-8, atol=1e-12)
+            assert a["directional_displacement_mm"] == pytest.approx(b["directional_displacement_mm"], rel=1e-8, abs=1e-14)
