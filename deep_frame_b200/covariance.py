@@ -54,20 +54,32 @@ class InterfaceCovariance:
         self._groups = None
 
     def wrenches(self, interface):
+        """Per unit wrench component (Fx, Fy, Fz, Mx, My, Mz about the interface's reference point):
+        (direct dofs, direct values, mirror dofs, mirror values) of the least-norm nodal forces over the
+        interface nodes that carry exactly that wrench, f = B^T (B B^T)^-1 e_j with B_i = [I; [r_i]x]
+        (topology_problem.py:624-638).  Mirror-side nodes enter with their reflected positions and get
+        their forces reflected back."""
         system = self.system
-        picked = [system._select_both(region, "covariance", "load") for region in interface["regions"]]
-        direct, mirror = (np.unique(np.concatenate([item[side] for item in picked])) for side in (0, 1))
-        flip = np.ones(3) if system.symmetry is None else system._flip()
-        arms = np.concatenate([system.points[direct], system.points[mirror] * flip]) - np.asarray(interface["reference_mm"], dtype=float)
-        if np.linalg.matrix_rank(arms - arms[0], tol=1e-8) < 2:
+        sides = [system._select_both(region, "covariance", "load") for region in interface["regions"]]
+        direct = np.unique(np.concatenate([here for here, _ in sides]))
+        mirror = np.unique(np.concatenate([there for _, there in sides]))
+        reflect = np.ones(3) if system.symmetry is None else system._flip()
+        r = np.vstack([system.points[direct], system.points[mirror] * reflect]) - np.asarray(interface["reference_mm"], dtype=float)
+        if np.linalg.matrix_rank(r - r[0], tol=1e-8) < 2:
             raise ValueError("An interface wrench needs at least three non-collinear nodes")
-        b = np.zeros((6, 3 * len(arms)))
-        for index, (x, y, z) in enumerate(arms):
-            b[:3, 3 * index:3 * index + 3] = np.eye(3)
-            b[3:, 3 * index:3 * index + 3] = [[0, -z, y], [z, 0, -x], [-y, x, 0]]
-        nodal = (b.T @ np.linalg.solve(b @ b.T, np.eye(6))).reshape(len(arms), 3, 6)
-        dofs = lambda nodes: (3 * nodes[:, None] + np.arange(3)).ravel()
-        return [(dofs(direct), nodal[:len(direct), :, j].ravel(), dofs(mirror), (nodal[len(direct):, :, j] * flip).ravel()) for j in range(6)]
+        count = len(r)
+        # B as [6, node, 3]: a force f_i at r_i contributes f_i to the resultant and r_i x f_i to the moment
+        b = np.zeros((6, count, 3))
+        b[0, :, 0] = b[1, :, 1] = b[2, :, 2] = 1.0
+        x, y, z = r.T
+        b[3, :, 1], b[3, :, 2] = -z, y
+        b[4, :, 0], b[4, :, 2] = z, -x
+        b[5, :, 0], b[5, :, 1] = -y, x
+        flat = b.reshape(6, 3 * count)
+        nodal = np.linalg.solve(flat @ flat.T, flat).reshape(6, count, 3)            # row j: the forces for e_j
+        dof = lambda nodes: (3 * nodes[:, None] + np.arange(3)).ravel()
+        k = len(direct)
+        return [(dof(direct), nodal[j, :k].ravel(), dof(mirror), (nodal[j, k:] * reflect).ravel()) for j in range(6)]
 
     def _worst_wrench(self, vector):
         """The six interface wrench components of largest magnitude in Sigma^1/2's image of F's top
@@ -101,13 +113,12 @@ class InterfaceCovariance:
         return (flexibility + flexibility.T) / 2, stacked
 
     def energy(self, stacked, vector, derivative):
-        """-factor * dE/drho * sum_s (U_s v)_e^T K0 (U_s v)_e per element: the sensitivity of v^T F v
-        (the reference's energy, topology_problem.py:647-652)."""
-        total = np.zeros(self.system.nelem)
-        for field in stacked.values():
-            ue = (field @ vector)[self.system.dofs]
-            total += np.einsum("ei,ij,ej->e", ue, self.system.ke, ue, optimize=True)
-        return -self.factor * np.asarray(derivative) * total
+        """Sensitivity of v^T F v to the element densities: -factor * dE/drho times the strain energy
+        density of the combined displacement U_s v, summed over mirror signs
+        (topology_problem.py:647-652)."""
+        combined = [field @ vector for field in stacked.values()]
+        per_element = sum(np.einsum("ea,ab,eb->e", u[self.system.dofs], self.system.ke, u[self.system.dofs], optimize=True) for u in combined)
+        return -self.factor * np.asarray(derivative) * per_element
 
     def measure(self, solutions):
         """The load_mean / load_worst rows from host solutions (the reference's measure,

@@ -75,3 +75,31 @@ def test_relief_cases_are_balanced_and_oracle_compliance_matches(name):
                 reaction = matrix @ u - part["force"]
                 assert np.max(np.abs(reaction[part["support"]])) < 1e-9 * np.abs(part["force"]).sum()
         assert compliance == pytest.approx(float(GOLDEN[f"{name}_{case_name}_compliance"]), rel=1e-9)
+
+
+@pytest.mark.parametrize("name", ["relief_full", "relief_half"])
+def test_balanced_relief_cases_leave_the_support_unloaded(name):
+    """support_reactions (the reference's check, topology_optimization.py:570-580) on the relief
+    domains, with a SciPy stand-in for the device direct solver: the d'Alembert loads balance every
+    part, so its determinate support carries (numerically) nothing."""
+    from scipy.sparse.linalg import splu
+    from deep_frame_b200.elasticity import HexElasticity
+
+    class HostSolver:
+        def __init__(self, matrix, rhs):
+            self.lu = splu(matrix.tocsc())
+
+        def solve(self, matrix, rhs):
+            return self.lu.solve(rhs)
+
+        def close(self):
+            return []
+
+    system = HexElasticity(domain_of(name))
+    density = GOLDEN[f"{name}_density"]
+    for case in system.cases:
+        if "inertia_relief" not in case:
+            continue
+        for row in system.support_reactions(density, case["name"], solver=HostSolver):
+            assert row["support_dofs"] >= 3
+            assert row["max_reaction_n"] < 1e-9 * row["nodal_force_sum_n"]
