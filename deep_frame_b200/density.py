@@ -198,21 +198,17 @@ class DensityMap:
         return self._host(self.pullback_device(self._dev(sensitivity), self._dev(projection_derivative)))
 
     def initial(self, target):
-        design = np.zeros(self.n)
-        design[self.preserve] = 1
-        lower = self.settings["minimum_design_density"]
-        design[self.free] = lower
+        """Uniform free density whose physical volume meets ``target`` (preserves at 1), found by 70
+        bisection steps from the minimum design density up (topology_optimization.py:1179-1195)."""
+        design = np.where(self.preserve, 1.0, 0.0)
+        low, high = self.settings["minimum_design_density"], 1.0
+        design[self.free] = low
         if self.volume(design) > target + 1e-8:
             raise ValueError("Volume budget cannot contain preserves and their filtered transition")
-        upper = 1.0
         for _ in range(70):
-            value = (lower + upper) / 2
-            design[self.free] = value
-            if self.volume(design) > target:
-                upper = value
-            else:
-                lower = value
-        design[self.free] = lower
+            design[self.free] = mid = 0.5 * (low + high)
+            low, high = (low, mid) if self.volume(design) > target else (mid, high)
+        design[self.free] = low
         return design
 
     def close(self):

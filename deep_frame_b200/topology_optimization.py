@@ -131,59 +131,61 @@ def _settings(settings):
 
 
 def validate_masks(domain):
-    """Boolean masks of grid shape, forbidden = ~allowed, preserve within allowed, some free cell (:1056-1069)."""
+    """(allowed, preserve, forbidden) as flat boolean arrays after the reference's checks
+    (topology_optimization.py:1056-1069): grid-shaped booleans, forbidden the complement of allowed,
+    preserve inside allowed, and at least one free cell."""
     shape = tuple(domain["grid"]["shape"])
-    masks = []
-    for name in ("allowed", "preserve", "forbidden"):
-        array = np.asarray(domain[name])
-        if array.shape != shape or array.dtype != bool:
+    arrays = {name: np.asarray(domain[name]) for name in ("allowed", "preserve", "forbidden")}
+    for name, array in arrays.items():
+        if array.dtype != bool or array.shape != shape:
             raise ValueError(f"{name} must be a boolean array with grid shape")
-        masks.append(array.ravel().copy())
-    allowed, preserve, forbidden = masks
-    if not np.array_equal(forbidden, ~allowed) or np.any(preserve & forbidden):
+    allowed, preserve, forbidden = (arrays[name].ravel().copy() for name in ("allowed", "preserve", "forbidden"))
+    if (forbidden != ~allowed).any() or (preserve & forbidden).any():
         raise ValueError("Forbidden must complement allowed; preserve must be allowed")
-    if not np.any(allowed & ~preserve):
+    if not (allowed & ~preserve).any():
         raise ValueError("The design domain has no free material cells")
     return allowed, preserve, forbidden
 
 
 def continuation_decision(iterations, final_level, change, violation, minimum, maximum, change_tolerance, violation_tolerance):
-    """"converged" / "advance" / "iteration_cap" / None for one continuation level (topology_optimization.py:17-25)."""
-    violation_tolerance = 1e-3 if violation_tolerance is None else violation_tolerance
-    settled = change is not None and np.isfinite(change) and change < change_tolerance
-    feasible = np.isfinite(violation) and violation <= violation_tolerance
-    if iterations >= minimum and settled and feasible:
+    """The reference's stopping rule for one continuation level (topology_optimization.py:17-25):
+    "converged" (final level) or "advance" once past the minimum iterations with a design change
+    below tolerance and a feasible design; at the iteration cap "iteration_cap" on the final level
+    (or when the cap is below the minimum), "advance" otherwise; None to keep iterating."""
+    limit = 1e-3 if violation_tolerance is None else violation_tolerance
+    done = (iterations >= minimum and change is not None and np.isfinite(change) and change < change_tolerance
+            and np.isfinite(violation) and violation <= limit)
+    if done:
         return "converged" if final_level else "advance"
-    if iterations >= maximum:
-        return "iteration_cap" if final_level or iterations < minimum else "advance"
-    return None
+    if iterations < maximum:
+        return None
+    return "iteration_cap" if (final_level or iterations < minimum) else "advance"
 
 
 def _case_scaling(solutions, settings):
-    """Per-case weight / (total weight * first compliance) (:1235-1245)."""
-    supplied = settings["case_weights"]
-    if set(supplied) - set(solutions):
+    """(objective scale per case, first compliances, normalised weights): each static case counts with
+    weight / total weight / its first compliance (topology_optimization.py:1235-1245)."""
+    given = settings["case_weights"]
+    if not set(given) <= set(solutions):
         raise ValueError("case_weights references an unknown static load case")
-    weights = {name: float(supplied.get(name, 1.0)) for name in solutions}
-    if any(not np.isfinite(weight) or weight <= 0 for weight in weights.values()):
+    weights = {name: float(given.get(name, 1.0)) for name in solutions}
+    if not all(np.isfinite(w) and w > 0 for w in weights.values()):
         raise ValueError("Every static load case requires a finite positive weight")
     total = sum(weights.values())
-    normalization = {name: result["compliance_n_mm"] for name, result in solutions.items()}
-    return ({name: weights[name] / total / normalization[name] for name in solutions}, normalization,
-            {name: weight / total for name, weight in weights.items()})
+    first = {name: entry["compliance_n_mm"] for name, entry in solutions.items()}
+    shares = {name: w / total for name, w in weights.items()}
+    return {name: shares[name] / first[name] for name in solutions}, first, shares
 
 
 def _history_entry(iteration, physical_sum, solutions, scales, change, elapsed, final=False):
-    return {
-        "iteration": iteration,
-        "final_evaluation": final,
-        "objective": float(sum(scales[name] * result["compliance_n_mm"] for name, result in solutions.items())),
-        "physical_density_sum": float(physical_sum),
-        "compliances_n_mm": {name: result["compliance_n_mm"] for name, result in solutions.items()},
-        "maximum_design_change": change,
-        "maximum_relative_residual": float(max(result["relative_residual"] for result in solutions.values())),
-        "elapsed_s": elapsed,
-    }
+    """One record of the OC history with the reference's keys (topology_optimization.py:1246-1256)."""
+    compliances = {name: entry["compliance_n_mm"] for name, entry in solutions.items()}
+    return {"iteration": iteration, "final_evaluation": final,
+            "objective": float(sum(scales[name] * value for name, value in compliances.items())),
+            "physical_density_sum": float(physical_sum), "compliances_n_mm": compliances,
+            "maximum_design_change": change,
+            "maximum_relative_residual": float(max(entry["relative_residual"] for entry in solutions.values())),
+            "elapsed_s": elapsed}
 
 
 def _stage_entry(mapping, sums, volume_target, move_limit):
