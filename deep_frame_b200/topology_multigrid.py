@@ -490,30 +490,28 @@ class GeometricMultigrid:
 
 
 def solve_elasticity(system, multigrid, physical_density, penalization=3.0, min_stiffness_ratio=1e-6):
-    """Compliance and sensitivities of every static case (topology_multigrid.py:553-581) on the device."""
-    torch = multigrid.torch
-    density = np.asarray(physical_density, dtype=float).ravel()
-    moduli = system.young * (min_stiffness_ratio + (1 - min_stiffness_ratio) * density ** penalization)
-    derivative = system.young * (1 - min_stiffness_ratio) * penalization * density ** (penalization - 1)
-    moduli[~system.active_elements] = 0
-    derivative[~system.active_elements] = 0
+    """Compliance, sensitivity and displacement fields of every static case of ``system`` with the
+    device multigrid (the reference's module-level solve_elasticity, topology_multigrid.py:553-581):
+    one batched solve per fixture group, the parts of a case summed with the half-model factor."""
+    moduli, slope = system.moduli(physical_density, penalization, min_stiffness_ratio)
     multigrid.update(moduli)
-    factor = 1.0 if system.symmetry is None else 2.0
+    factor = 2.0 if system.symmetry is not None else 1.0
     results = {}
     for members in system.groups.values():
-        part = members[0][1]
-        forces = np.column_stack([member["force"] for _, member in members])
-        columns = multigrid._columns(forces)
-        solutions, report = multigrid.solve_device(part["fixed"].tobytes(), part["fixed"], columns)
-        energies = multigrid.energy_device(solutions).cpu().numpy()
-        host = solutions.cpu().numpy()
-        for column, (case, member) in enumerate(members):
-            entry = results.setdefault(case["name"], {"compliance_n_mm": 0.0, "energy": np.zeros(system.nelem), "relative_residual": 0.0, "iterations": [], "fields": {}})
-            entry["compliance_n_mm"] += factor * float(member["force"] @ host[column])
+        held = members[0][1]["fixed"]
+        u, report = multigrid.solve_device(held.tobytes(), held, multigrid._columns(np.column_stack([part["force"] for _, part in members])))
+        energies = multigrid.energy_device(u).cpu().numpy()
+        host = u.cpu().numpy()
+        for column, (case, part) in enumerate(members):
+            entry = results.get(case["name"])
+            if entry is None:
+                entry = results[case["name"]] = {"compliance_n_mm": 0.0, "energy": np.zeros(system.nelem), "relative_residual": 0.0,
+                                                 "iterations": [], "fields": {}}
+            entry["compliance_n_mm"] += factor * float(host[column] @ part["force"])
             entry["energy"] += factor * energies[column]
             entry["relative_residual"] = max(entry["relative_residual"], report["relative_residual"][column])
             entry["iterations"].append(report["iterations"][column])
-            entry["fields"][member["sign"]] = host[column]
+            entry["fields"][part["sign"]] = host[column]
     for entry in results.values():
-        entry["derivative"] = -derivative * entry.pop("energy")
+        entry["derivative"] = -slope * entry.pop("energy")
     return results
