@@ -74,56 +74,65 @@ def _positive_integer(value):
     return not isinstance(value, bool) and int(value) == value and value >= 1
 
 
+def _is_positive_finite(value):
+    return bool(np.isfinite(value)) and value > 0
+
+
+def _robust_ok(s):
+    delta, eta = s["robust_delta"], s["projection_eta"]
+    return s["projection"] != "robust" or (np.isfinite(delta) and delta > 0 and 0 < eta - delta < eta + delta < 1)
+
+
+def _schedule_ok(schedule):
+    if schedule is None:
+        return True
+    values = [float(beta) for beta in schedule]
+    return bool(values) and all(np.isfinite(values)) and values[0] > 0 and all(b > a for a, b in zip(values, values[1:]))
+
+
+# The reference's settings rules in its order, each with its message (topology_optimization.py:993-1054).
+_RULES = (
+    [(lambda s, n=name: _is_positive_finite(s[n]), f"{name} must be finite and positive")
+     for name in ("filter_radius_mm", "penalization", "min_stiffness_ratio", "change_tolerance", "move_limit", "minimum_design_density")]
+    + [(lambda s, n=name: _positive_integer(s[n]), f"{name} must be a positive integer") for name in ("max_iterations", "minimum_iterations")]
+    + [(lambda s: bool(np.isfinite(s["volume_fraction"])) and 0 < s["volume_fraction"] <= 1, "volume_fraction must be in (0, 1]"),
+       (lambda s: s["penalization"] >= 1 and 0 < s["min_stiffness_ratio"] < 1 and s["minimum_design_density"] < 1 and s["move_limit"] <= 1,
+        "Invalid SIMP or OC settings"),
+       (lambda s: bool(np.isfinite(s["projection_beta"])) and s["projection_beta"] >= 0 and 0 < s["projection_eta"] < 1,
+        "Invalid density projection settings"),
+       (lambda s: s["max_runtime_s"] is None or _is_positive_finite(s["max_runtime_s"]), "max_runtime_s must be positive or None"),
+       (lambda s: s["interface_node_policy"] in ("allowed_adjacent", "preserve_adjacent"), "Invalid topology interface_node_policy"),
+       (lambda s: s["linear_solver"] in LINEAR_SOLVERS, "Invalid topology linear_solver"),
+       (lambda s: s["gpu_solver_residency"] in ("resident", "transient"), "Invalid topology gpu_solver_residency"),
+       (lambda s: s["density_filter"] in DENSITY_FILTERS, "Invalid topology density_filter"),
+       (lambda s: s["projection"] in ("single", "robust"), "Invalid topology projection"),
+       (_robust_ok, "Robust projection thresholds must lie within (0, 1)")]
+    + [(lambda s, n=name: _positive_integer(s[n]), f"{name} must be a positive integer") for name in ("beta_interval", "beta_minimum_iterations")]
+    + [(lambda s: not isinstance(s["objective_window"], bool) and int(s["objective_window"]) == s["objective_window"] and s["objective_window"] >= 2,
+        "objective_window must be an integer of at least 2"),
+       (lambda s: _schedule_ok(s["beta_schedule"]), "beta_schedule must be a nonempty strictly increasing list of positive values"),
+       (lambda s: s["move_limit_late"] is None or (bool(np.isfinite(s["move_limit_late"])) and 0 < s["move_limit_late"] <= 1),
+        "move_limit_late must be in (0, 1] or None"),
+       (lambda s: _is_positive_finite(s["beta_change_tolerance"]) and bool(np.isfinite(s["move_limit_late_beta"]))
+        and bool(np.isfinite(s["volume_target_relaxation"])) and 0 < s["volume_target_relaxation"] <= 1, "Invalid beta continuation settings")]
+)
+
+
 def _settings(settings):
-    """Defaults plus validation with the reference's rules and messages (topology_optimization.py:993-1054)."""
+    """Defaults plus the reference's validation rules and messages, checked in the reference's order;
+    the minimum iteration counts are clipped to their maxima and the beta schedule made floats.
+    Options this library does not implement are rejected as invalid."""
     result = deepcopy(DEFAULT_SETTINGS)
     result.update(deepcopy(settings))
-    for name in ("filter_radius_mm", "penalization", "min_stiffness_ratio", "change_tolerance", "move_limit", "minimum_design_density"):
-        if not np.isfinite(result[name]) or result[name] <= 0:
-            raise ValueError(f"{name} must be finite and positive")
-    for name in ("max_iterations", "minimum_iterations"):
-        if not _positive_integer(result[name]):
-            raise ValueError(f"{name} must be a positive integer")
-    result["minimum_iterations"] = min(result["minimum_iterations"], result["max_iterations"])
-    if not np.isfinite(result["volume_fraction"]) or not 0 < result["volume_fraction"] <= 1:
-        raise ValueError("volume_fraction must be in (0, 1]")
-    if result["penalization"] < 1 or not 0 < result["min_stiffness_ratio"] < 1 or result["minimum_design_density"] >= 1 or result["move_limit"] > 1:
-        raise ValueError("Invalid SIMP or OC settings")
-    if not np.isfinite(result["projection_beta"]) or result["projection_beta"] < 0 or not 0 < result["projection_eta"] < 1:
-        raise ValueError("Invalid density projection settings")
-    if result["max_runtime_s"] is not None and (not np.isfinite(result["max_runtime_s"]) or result["max_runtime_s"] <= 0):
-        raise ValueError("max_runtime_s must be positive or None")
-    if result["interface_node_policy"] not in ("allowed_adjacent", "preserve_adjacent"):
-        raise ValueError("Invalid topology interface_node_policy")
-    if result["linear_solver"] not in LINEAR_SOLVERS:
-        raise ValueError("Invalid topology linear_solver")
-    if result["gpu_solver_residency"] not in ("resident", "transient"):
-        raise ValueError("Invalid topology gpu_solver_residency")
-    if result["density_filter"] not in DENSITY_FILTERS:
-        raise ValueError("Invalid topology density_filter")
-    if result["projection"] not in ("single", "robust"):
-        raise ValueError("Invalid topology projection")
-    delta, eta = result["robust_delta"], result["projection_eta"]
-    if result["projection"] == "robust" and (not np.isfinite(delta) or delta <= 0 or not 0 < eta - delta < eta + delta < 1):
-        raise ValueError("Robust projection thresholds must lie within (0, 1)")
-    for name in ("beta_interval", "beta_minimum_iterations"):
-        if not _positive_integer(result[name]):
-            raise ValueError(f"{name} must be a positive integer")
-    if isinstance(result["objective_window"], bool) or int(result["objective_window"]) != result["objective_window"] or result["objective_window"] < 2:
-        raise ValueError("objective_window must be an integer of at least 2")
-    result["beta_minimum_iterations"] = min(result["beta_minimum_iterations"], result["beta_interval"])
+    for rule, message in _RULES:
+        if not rule(result):
+            raise ValueError(message)
+        if message.startswith("minimum_iterations"):
+            result["minimum_iterations"] = min(result["minimum_iterations"], result["max_iterations"])
+        if message.startswith("beta_minimum_iterations"):
+            result["beta_minimum_iterations"] = min(result["beta_minimum_iterations"], result["beta_interval"])
     if result["beta_schedule"] is not None:
-        schedule = [float(beta) for beta in result["beta_schedule"]]
-        if not schedule or not np.all(np.isfinite(schedule)) or schedule[0] <= 0 or np.any(np.diff(schedule) <= 0):
-            raise ValueError("beta_schedule must be a nonempty strictly increasing list of positive values")
-        result["beta_schedule"] = schedule
-    late = result["move_limit_late"]
-    if late is not None and (not np.isfinite(late) or not 0 < late <= 1):
-        raise ValueError("move_limit_late must be in (0, 1] or None")
-    relaxation = result["volume_target_relaxation"]
-    if not np.isfinite(result["beta_change_tolerance"]) or result["beta_change_tolerance"] <= 0 or not np.isfinite(result["move_limit_late_beta"]) \
-            or not np.isfinite(relaxation) or not 0 < relaxation <= 1:
-        raise ValueError("Invalid beta continuation settings")
+        result["beta_schedule"] = [float(beta) for beta in result["beta_schedule"]]
     for name, what in (("modal", "modal constraints"), ("corridor", "corridor blends"), ("prop_discs", "prop-disc volume weights")):
         if result[name] is not None:
             raise ValueError(f"{what} are not part of this library")
