@@ -26,12 +26,18 @@ def elasticity_matrix(poisson_ratio):
 
 
 def orthotropic_matrix(constants):
-    exy, ez = constants["e_xy_mpa"], constants["e_z_mpa"]
-    nxy, nxz = constants["nu_xy"], constants["nu_xz"]
-    compliance = np.zeros((6, 6))
-    compliance[:3, :3] = np.array([[1.0, -nxy, -nxz], [-nxy, 1.0, -nxz], [-nxz, -nxz, exy / ez]]) / exy
-    compliance[3:, 3:] = np.diag([1 / constants["g_xy_mpa"], 1 / constants["g_z_mpa"], 1 / constants["g_z_mpa"]])
-    if np.any(np.linalg.eigvalsh(compliance) <= 0):
+    """Stiffness of a transversely isotropic material (in-plane x-y, axis z) from its engineering
+    constants: the inverse of the compliance with 1/E on the normal diagonal, -nu/E off it (nu_xz
+    for every coupling with z, taken over E_xy) and 1/G on the shear diagonal (G_xy, G_z, G_z);
+    rejected unless that compliance is positive definite (topology_optimization.py:260-267)."""
+    e_in, e_z = constants["e_xy_mpa"], constants["e_z_mpa"]
+    poisson = np.array([[0.0, constants["nu_xy"], constants["nu_xz"]],
+                        [constants["nu_xy"], 0.0, constants["nu_xz"]],
+                        [constants["nu_xz"], constants["nu_xz"], 0.0]])
+    normal = np.diag([1.0 / e_in, 1.0 / e_in, 1.0 / e_z]) - poisson / e_in
+    shear = np.diag(1.0 / np.array([constants["g_xy_mpa"], constants["g_z_mpa"], constants["g_z_mpa"]], dtype=float))
+    compliance = np.block([[normal, np.zeros((3, 3))], [np.zeros((3, 3)), shear]])
+    if np.linalg.eigvalsh(compliance).min() <= 0:
         raise ValueError("Orthotropic engineering constants are not positive definite")
     return np.linalg.inv(compliance)
 
@@ -85,14 +91,16 @@ def regular_grid(grid):
 
 
 def select_nodes(points, region):
+    """Indices of the nodes inside an axis-aligned box region (bounds included, 1e-7 mm slack);
+    an empty box raises "Empty topology node selector" (topology_optimization.py:321-331)."""
     if region.get("kind") != "box":
         raise ValueError("Topology node selectors must be boxes")
-    lo = np.asarray(region["min_mm"], dtype=float)
-    hi = np.asarray(region["max_mm"], dtype=float)
-    if lo.shape != (3,) or hi.shape != (3,) or not np.all(np.isfinite([lo, hi])) or np.any(lo > hi):
+    bounds = np.array([region["min_mm"], region["max_mm"]], dtype=float)
+    if bounds.shape != (2, 3) or not np.isfinite(bounds).all() or (bounds[0] > bounds[1]).any():
         raise ValueError("Invalid node-selection box")
-    inside = np.flatnonzero(((points >= lo - 1e-7) & (points <= hi + 1e-7)).all(axis=1))
-    if not len(inside):
+    outside = np.maximum((bounds[0] - 1e-7) - points, points - (bounds[1] + 1e-7)).max(axis=1)
+    inside = np.flatnonzero(outside <= 0)
+    if inside.size == 0:
         raise ValueError(f"Empty topology node selector: {region}")
     return inside
 
