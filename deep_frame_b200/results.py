@@ -31,29 +31,32 @@ def _host(value):
     return value
 
 
+_LEAF = ((np.ndarray, lambda v: v.tolist()), (np.generic, lambda v: v.item()), (Path, str))
+
+
 def jsonable(value):
     """Plain-JSON copy: dict keys as strings, arrays and tensors as lists, NumPy scalars as Python numbers."""
     value = _host(value)
+    for kind, convert in _LEAF:
+        if isinstance(value, kind):
+            return convert(value)
     if isinstance(value, dict):
         return {str(key): jsonable(item) for key, item in value.items()}
     if isinstance(value, (tuple, list)):
-        return [jsonable(item) for item in value]
-    if isinstance(value, np.ndarray):
-        return value.tolist()
-    if isinstance(value, np.generic):
-        return value.item()
-    if isinstance(value, Path):
-        return str(value)
+        return list(map(jsonable, value))
     return value
 
 
 def save_json(path, value):
-    """Atomic JSON write (temporary file, then replace); NaN and infinities raise ValueError."""
-    path = Path(path)
-    path.parent.mkdir(parents=True, exist_ok=True)
-    temporary = path.with_suffix(path.suffix + ".tmp")
-    temporary.write_text(json.dumps(jsonable(value), indent=2, allow_nan=False), encoding="utf-8")
-    temporary.replace(path)
+    """Write ``value`` as JSON so that readers see the old file or the complete new one, never a part:
+    the text goes to a sibling temporary file that then replaces the target.  NaN and infinities
+    raise ValueError (and leave the target untouched)."""
+    target = Path(path)
+    target.parent.mkdir(parents=True, exist_ok=True)
+    text = json.dumps(jsonable(value), indent=2, allow_nan=False)
+    staging = target.with_name(target.name + ".tmp")
+    staging.write_text(text, encoding="utf-8")
+    staging.replace(target)
 
 
 def read_json(path):
@@ -70,22 +73,19 @@ def artifact(path, directory):
 
 
 def valid_artifacts(record, directory):
-    """True when every artifact with a digest exists under ``directory`` with that digest."""
-    directory = Path(directory)
-    for item in record.get("artifacts", {}).values():
-        if not isinstance(item, dict) or "sha256" not in item:
-            continue
-        path = directory / item["path"]
-        if not path.is_file() or file_digest(path) != item["sha256"]:
-            return False
-    return True
+    """True when every artifact of ``record`` that names a digest is a file under ``directory`` with
+    that SHA-256."""
+    root = Path(directory)
+    listed = [item for item in record.get("artifacts", {}).values() if isinstance(item, dict) and "sha256" in item]
+    return all((root / item["path"]).is_file() and file_digest(root / item["path"]) == item["sha256"] for item in listed)
 
 
 def save_fields(path, domain, result):
-    arrays = {name: np.asarray(domain[name], dtype=bool) for name in ("allowed", "preserve", "forbidden")}
-    arrays["density"] = np.asarray(_host(result["density"]), dtype=float)
+    """fields.npz: the domain masks and the result's physical (and, if present, design) density."""
+    arrays = {"density": np.asarray(_host(result["density"]), dtype=float)}
     if result.get("design_density") is not None:
         arrays["design_density"] = np.asarray(_host(result["design_density"]), dtype=float)
+    arrays.update({name: np.asarray(domain[name], dtype=bool) for name in ("allowed", "preserve", "forbidden")})
     Path(path).parent.mkdir(parents=True, exist_ok=True)
     np.savez_compressed(path, **arrays)
 
