@@ -128,19 +128,23 @@ class GeometricMultigrid:
         return data.T.contiguous()
 
     def grid(self, flat, dtype=None):
-        """Flat [ndof, R] -> reference grid layout [R, 3, padded nodes] (topology_multigrid.py:80-88)."""
+        """Flat [ndof, R] (dof = 3 node + component, C-order nodes) -> the reference's grid layout
+        [R, 3, padded nodes] with zeros in the padding (topology_multigrid.py:80-88)."""
         torch = self.torch
-        flat = torch.as_tensor(flat, device=self.device, dtype=dtype or torch.float64)
-        flat = flat[:, None] if flat.ndim == 1 else flat
-        count = flat.shape[1]
-        out = torch.zeros((count, 3) + self.levels[0].nodes, dtype=flat.dtype, device=self.device)
-        n = self.nodes
-        out[:, :, :n[0], :n[1], :n[2]] = flat.T.reshape((count,) + n + (3,)).permute(0, 4, 1, 2, 3)
+        values = torch.as_tensor(flat, device=self.device, dtype=dtype or torch.float64)
+        if values.ndim == 1:
+            values = values.unsqueeze(1)
+        columns = values.shape[1]
+        nx, ny, nz = self.nodes
+        planes = values.T.reshape(columns, nx, ny, nz, 3).movedim(-1, 1)          # component planes [R, 3, nx, ny, nz]
+        out = values.new_zeros((columns, 3) + tuple(self.levels[0].nodes))
+        out[..., :nx, :ny, :nz] = planes
         return out
 
     def flat(self, grid):
-        n = self.nodes
-        return grid[:, :, :n[0], :n[1], :n[2]].permute(0, 2, 3, 4, 1).reshape(grid.shape[0], -1).T
+        """Inverse of ``grid``: [R, 3, padded nodes] -> [ndof, R] without the padding."""
+        nx, ny, nz = self.nodes
+        return grid[..., :nx, :ny, :nz].movedim(1, -1).reshape(grid.shape[0], -1).T
 
     def element_field(self, values, dtype=None):
         torch = self.torch

@@ -150,3 +150,22 @@ def test_cleanup_errors_follow_the_primary_error(monkeypatch):
     assert result["status"] == "failed" and result["history"] == []
     assert result["diagnostics"] == ["CUDA solve unavailable in controlled test", "cleanup failed in controlled test"]
     assert closed == ["system", "mapping"]
+
+
+def test_grid_layout_round_trip():
+    """GeometricMultigrid.grid / .flat (the reference's layout helpers, topology_multigrid.py:80-96) on
+    the CPU: dof 3 n + c of node n = (i, j, k) lands at [column, c, i, j, k], padding stays zero and
+    flat undoes grid."""
+    from types import SimpleNamespace
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    mg = object.__new__(GeometricMultigrid)
+    mg.torch, mg.device, mg.nodes = torch, torch.device("cpu"), (3, 2, 4)
+    mg.levels = [SimpleNamespace(nodes=(5, 3, 5))]
+    flat = np.random.default_rng(0).standard_normal((3 * 3 * 2 * 4, 2))
+    grid = mg.grid(flat)
+    assert tuple(grid.shape) == (2, 3, 5, 3, 5)
+    i, j, k, c, col = 2, 1, 3, 2, 1
+    assert grid[col, c, i, j, k].item() == flat[3 * ((i * 2 + j) * 4 + k) + c, col]
+    assert not grid[:, :, 3:].any() and not grid[:, :, :, 2:].any() and not grid[..., 4:].any()
+    assert np.array_equal(mg.flat(grid).numpy(), flat)
+    assert tuple(mg.grid(flat[:, 0]).shape) == (1, 3, 5, 3, 5)
