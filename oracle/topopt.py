@@ -19,14 +19,15 @@ from . import operator as op
 
 
 def continuation_decision(iterations, final_level, change, violation, minimum, maximum, change_tolerance, violation_tolerance):
-    violation_tolerance = 1e-3 if violation_tolerance is None else violation_tolerance
-    settled = change is not None and np.isfinite(change) and change < change_tolerance
-    feasible = np.isfinite(violation) and violation <= violation_tolerance
-    if iterations >= minimum and settled and feasible:
-        return "converged" if final_level else "advance"
-    if iterations >= maximum:
-        return "iteration_cap" if final_level or iterations < minimum else "advance"
-    return None
+    """Stopping rule of one continuation level (topology_optimization.py:17-25)."""
+    tolerance = 1e-3 if violation_tolerance is None else violation_tolerance
+    quiet = change is not None and bool(np.isfinite(change)) and change < change_tolerance
+    feasible = bool(np.isfinite(violation)) and violation <= tolerance
+    if quiet and feasible and iterations >= minimum:
+        return ("advance", "converged")[bool(final_level)]
+    if iterations < maximum:
+        return None
+    return "iteration_cap" if (final_level or iterations < minimum) else "advance"
 
 
 def solve_cases(shape, ke, young, active, cases, density, p, eps):
