@@ -17,7 +17,7 @@ COARSE = {"galerkin": 0, "rediscretize": 1}
 
 # every symbol include/tf_b200.h declares (checked by the CPU test suite)
 SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set_bc", "tf_prepare", "tf_precondition",
-           "tf_solve", "tf_solve_guess", "tf_apply", "tf_mass_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_timers", "tf_launch_count",
+           "tf_solve", "tf_solve_guess", "tf_apply", "tf_mass_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_combine", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
 SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_volume", "tf_oc_update",
             "tf_filter_destroy",
@@ -115,6 +115,7 @@ def load():
             "tf_mma_destroy": [P],
             "tf_mma_last_error": [P],
             "tf_simp": [P, I64, D, D, D, P, P, P, P, P],
+            "tf_combine": [P, I32, I64, P, I32, P, P],
             "tf_chol_create": [I64, ctypes.POINTER(P)],
             "tf_chol_factor_csr": [P, P, P, P, P],
             "tf_chol_solve": [P, P, I32, P, P],

@@ -57,6 +57,15 @@ __global__ void __launch_bounds__(256) gram_partial_kernel(const double* __restr
   }
 }
 
+// Count a launch and turn a launch error into TF_CUDA with the message tf_last_error(NULL) returns.
+int launch_status(const char* name) {
+  g_launch_count.fetch_add(1, std::memory_order_relaxed);
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return TF_OK;
+  record_unhandled_error(std::string(name) + ": " + cudaGetErrorString(e));
+  return TF_CUDA;
+}
+
 __global__ void gram_reduce_kernel(const double* __restrict__ partial, int pairs, int blocks, double* __restrict__ out) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < pairs; p += gridDim.x * blockDim.x) {
     double s = 0.0;
@@ -75,12 +84,10 @@ extern "C" int tf_gram(const double* a_dev, int32_t ra, const double* b_dev, int
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = static_cast<int>(std::min<long long>(GRAM_BLOCKS, (n + KC - 1) / KC));
   gram_partial_kernel<<<blocks, 256, 0, s>>>(a_dev, ra, b_dev, rb, n, scratch_dev);
-  g_launch_count.fetch_add(1, std::memory_order_relaxed);
-  if (cudaGetLastError() != cudaSuccess) return TF_CUDA;
+  int status = launch_status("tf_gram");
+  if (status != TF_OK) return status;
   gram_reduce_kernel<<<(ra * rb + 255) / 256, 256, 0, s>>>(scratch_dev, ra * rb, blocks, out_dev);
-  g_launch_count.fetch_add(1, std::memory_order_relaxed);
-  if (cudaGetLastError() != cudaSuccess) return TF_CUDA;
-  return TF_OK;
+  return launch_status("tf_gram");
 }
 
 namespace tfb {
@@ -89,21 +96,27 @@ std::atomic<long long> g_launch_count{0};
 
 namespace {
 // SIMP interpolation E = E0 (eps + (1 - eps) rho^p), dE/drho = E0 (1 - eps) p rho^(p-1), zero on
-// inactive cells (topology_optimization.py:657-661); one CTA also sums rho over the
-// active cells (the volume row of topology_problem.py:345) in a fixed order.
-__global__ void __launch_bounds__(1024) simp_kernel(const double* __restrict__ rho, long long n, double p, double eps, double young,
-                                                    const uint8_t* __restrict__ active, double* __restrict__ moduli,
-                                                    double* __restrict__ derivative, double* __restrict__ volume) {
-  __shared__ double sh[32];
-  double acc = 0.0;
-  for (long long c = threadIdx.x; c < n; c += blockDim.x) {
+// inactive cells (topology_optimization.py:657-661), one cell per thread over the whole grid.
+__global__ void __launch_bounds__(256) simp_kernel(const double* __restrict__ rho, long long n, double p, double eps, double young,
+                                                   const uint8_t* __restrict__ active, double* __restrict__ moduli,
+                                                   double* __restrict__ derivative) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     const double r = rho[c];
     const bool on = active ? active[c] != 0 : true;
     moduli[c] = on ? young * (eps + (1.0 - eps) * pow(r, p)) : 0.0;
     if (derivative) derivative[c] = on ? young * (1.0 - eps) * p * pow(r, p - 1.0) : 0.0;
-    if (on) acc += r;
   }
-  if (!volume) return;
+}
+
+// Sum of rho over the active cells (the volume row of topology_problem.py:345): one CTA, every
+// thread a fixed stride of cells, then a fixed tree, so the value is bitwise reproducible.  It only
+// streams rho and the flags (9 bytes per cell).
+__global__ void __launch_bounds__(1024) volume_kernel(const double* __restrict__ rho, long long n, const uint8_t* __restrict__ active,
+                                                      double* __restrict__ volume) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (long long c = threadIdx.x; c < n; c += blockDim.x)
+    if (!active || active[c]) acc += rho[c];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
@@ -114,6 +127,35 @@ __global__ void __launch_bounds__(1024) simp_kernel(const double* __restrict__ r
     *volume = t;
   }
 }
+
+// out[j][i] = sum_c coef[c * ncomb + j] * u[c][i]: combinations of solution columns (the partial
+// U v_i of the column-sharded lambda_max gradient).  HBM-bound: the columns are read once per
+// group of 16 combinations (L1 serves the repeats), the outputs written once.
+constexpr int COMBINE_MAX = 64;
+constexpr int COMBINE_GROUP = 16;
+__global__ void __launch_bounds__(256) combine_kernel(const double* __restrict__ u, int nrhs, long long n, const double* __restrict__ coef,
+                                                      int ncomb, double* __restrict__ out) {
+  __shared__ double c_s[COMBINE_MAX * COMBINE_MAX];
+  for (int t = threadIdx.x; t < nrhs * ncomb; t += blockDim.x) c_s[t] = coef[t];
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    for (int j0 = 0; j0 < ncomb; j0 += COMBINE_GROUP) {
+      double acc[COMBINE_GROUP];
+#pragma unroll
+      for (int q = 0; q < COMBINE_GROUP; ++q) acc[q] = 0.0;
+      for (int c = 0; c < nrhs; ++c) {
+        const double v = u[(long long)c * n + i];
+#pragma unroll
+        for (int q = 0; q < COMBINE_GROUP; ++q)
+          if (j0 + q < ncomb) acc[q] += c_s[c * ncomb + j0 + q] * v;
+      }
+#pragma unroll
+      for (int q = 0; q < COMBINE_GROUP; ++q)
+        if (j0 + q < ncomb) out[(long long)(j0 + q) * n + i] = acc[q];
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" int tf_simp(const double* rho_dev, int64_t n, double penalization, double min_stiffness_ratio, double young,
@@ -123,10 +165,23 @@ extern "C" int tf_simp(const double* rho_dev, int64_t n, double penalization, do
     record_unhandled_error("tf_simp: invalid arguments");
     return TF_INVALID;
   }
-  simp_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(rho_dev, n, penalization, min_stiffness_ratio, young, active_dev,
-                                                                  moduli_dev, derivative_dev, volume_dev);
-  g_launch_count.fetch_add(1, std::memory_order_relaxed);
-  return cudaGetLastError() == cudaSuccess ? TF_OK : TF_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  simp_kernel<<<grid_for(n, 256), 256, 0, s>>>(rho_dev, n, penalization, min_stiffness_ratio, young, active_dev, moduli_dev,
+                                               derivative_dev);
+  int status = launch_status("tf_simp");
+  if (status != TF_OK || !volume_dev) return status;
+  volume_kernel<<<1, 1024, 0, s>>>(rho_dev, n, active_dev, volume_dev);
+  return launch_status("tf_simp");
+}
+
+extern "C" int tf_combine(const double* u_dev, int32_t nrhs, int64_t n, const double* coef_dev, int32_t ncomb, double* out_dev,
+                          void* stream) {
+  if (nrhs < 1 || ncomb < 1 || nrhs > COMBINE_MAX || ncomb > COMBINE_MAX || n < 1 || !u_dev || !coef_dev || !out_dev) {
+    record_unhandled_error("tf_combine: need 1 <= nrhs, ncomb <= 64, n >= 1 and non-NULL pointers");
+    return TF_INVALID;
+  }
+  combine_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(u_dev, nrhs, n, coef_dev, ncomb, out_dev);
+  return launch_status("tf_combine");
 }
 
 extern "C" int64_t tf_launch_count(void) { return g_launch_count.load(); }
@@ -198,10 +253,8 @@ extern "C" int tf_gram_static(const double* a_dev, int32_t ra, const double* b_d
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = static_cast<int>(std::min<long long>(GRAM_BLOCKS, (n + KC - 1) / KC));
   gram_partial_kernel<<<blocks, 256, 0, s>>>(a_dev, ra, b_dev, rb, n, scratch);
-  g_launch_count.fetch_add(1, std::memory_order_relaxed);
-  if (cudaGetLastError() != cudaSuccess) return TF_CUDA;
+  int status = launch_status("tf_gram_static");
+  if (status != TF_OK) return status;
   gram_reduce_kernel<<<(ra * rb + 255) / 256, 256, 0, s>>>(scratch, ra * rb, blocks, out_dev);
-  g_launch_count.fetch_add(1, std::memory_order_relaxed);
-  if (cudaGetLastError() != cudaSuccess) return TF_CUDA;
-  return TF_OK;
+  return launch_status("tf_gram_static");
 }

@@ -18,6 +18,8 @@ doubles.  Every rank takes the same collective steps in the same order.
 """
 import numpy as np
 
+from .covariance import Spectrum
+
 
 class ShardedMeasure:
     def __init__(self, groups, rank_count, factor, ops, group=None, ks=50.0, ks_cutoff=1e-9):
@@ -55,36 +57,31 @@ class ShardedMeasure:
                 loc = torch.as_tensor(g["local_ks"], device=device)
                 flex[idx[:, None], loc[None, :]] += self.factor * block
         self._all_reduce(flex)
-        host = flex.cpu().numpy()
-        host = (host + host.T) / 2
-        mean = float(np.trace(host))
-        values, vectors = np.linalg.eigh(host)
-        values, vectors = values[::-1], vectors[:, ::-1]
-        worst = float(values[0])
-        weights = np.exp(self.ks * (values - worst) / worst)
-        ks_value = worst + worst * np.log(weights.sum()) / self.ks
-        weights /= weights.sum()
+        spectrum = Spectrum(flex.cpu().numpy(), self.ks)
         nelem = scale.numel()
         grad_mean = torch.zeros(nelem, dtype=torch.float64, device=device)
         for g, u in zip(self.groups, solved):
             if u is not None:
                 grad_mean += self.ops.energy(u, np.full(len(g["local"]), self.factor), scale)
         self._all_reduce(grad_mean)
-        keep = np.flatnonzero(weights > self.ks_cutoff)
+        kept = spectrum.kept(self.ks_cutoff)
+        coefficients = spectrum.weights[kept] * self.factor
         grad_worst = torch.zeros(nelem, dtype=torch.float64, device=device)
         for g, u in zip(self.groups, solved):
-            ndof = g["forces"].shape[1]
-            comb = np.zeros((len(g["local"]), len(keep)))
-            if u is not None:
-                comb = vectors[np.ix_(g["local_ks"], keep)]
-                w = torch.as_tensor(comb.T, dtype=torch.float64, device=device) @ u      # [keep, ndof] partial sums
-            else:
-                w = torch.zeros((len(keep), ndof), dtype=torch.float64, device=device)
-            self._all_reduce(w)
-            grad_worst += self.ops.energy(w.contiguous(), weights[keep] * self.factor, scale)
-        rows = [{"name": "load_mean", "value": mean, "gradient": grad_mean},
-                {"name": "load_worst", "value": worst, "gradient": grad_worst, "info": {"ks_n_mm": float(ks_value), "eigenvalues_n_mm": values[:6].tolist()}}]
-        return rows, host
+            mixing = spectrum.vectors[np.ix_(g["local_ks"], kept)]
+            if self.world == 1:
+                # every direction is local: the energy kernel forms the combinations U v_i itself
+                grad_worst += self.ops.energy(u, coefficients, scale, combination=mixing)
+                continue
+            # partial combinations of this rank's columns, completed by one all-reduce of [kept, ndof]
+            partial = (self.ops.combine(u, mixing) if u is not None else
+                       torch.zeros((len(kept), g["forces"].shape[1]), dtype=torch.float64, device=device))
+            self._all_reduce(partial)
+            grad_worst += self.ops.energy(partial, coefficients, scale)
+        rows = [{"name": "load_mean", "value": spectrum.trace, "gradient": grad_mean},
+                {"name": "load_worst", "value": spectrum.top, "gradient": grad_worst,
+                 "info": {"ks_n_mm": spectrum.ks, "eigenvalues_n_mm": spectrum.values[:6].tolist()}}]
+        return rows, spectrum.matrix
 
 
 class DeviceOps:
@@ -108,5 +105,18 @@ class DeviceOps:
                                mg._stream()), None, "tf_gram")
         return out
 
-    def energy(self, columns, coefficients, scale):
-        return self.system._multigrid().energy_device(columns, coefficients=coefficients, scale=scale)
+    def energy(self, columns, coefficients, scale, combination=None):
+        return self.system._multigrid().energy_device(columns, combination=combination, coefficients=coefficients, scale=scale)
+
+    def combine(self, columns, mixing):
+        """[k, ndof] = mixing^T columns, on the device (tf_combine)."""
+        import torch
+        from . import _lib
+        lib = _lib.load()
+        mg = self.system._multigrid()
+        m, n = columns.shape
+        k = mixing.shape[1]
+        coef = torch.as_tensor(np.ascontiguousarray(mixing), dtype=torch.float64, device=columns.device)
+        out = torch.empty((k, n), dtype=torch.float64, device=columns.device)
+        _lib.check(lib.tf_combine(_lib.ptr(columns), m, n, _lib.ptr(coef), k, _lib.ptr(out), mg._stream()), None, "tf_combine")
+        return out

@@ -176,9 +176,19 @@ TF_API int64_t tf_gram_scratch_size(int32_t ra, int32_t rb);
  * TF_STATUS_INVALID with a message in tf_last_error(NULL).  The first call on a device
  * resolves the array's device address and should come before any stream capture.  All
  * calls share the array: calls that overlap on the GPU race and must be ordered by the
- * caller.  Allocates nothing. */
+ * caller.  The cached address belongs to the device's primary context (the one the CUDA runtime
+ * uses): a caller that makes another driver-API context current, or resets the device, must not
+ * call it afterwards in the same process.  Allocates nothing. */
 TF_API int tf_gram_static(const double* a_dev, int32_t ra, const double* b_dev, int32_t rb, int64_t n, double* out_dev,
                           void* stream);
+
+/* out[j][i] = sum_c coef[c * ncomb + j] * u[c][i] for column blocks u [nrhs][n] and out [ncomb][n]
+ * (device FP64, 1 <= nrhs, ncomb <= 64; coef is a device [nrhs][ncomb] array): the combinations
+ * U v of solution columns that the lambda_max sensitivity of InterfaceCovariance.measure needs
+ * (deep_frame/topology_problem.py:647-652, 680-683), formed per rank before the all-reduce when the
+ * columns are sharded over GPUs. */
+TF_API int tf_combine(const double* u_dev, int32_t nrhs, int64_t n, const double* coef_dev, int32_t ncomb, double* out_dev,
+                      void* stream);
 
 /* SIMP interpolation (HexElasticity.solve, deep_frame/topology_optimization.py:657-661):
  * moduli = young (eps + (1 - eps) rho^p), derivative = young (1 - eps) p rho^(p-1), both zero

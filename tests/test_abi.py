@@ -72,6 +72,7 @@ def test_handleless_failures_carry_a_message(library):
     assert lib.tf_gram(None, -1, None, 2, 10, None, None, None) == 1 and lib.tf_last_error(None).startswith(b"tf_gram:")
     assert lib.tf_simp(None, 10, 3.0, 1e-9, 1.0, None, None, None, None, None) == 1
     assert lib.tf_last_error(None).startswith(b"tf_simp:")
+    assert lib.tf_combine(None, 3, 10, None, 65, None, None) == 1 and lib.tf_last_error(None).startswith(b"tf_combine:")
 
 
 @pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the path of a host without a CUDA device")

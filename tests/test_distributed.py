@@ -51,11 +51,18 @@ class OracleOps:
     def gram(self, p_all, u_local):
         return p_all @ u_local.T
 
-    def energy(self, columns, coefficients, scale):
+    def energy(self, columns, coefficients, scale, combination=None):
         import torch
+        if combination is not None:
+            columns = torch.as_tensor(np.asarray(combination).T) @ columns
         e = self.op.element_energy(self.shape, self.system.ke, columns.numpy().T)
         e = e.reshape(len(coefficients), -1) if e.ndim == 2 else e[None]
         return torch.as_tensor(scale.numpy() * (np.asarray(coefficients) @ e))
+
+
+    def combine(self, columns, mixing):
+        import torch
+        return torch.as_tensor(np.asarray(mixing).T) @ columns
 
 
 def _groups(model):
@@ -86,8 +93,9 @@ def _worker(rank, world, port, out):
         dist.destroy_process_group()
 
 
-def test_sharded_measure_matches_single_process_oracle():
+def _oracle_reference():
     from oracle import covariance as ocov
+    import torch
     shape, system, model, density = _problem()
     moduli, derivative = system.moduli(density, 3.0, 1e-9)
     ops = OracleOps(shape, system, moduli)
@@ -97,10 +105,30 @@ def test_sharded_measure_matches_single_process_oracle():
         forces = np.zeros((system.ndof, model.rank))
         for case, part in members:
             forces[:, index[case["name"]]] = part["force"]
-        import torch
         u = ops.solve(key, torch.as_tensor(forces.T.copy())).numpy().T
         parts.append((forces, u))
-    ref = ocov.measure(parts, model.factor, shape, system.ke, derivative)
+    return ocov.measure(parts, model.factor, shape, system.ke, derivative)
+
+
+def test_unsharded_measure_forms_combinations_in_the_energy_call():
+    """One process (no process group): every direction is local, so the lambda_max gradient passes
+    the eigenvector combinations to the energy call instead of forming U v first."""
+    import torch
+    from deep_frame_b200.distributed import ShardedMeasure
+    ref = _oracle_reference()
+    shape, system, model, density = _problem()
+    moduli, derivative = system.moduli(density, 3.0, 1e-9)
+    ops = OracleOps(shape, system, moduli)
+    ops.combine = lambda *a: pytest.fail("one process must not form partial combinations")
+    rows, _ = ShardedMeasure(_groups(model), model.rank, model.factor, ops).measure(torch.as_tensor(-derivative))
+    assert rows[0]["value"] == pytest.approx(ref["load_mean"], rel=1e-12)
+    assert rows[1]["value"] == pytest.approx(ref["load_worst"], rel=1e-12)
+    assert rows[1]["info"]["ks_n_mm"] == pytest.approx(ref["ks"], rel=1e-12)
+    assert np.linalg.norm(rows[1]["gradient"].numpy() - ref["grad_worst"]) < 1e-10 * np.linalg.norm(ref["grad_worst"])
+
+
+def test_sharded_measure_matches_single_process_oracle():
+    ref = _oracle_reference()
     world, port = 2, _free_port()
     manager = mp.get_context("spawn").Manager()
     out = manager.dict()

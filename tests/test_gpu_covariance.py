@@ -66,6 +66,22 @@ def test_gram_is_reproducible_and_exact(cuda):
     assert np.max(np.abs(results[0] - expected)) < 1e-9 * np.max(np.abs(expected))
 
 
+def test_combine_matches_host_product(cuda):
+    """tf_combine (the per-rank partial U v of the sharded lambda_max gradient) equals the host
+    product mixing^T U to FP64 rounding, for more combinations than one 16-wide group."""
+    import torch
+    from deep_frame_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(1)
+    u = rng.normal(size=(21, 50021))
+    mixing = rng.normal(size=(21, 19))
+    out = torch.empty((19, 50021), dtype=torch.float64, device=cuda)
+    u_dev, mixing_dev = torch.as_tensor(u, device=cuda), torch.as_tensor(mixing, device=cuda)
+    _lib.check(lib.tf_combine(_lib.ptr(u_dev), 21, 50021, _lib.ptr(mixing_dev), 19, _lib.ptr(out), None))
+    expected = mixing.T @ u
+    assert np.max(np.abs(out.cpu().numpy() - expected)) < 1e-12 * np.max(np.abs(expected))
+
+
 @pytest.mark.parametrize("precision", ["float32", "float64"])
 def test_benchmark_plate_matches_fp64_oracle(cuda, precision):
     """The benchmark workload itself (96 x 96 x 16 plate, seed 0, 2 x 42 columns solved to the
