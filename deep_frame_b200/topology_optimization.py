@@ -197,169 +197,249 @@ def _history_entry(iteration, physical_sum, solutions, scales, change, elapsed, 
             "elapsed_s": elapsed}
 
 
-def _stage_entry(mapping, sums, volume_target, move_limit):
-    entry = {"projection_beta": mapping.beta, "move_limit": move_limit}
-    if mapping.robust:
-        entry.update({"dilated_volume_target": volume_target, "eroded_density_sum": sums["eroded"],
-                      "dilated_density_sum": sums["dilated"]})
-    return entry
+class _Levels:
+    """The projection continuation of an OC run.
+
+    Holds the beta schedule and the current level, the iterations spent at that level, and, for
+    robust runs, the dilated-volume target that relaxes toward the budget scaled by the
+    dilated / intermediate volume ratio (topology_optimization.py:1296-1300).  ``rule`` gives the
+    arguments of ``continuation_decision`` that end the current level: the final level runs to
+    the change tolerance with the run's minimum iterations; earlier levels advance after
+    beta_minimum_iterations with the beta change tolerance, or at beta_interval."""
+
+    def __init__(self, settings, mapping, budget):
+        self.settings, self.mapping, self.budget = settings, mapping, budget
+        self.schedule = settings["beta_schedule"] or [mapping.beta]
+        self.staged = mapping.robust or settings["beta_schedule"] is not None
+        self.level, self.count, self.volume_target = 0, 0, budget
+        self.minimum = (max(settings["minimum_iterations"], settings["beta_minimum_iterations"]) if self.staged
+                        else settings["minimum_iterations"])
+
+    @property
+    def final(self):
+        return self.level == len(self.schedule) - 1
+
+    def relax(self, dilated, intermediate):
+        anchor = dilated if self.count == 0 else self.volume_target
+        self.volume_target = anchor + self.settings["volume_target_relaxation"] * (self.budget * dilated / intermediate - anchor)
+
+    def move_limit(self):
+        late = self.settings["move_limit_late"]
+        return late if late is not None and self.mapping.beta >= self.settings["move_limit_late_beta"] else self.settings["move_limit"]
+
+    def rule(self):
+        if self.final:
+            return self.minimum, float("inf"), self.settings["change_tolerance"]
+        return self.settings["beta_minimum_iterations"], self.settings["beta_interval"], self.settings["beta_change_tolerance"]
+
+    def stall(self, objectives):
+        """Relative spread of the objective over the last objective_window iterations of this level,
+        or None before the window is full."""
+        window = objectives[-min(self.count + 1, self.settings["objective_window"]):]
+        if len(window) < self.settings["objective_window"]:
+            return None
+        return (max(window) - min(window)) / min(window)
+
+    def record(self, sums, move_limit):
+        entry = {"projection_beta": self.mapping.beta, "move_limit": move_limit}
+        if self.mapping.robust:
+            entry.update(dilated_volume_target=self.volume_target, eroded_density_sum=sums["eroded"], dilated_density_sum=sums["dilated"])
+        return entry
+
+    def advance(self):
+        self.level += 1
+        self.count = 0
+        self.mapping.beta = self.schedule[self.level]
 
 
-def _sums(torch, fields):
-    return {name: float(torch.sum(value)) for name, (value, _) in fields.items()}
+class _OcRun:
+    """State of one device-resident OC run: the density map and elasticity system, the design on the
+    device, the case scaling fixed by the first evaluation, and the history."""
 
-
-def optimize_topology(domain, settings, *, progress_callback=None, device="cuda"):
-    """The reference's OC driver; returns the same outcome dict (status ok / invalid / failed)."""
-    started = perf_counter()
-    history, diagnostics = [], []
-    system = mapping = outcome = None
-    density = np.zeros(tuple(domain.get("grid", {}).get("shape", (0, 0, 0))))
-    try:
+    def __init__(self, settings, started, shape):
         import torch
-        settings = _settings(settings)
+        self.torch, self.settings, self.started = torch, settings, started
+        self.mapping = self.system = None
+        self.history, self.shape, self.density = [], shape, np.zeros(shape)
+
+    def start(self, domain, device):
+        """Masks, density map, volume budget, initial design and the elasticity system."""
+        settings = self.settings
         validate_masks(domain)
         # the reference's HexElasticity refuses a domain without a static case (topology_optimization.py:440-441);
         # this library's HexElasticity accepts one (a covariance-only plate), so the OC driver checks it here
         if not any(case.get("analysis") == "static" for case in domain.get("load_cases", [])):
             raise ValueError("Topology optimization requires at least one static case")
-        mapping = DensityMap(domain, settings, device)
-        grid_shape = tuple(domain["grid"]["shape"])
-        target = settings["volume_fraction"] * int(np.count_nonzero(mapping.allowed))
-        if np.count_nonzero(mapping.preserve) >= target:
+        self.mapping = DensityMap(domain, settings, device)
+        self.allowed_cells = int(np.count_nonzero(self.mapping.allowed))
+        budget = settings["volume_fraction"] * self.allowed_cells
+        if np.count_nonzero(self.mapping.preserve) >= budget:
             raise ValueError("The volume budget must exceed the preserve-cell volume")
-        design = mapping._dev(mapping.initial(target))
-        system = HexElasticity(domain, interface_node_policy=settings["interface_node_policy"], linear_solver=settings["linear_solver"],
-                               solver_choice=settings["solver_choice"], gpu_solver_residency=settings["gpu_solver_residency"],
-                               multigrid={"device": str(mapping.device)})
-        weights = torch.ones(mapping.n, dtype=torch.float64, device=mapping.device)
-        scales = normalization = case_weights = None
-        converged, stop_reason = False, "max_iterations"
-        schedule = settings["beta_schedule"] or [mapping.beta]
-        staged = mapping.robust or settings["beta_schedule"] is not None
-        stiffness_name, volume_name = ("eroded", "dilated") if mapping.robust else ("intermediate", "intermediate")
-        minimum_iterations = max(settings["minimum_iterations"], settings["beta_minimum_iterations"]) if staged else settings["minimum_iterations"]
-        level = level_iterations = 0
-        volume_target = target
+        self.levels = _Levels(settings, self.mapping, budget)
+        self.stiffness_field, self.volume_field = ("eroded", "dilated") if self.mapping.robust else ("intermediate", "intermediate")
+        self.design = self.mapping._dev(self.mapping.initial(budget))
+        self.system = HexElasticity(domain, interface_node_policy=settings["interface_node_policy"], linear_solver=settings["linear_solver"],
+                                    solver_choice=settings["solver_choice"], gpu_solver_residency=settings["gpu_solver_residency"],
+                                    multigrid={"device": str(self.mapping.device)})
+        self.unit = self.torch.ones(self.mapping.n, dtype=self.torch.float64, device=self.mapping.device)
+        self.scales = self.normalization = self.shares = None
+
+    def evaluate(self, design):
+        """Density fields of ``design`` (with the filtered field) and their sums; keeps the physical
+        density on the host for the outcome."""
+        fields, filtered = self.mapping.fields_device(design)
+        sums = {name: float(self.torch.sum(value)) for name, (value, _) in fields.items()}
+        self.density = fields["intermediate"][0].cpu().numpy().reshape(self.shape)
+        return fields, filtered, sums
+
+    def solve(self, fields, metrics=False):
+        return self.system.solve(fields[self.stiffness_field][0].cpu().numpy(), self.settings["penalization"],
+                                 self.settings["min_stiffness_ratio"], metrics=metrics)
+
+    def entry(self, iteration, sums, solutions, change, final=False):
+        self.history.append(_history_entry(iteration, sums["intermediate"], solutions, self.scales, change,
+                                           perf_counter() - self.started, final=final))
+        return self.history[-1]
+
+    def step(self, iteration):
+        """One OC iteration: evaluate, scale, pull the gradients back through the filter, run the
+        device multiplier search.  Returns (candidate design, history entry, design change, volume
+        violation)."""
+        levels, mapping = self.levels, self.mapping
+        fields, _, sums = self.evaluate(self.design)
+        if mapping.robust:
+            levels.relax(sums[self.volume_field], sums["intermediate"])
+        solutions = self.solve(fields)
+        if self.scales is None:
+            self.scales, self.normalization, self.shares = _case_scaling(solutions, self.settings)
+        objective_gradient = mapping._dev(sum(self.scales[name] * result["derivative"] for name, result in solutions.items()))
+        move_limit = levels.move_limit()
+        candidate, _ = mapping.oc_update_device(self.design, mapping.pullback_device(objective_gradient, fields[self.stiffness_field][1]),
+                                                mapping.pullback_device(self.unit, fields[self.volume_field][1]),
+                                                levels.volume_target, move_limit)
+        change = float(self.torch.max(self.torch.abs(candidate - self.design)))
+        entry = self.entry(iteration, sums, solutions, change)
+        entry.update(modal_penalty=0.0, f1_hz=None)
+        if levels.staged:
+            entry.update(levels.record(sums, move_limit), objective_stall=levels.stall([item["objective"] for item in self.history]))
+        levels.count += 1
+        violation = float(self.torch.dot(self.unit, fields[self.volume_field][0])) / levels.volume_target - 1
+        entry["max_violation"] = violation
+        return candidate, entry, change, violation
+
+    def iterate(self, callback):
+        """Iterations until a level rule converges, the runtime or iteration cap is hit.  Returns
+        (iterations run, converged, stop reason)."""
+        settings, levels = self.settings, self.levels
         iteration = 0
         for iteration in range(1, settings["max_iterations"] + 1):
-            fields, _ = mapping.fields_device(design)
-            sums = _sums(torch, fields)
-            physical_sum = sums["intermediate"]
-            density = fields["intermediate"][0].cpu().numpy().reshape(grid_shape)
-            if mapping.robust:
-                dilated = sums[volume_name]
-                reference = dilated if level_iterations == 0 else volume_target
-                volume_target = reference + settings["volume_target_relaxation"] * (target * dilated / physical_sum - reference)
-            solutions = system.solve(fields[stiffness_name][0].cpu().numpy(), settings["penalization"], settings["min_stiffness_ratio"])
-            if scales is None:
-                scales, normalization, case_weights = _case_scaling(solutions, settings)
-            physical_gradient = sum(scales[name] * result["derivative"] for name, result in solutions.items())
-            gradient = mapping.pullback_device(mapping._dev(physical_gradient), fields[stiffness_name][1])
-            volume_gradient = mapping.pullback_device(weights, fields[volume_name][1])
-            late = settings["move_limit_late"] is not None and mapping.beta >= settings["move_limit_late_beta"]
-            move_limit = settings["move_limit_late"] if late else settings["move_limit"]
-            candidate, _ = mapping.oc_update_device(design, gradient, volume_gradient, volume_target, move_limit)
-            change = float(torch.max(torch.abs(candidate - design)))
-            history.append(_history_entry(iteration, physical_sum, solutions, scales, change, perf_counter() - started))
-            history[-1].update(modal_penalty=0.0, f1_hz=None)
-            if staged:
-                recent = [entry["objective"] for entry in history[-min(level_iterations + 1, settings["objective_window"]):]]
-                stall = (max(recent) - min(recent)) / min(recent) if len(recent) == settings["objective_window"] else None
-                history[-1].update(_stage_entry(mapping, sums, volume_target, move_limit), objective_stall=stall)
-            level_iterations += 1
-            final_level = level == len(schedule) - 1
-            violation = float(torch.dot(weights, fields[volume_name][0])) / volume_target - 1
-            history[-1]["max_violation"] = violation
-            if progress_callback is not None:
-                progress_callback(deepcopy(history[-1]))
-            decision = continuation_decision(level_iterations, final_level, change, violation,
-                                             minimum_iterations if final_level else settings["beta_minimum_iterations"],
-                                             float("inf") if final_level else settings["beta_interval"],
-                                             settings["change_tolerance"] if final_level else settings["beta_change_tolerance"],
+            candidate, entry, change, violation = self.step(iteration)
+            if callback is not None:
+                callback(deepcopy(entry))
+            minimum, maximum, tolerance = levels.rule()
+            decision = continuation_decision(levels.count, levels.final, change, violation, minimum, maximum, tolerance,
                                              settings["feasibility_tolerance"])
             if decision == "converged":
-                converged, stop_reason = True, "change_tolerance"
-                break
-            if settings["max_runtime_s"] is not None and perf_counter() - started >= settings["max_runtime_s"]:
-                stop_reason = "max_runtime_s"
-                break
+                return iteration, True, "change_tolerance"
+            if settings["max_runtime_s"] is not None and perf_counter() - self.started >= settings["max_runtime_s"]:
+                return iteration, False, "max_runtime_s"
             if iteration == settings["max_iterations"]:
                 break
-            design = candidate
+            self.design = candidate
             if decision == "advance":
-                level += 1
-                level_iterations = 0
-                mapping.beta = schedule[level]
-        fields, filtered = mapping.fields_device(design)
-        sums = _sums(torch, fields)
+                levels.advance()
+        return iteration, False, "max_iterations"
+
+    def finish(self, iterations, converged, stop_reason, callback):
+        """The final evaluation (with metrics) and the reference's outcome record."""
+        fields, filtered, sums = self.evaluate(self.design)
+        solutions = self.solve(fields, metrics=True)
+        final = self.entry(iterations + 1, sums, solutions, None, final=True)
+        if self.levels.staged:
+            final.update(self.levels.record(sums, None))
+        if callback is not None:
+            callback(deepcopy(final))
         physical = fields["intermediate"][0].cpu().numpy()
-        density = physical.reshape(grid_shape)
-        solutions = system.solve(fields[stiffness_name][0].cpu().numpy(), settings["penalization"], settings["min_stiffness_ratio"], metrics=True)
-        final_entry = _history_entry(iteration + 1, sums["intermediate"], solutions, scales, None, perf_counter() - started, final=True)
-        if staged:
-            final_entry.update(_stage_entry(mapping, sums, volume_target, None))
-        history.append(final_entry)
-        if progress_callback is not None:
-            progress_callback(deepcopy(final_entry))
-        volume = float(np.sum(physical) * np.prod(system.spacing))
-        allowed = int(np.count_nonzero(mapping.allowed))
-        summary = {
+        outcome = {"status": "ok", "density": self.density.copy(), "design_density": self.design.cpu().numpy().reshape(self.shape),
+                   "summary": self.summary(physical, solutions, final, iterations, converged, stop_reason), "history": self.history,
+                   "diagnostics": []}
+        if self.mapping.robust:
+            self._robust(outcome, fields, filtered)
+        if not converged:
+            outcome["diagnostics"].append(f"Density iteration stopped at {stop_reason}; convergence is not claimed")
+        return outcome
+
+    def summary(self, physical, solutions, final, iterations, converged, stop_reason):
+        settings, system, levels = self.settings, self.system, self.levels
+        cell_volume = float(np.prod(system.spacing))
+        volume = float(np.sum(physical)) * cell_volume
+        free = physical[self.mapping.free]
+        out = {
             "method": "3D Hex8 SIMP, spatial density filter, smooth projection, normalized multi-load compliance, OC volume constraint",
             "initialization": "uniform in every free cell; fixed preserves",
-            "settings": settings,
-            "converged": converged,
-            "stop_reason": stop_reason,
-            "iterations": iteration,
-            "volume_fraction": float(np.sum(physical) / allowed),
-            "target_volume_fraction": settings["volume_fraction"],
-            "density_volume_mm3": volume,
-            "density_frame_mass_g": volume * system.density / 1000,
-            "objective_initial": history[0]["objective"],
-            "objective_final": final_entry["objective"],
-            "normalization_compliances_n_mm": normalization,
-            "normalized_case_weights": case_weights,
+            "settings": settings, "converged": converged, "stop_reason": stop_reason, "iterations": iterations,
+            "volume_fraction": float(np.sum(physical) / self.allowed_cells), "target_volume_fraction": settings["volume_fraction"],
+            "density_volume_mm3": volume, "density_frame_mass_g": volume * system.density / 1000,
+            "objective_initial": self.history[0]["objective"], "objective_final": final["objective"],
+            "normalization_compliances_n_mm": self.normalization, "normalized_case_weights": self.shares,
             "static_surrogate_metrics": {name: {key: value for key, value in result.items() if key not in ("derivative", "fields", "modulus_derivative")}
                                          for name, result in solutions.items()},
-            "gray_fraction_free": float(np.mean((physical[mapping.free] > 0.1) & (physical[mapping.free] < 0.9))),
+            "gray_fraction_free": float(np.mean((free > 0.1) & (free < 0.9))),
             "modal": None,
             "element_model": "three displacement DOFs/node, fully integrated trilinear 8-node 3D elasticity, 2x2x2 Gauss integration",
             "units": {"length": "mm", "force": "N", "stress": "MPa", "density": "g/cm3"},
-            "system": system.diagnostics(),
-            "elapsed_s": perf_counter() - started,
+            "system": system.diagnostics(), "elapsed_s": perf_counter() - self.started,
         }
-        if staged:
-            summary["continuation"] = {"beta_schedule": schedule, "beta_final": mapping.beta, "final_level_reached": level == len(schedule) - 1,
-                                       "level_iterations_final": level_iterations}
-        host_design = design.cpu().numpy().reshape(grid_shape)
-        outcome = {"status": "ok", "density": density.copy(), "design_density": host_design, "summary": summary, "history": history,
-                   "diagnostics": diagnostics}
-        if mapping.robust:
-            eroded, dilated = (fields[name][0].cpu().numpy() for name in ("eroded", "dilated"))
-            summary["method"] = ("3D Hex8 SIMP, spatial density filter, robust eroded/intermediate/dilated Heaviside projection with beta "
-                                 "continuation, eroded-design normalized multi-load compliance, OC dilated-volume constraint")
-            summary["robust"] = {"thresholds": mapping.thresholds, "objective_field": "eroded", "volume_constraint_field": "dilated",
-                                 "reported_density_field": "intermediate", "dilated_volume_target_final": volume_target,
-                                 "eroded_volume_fraction": float(np.sum(eroded) / allowed),
-                                 "dilated_volume_fraction": float(np.sum(dilated) / allowed),
-                                 "dilated_frame_mass_g": float(np.sum(dilated) * np.prod(system.spacing) * system.density / 1000)}
-            outcome["eroded_density"] = eroded.reshape(grid_shape)
-            outcome["dilated_density"] = dilated.reshape(grid_shape)
-            outcome["filtered_density"] = filtered.cpu().numpy().reshape(grid_shape)
-        if not converged:
-            diagnostics.append(f"Density iteration stopped at {stop_reason}; convergence is not claimed")
-        return outcome
-    except ValueError as error:
-        outcome = {"status": "invalid", "density": density, "summary": {}, "history": history, "diagnostics": [str(error)]}
-        return outcome
-    except (RuntimeError, MemoryError, np.linalg.LinAlgError) as error:
-        outcome = {"status": "failed", "density": density, "summary": {}, "history": history, "diagnostics": [str(error)]}
-        return outcome
+        if levels.staged:
+            out["continuation"] = {"beta_schedule": levels.schedule, "beta_final": self.mapping.beta, "final_level_reached": levels.final,
+                                   "level_iterations_final": levels.count}
+        return out
+
+    def _robust(self, outcome, fields, filtered):
+        """Robust runs also report the eroded / dilated / filtered fields and their volumes."""
+        eroded, dilated = (fields[name][0].cpu().numpy() for name in ("eroded", "dilated"))
+        mass_scale = float(np.prod(self.system.spacing)) * self.system.density / 1000
+        summary = outcome["summary"]
+        summary["method"] = ("3D Hex8 SIMP, spatial density filter, robust eroded/intermediate/dilated Heaviside projection with beta "
+                             "continuation, eroded-design normalized multi-load compliance, OC dilated-volume constraint")
+        summary["robust"] = {"thresholds": self.mapping.thresholds, "objective_field": "eroded", "volume_constraint_field": "dilated",
+                             "reported_density_field": "intermediate", "dilated_volume_target_final": self.levels.volume_target,
+                             "eroded_volume_fraction": float(np.sum(eroded) / self.allowed_cells),
+                             "dilated_volume_fraction": float(np.sum(dilated) / self.allowed_cells),
+                             "dilated_frame_mass_g": float(np.sum(dilated)) * mass_scale}
+        outcome["eroded_density"] = eroded.reshape(self.shape)
+        outcome["dilated_density"] = dilated.reshape(self.shape)
+        outcome["filtered_density"] = filtered.cpu().numpy().reshape(self.shape)
+
+    def close(self):
+        """Release the system, then the density map; the system's cleanup errors are returned."""
+        errors = self.system.close() if self.system is not None else []
+        if self.mapping is not None:
+            self.mapping.close()
+        return errors
+
+
+def optimize_topology(domain, settings, *, progress_callback=None, device="cuda"):
+    """The reference's OC driver (topology_optimization.py:1265-1406); returns the same outcome dict:
+    status "ok", "invalid" (a ValueError: bad settings, masks or domain) or "failed" (a runtime,
+    memory or linear-algebra error), with cleanup errors appended to the diagnostics and turning
+    the status to "failed"."""
+    started = perf_counter()
+    run, outcome = None, None
+    shape = tuple(domain.get("grid", {}).get("shape", (0, 0, 0)))
+    try:
+        run = _OcRun(_settings(settings), started, shape)
+        run.start(domain, device)
+        iterations, converged, stop_reason = run.iterate(progress_callback)
+        outcome = run.finish(iterations, converged, stop_reason, progress_callback)
+    except (ValueError, RuntimeError, MemoryError, np.linalg.LinAlgError) as error:
+        status = "invalid" if isinstance(error, ValueError) else "failed"
+        density, history = (run.density, run.history) if run is not None else (np.zeros(shape), [])
+        outcome = {"status": status, "density": density, "summary": {}, "history": history, "diagnostics": [str(error)]}
     finally:
-        if system is not None:
-            cleanup = system.close()
+        if run is not None:
+            cleanup = run.close()
             if cleanup and outcome is not None:
                 outcome["diagnostics"].extend(cleanup)
                 outcome["status"] = "failed"
-        if mapping is not None:
-            mapping.close()
+    return outcome
