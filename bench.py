@@ -1,20 +1,23 @@
-"""Benchmark: seconds per 42-RHS covariance hex8 solve to 1e-8 relative residual.
+"""Benchmark: seconds per 42-RHS covariance hex8 solve to 1e-8 relative residual, fast path vs plain FP64.
 
-One step = one design evaluation of the covariance-load plate half model
-(96 x 96 x 16 voxels, 479 859 dofs, mirror symmetry on x = 0): new element
-moduli, both multigrid hierarchies rebuilt (symmetric and antisymmetric
-fixture groups), the 42 load directions of each half solved by batched FP64
-GMG-PCG to a recomputed true relative residual below 1e-8 (84 column solves),
-then F = P^T U, tr(K^-1 Sigma), lambda_max and both sensitivity fields.
-``value`` times this with every input resident in HBM; ``e2e`` times the same
-step from host densities to host results, and ``e2e_solve_api`` the solves
-alone through ``GeometricMultigrid.update`` / ``.solve`` with host NumPy
-forces in and host solutions out (the reference's solver seam).
+One step = one design evaluation of the covariance-load plate half model (default 352 x 352 x 48
+voxels, 18 317 523 dofs, mirror symmetry on x = 0): new element moduli, both multigrid hierarchies
+rebuilt (symmetric and antisymmetric fixture groups), the 42 load directions of each half solved by
+batched GMG-PCG to a recomputed FP64 true relative residual below 1e-8 (84 column solves), then
+F = P^T U, tr(K^-1 Sigma), lambda_max and both sensitivity fields.
 
-Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-For N > 1 (torchrun, one rank per GPU) the 42 directions of each half are
-sharded across ranks; the flexibility columns are gathered with one NCCL
-all-reduce per solve.
+* ``value``: the fastest path (FP32 V-cycle; with ``--pcg float32`` FP32 inner PCG iterations under
+  FP64 reliable residual updates; with ``--tensor-cores`` the finest-level applies on tcgen05), every
+  input resident in HBM.
+* ``results.plain_fp64``: the same step with the plain FP64 GMG-PCG (FP64 V-cycle, FP64 PCG) on the
+  same GPU, its time, the ratio to ``value`` and the agreement of tr, lambda_max and the
+  sensitivities between the two paths.
+* ``e2e``: the reference-facing ``InterfaceCovariance.measure_device`` call with a host density in
+  and both sensitivity fields read back to the host.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config NAME]
+For N > 1 (torchrun, one rank per GPU) the 42 directions of each half are sharded across ranks;
+the flexibility columns are gathered with one NCCL all-reduce per solve.
 """
 import argparse
 import json
@@ -31,25 +34,33 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "42-RHS hex8 solve s @1e-8 resid; SIMP iter/s: learned+mixed vs plain FP64"
-CONFIG = "plate_96x96x16"
+CONFIG = "plate_352x352x48"
 PLATES = ("plate_96x96x16", "plate_128x128x24", "plate_192x192x32", "plate_352x352x48")
+#: the smoother schedule the autotuner picks on the 96 x 96 x 16 plate (Chebyshev degree 1, growth 2)
+SCHEDULE = "1,2"
+#: largest problem the oracle's CPU GMG-PCG is timed on in full (one evaluation = all columns solved)
+CPU_MAX_DOFS = 2_000_000
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default=CONFIG, choices=PLATES,
                     help="covariance plate workload (the 48 x 24 x 24 cantilever is a parity case of the tests, not a bench line)")
-    ap.add_argument("--precision", default="float32")
+    ap.add_argument("--precision", default="float32", help="work precision of the fast path's V-cycle")
+    ap.add_argument("--pcg", default="float64", choices=["float64", "float32"],
+                    help="fast path's PCG iterations: FP64, or FP32 with FP64 reliable residual updates")
+    ap.add_argument("--tensor-cores", action="store_true", help="fast path's finest-level V-cycle applies on tcgen05")
+    ap.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 arm (default min(steps, 3))")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 arm")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="timed steps of the end-to-end leg (default min(steps, 3))")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tensor-cores", action="store_true", help="FP32 finest-level V-cycle apply on tcgen05 (TF32)")
-    ap.add_argument("--schedule", default=None, metavar="DEGREE,GROWTH",
-                    help="use this Chebyshev smoother schedule instead of autotuning (e.g. 1,2)")
+    ap.add_argument("--autotune", action="store_true", help="pick the smoother schedule with the autotuner instead of --schedule")
+    ap.add_argument("--schedule", default=SCHEDULE, metavar="DEGREE,GROWTH", help="Chebyshev smoother schedule of both arms")
     ap.add_argument("--instances", type=int, default=0,
                     help="solve N independent seeded plates of uneven size and RHS count concurrently and report solves/s")
     ap.add_argument("--learned", action="store_true", help="train the learned initial guess and report PCG with / without it")
@@ -58,12 +69,14 @@ def parse():
     ap.add_argument("--warm-start", type=int, default=0, nargs="?", const=-1,
                     help="SIMP: start every PCG from the previous design's solution (no value), or from the energy-optimal "
                          "combination of the last M designs' solutions (--warm-start M)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one 42-column finest-level FP32 launch of
-# the 96 x 96 x 16 plate, by epilogue mode, from ncu captures of that launch
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one 42-column finest-level FP32 residual
+# apply of the 96 x 96 x 16 plate (159 953 nodes), from an ncu capture of that launch; other grids are
+# scaled by their node count (the kernel's traffic is proportional to nodes x columns)
 FINE_TRAFFIC = {"cheb": 434e6, "resid": 220.5e6}
+FINE_TRAFFIC_NODES = 159953
 
 
 def peaks():
@@ -146,16 +159,71 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_problem(config, precision, device, tensor_cores=False, smoother=None):
+def schedule_settings(text):
+    degree, growth = text.split(",")
+    return {"smoother": "chebyshev", "chebyshev_degree": int(degree), "growth": float(growth)}
+
+
+def fast_settings(args):
+    return {"precision": args.precision, "pcg_precision": args.pcg, "tensor_cores": bool(args.tensor_cores)}
+
+
+PLAIN = {"precision": "float64", "pcg_precision": "float64", "tensor_cores": False}
+
+
+def build_problem(config, device, multigrid):
     from deep_frame_b200 import problems
     from deep_frame_b200.covariance import InterfaceCovariance
     from deep_frame_b200.elasticity import HexElasticity
     spec = problems.CONFIGS[config]
     domain, density, cov = problems.plate(spec["shape"], 0)
-    system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": spec["tolerance"], "device": str(device),
-                                              "tensor_cores": tensor_cores, **(smoother or {})})
+    system = HexElasticity(domain, multigrid={"tolerance": spec["tolerance"], "device": str(device), **multigrid})
     model = InterfaceCovariance(system, cov, domain["interfaces"])
     return spec, system, model, density
+
+
+def rebuild_multigrid(system, multigrid):
+    """Close the system's multigrid handle and let the next use build one with ``multigrid`` settings
+    (the same grid, element stiffness and fixture groups)."""
+    if system.multigrid is not None:
+        system.multigrid.close()
+        system.multigrid = None
+    system.multigrid_settings = {**(system.multigrid_settings or {}), **multigrid}
+    system.multigrid_settings.pop("_tuned", None)
+
+
+def timed_steps(step, steps, warmup, world, dist, device, clocks_index=None):
+    """W untimed steps, then K steps bracketed by a barrier and a synchronize on both sides, timed
+    with CUDA events on the current stream; the max over ranks in ms per step, the last step's
+    output and the clock record (when ``clocks_index`` is given)."""
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(clocks_index) if clocks_index is not None else None
+    if clocks:
+        clocks.__enter__()
+    try:
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed")   # lets a profiler select the timed steps' launches
+        start.record()
+        for _ in range(steps):
+            out = step()
+        stop.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+    finally:
+        if clocks:
+            clocks.__exit__(None, None, None)
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([start.elapsed_time(stop) / steps], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), out, (clocks.summary() if clocks else None)
 
 
 def ours(args):
@@ -173,19 +241,16 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    fixed = None
-    if args.schedule:
-        degree, growth = args.schedule.split(",")
-        fixed = {"smoother": "chebyshev", "chebyshev_degree": int(degree), "growth": float(growth)}
-    spec, system, model, density = build_problem(args.config, args.precision, device, args.tensor_cores, fixed)
+    smoother = schedule_settings(args.schedule)
+    spec, system, model, density = build_problem(args.config, device, {**fast_settings(args), **smoother})
     moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
     moduli = torch.as_tensor(moduli_host, device=device)
     scale = torch.as_tensor(-derivative, device=device)
     groups = model.groups()
-    tuned, tuning = None, None
-    if not args.no_autotune and not args.schedule:
+    tuning = None
+    if args.autotune:
         # measured smoother choice (outside the timed region); every candidate solves to the same tolerance
-        from deep_frame_b200.autotune import CANDIDATES, tune_smoother
+        from deep_frame_b200.autotune import tune_smoother
         choice = [None]
         if rank == 0:
             tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli)
@@ -193,63 +258,45 @@ def ours(args):
         if world > 1:
             dist.broadcast_object_list(choice, src=0)
             if rank != 0:
-                tuned, tuning = tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
-                                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores", "coarsest_dofs")}],
-                                              repeats=1)
-    mg = system._multigrid()
-    measure = ShardedMeasure(groups, model.rank, model.factor, DeviceOps(system))
+                tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
+                              candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps",
+                                                                                        "tensor_cores", "coarsest_dofs")}], repeats=1)
+
+    def arm():
+        mg = system._multigrid()
+        measure = ShardedMeasure(groups, model.rank, model.factor, DeviceOps(system))
+
+        def step():
+            mg.update_device(moduli)
+            return measure.measure(scale)
+        return mg, step, measure
+
+    mg, step, measure = arm()
     reports = mg.statistics
-
-    def step():
-        mg.update_device(moduli)
-        return measure.measure(scale)
-
-    for _ in range(args.warmup):
-        step()
-    first_report = len(reports)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    first_report = len(reports) + args.warmup * len(groups)
     launches0 = int(_lib.load().tf_launch_count())
-    with Clocks(local) as clocks:
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_push("timed")   # lets a profiler select the timed steps' launches
-        start.record()
-        for _ in range(args.steps):
-            rows, flex = step()
-        stop.record()
-        torch.cuda.nvtx.range_pop()
-        torch.cuda.synchronize()
+    ms, (rows, flex), clocks = timed_steps(step, args.steps, args.warmup, world, dist, device, clocks_index=local)
     launches = int(_lib.load().tf_launch_count()) - launches0
-    if world > 1:
-        dist.barrier()
-    ms = start.elapsed_time(stop) / args.steps
-    t = torch.tensor([ms], device=device, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
     timed = reports[first_report:]
     # per-kernel-class breakdown of one more step (CUDA events on the launching stream)
     lib = _lib.load()
     lib.tf_timers(mg.handle, 1, None, None, 0)
     torch.cuda.synchronize()
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0.record()
     step()
-    s1.record()
     torch.cuda.synchronize()
     n = len(_lib.TIMER_CLASSES)
     tms, tcnt = (ctypes.c_double * n)(), (ctypes.c_int64 * n)()
     _lib.check(lib.tf_timers(mg.handle, 0, tms, tcnt, n), mg.handle, "tf_timers")
+    lib.tf_timers(mg.handle, 0, None, None, 0)
     breakdown = {name: {"ms": round(tms[i], 3), "launches": int(tcnt[i])} for i, name in enumerate(_lib.TIMER_CLASSES)}
-    result = {"ms": ms, "launches_per_step": launches / args.steps, "breakdown": breakdown, "profiled_step_ms": s0.elapsed_time(s1),
-              "iterations_max": [int(np.max(r["iterations"])) for r in timed[-len(groups):]], "clocks": clocks.summary(),
-              "world": world, "rank": rank, "columns": [len(g["local"]) for g in measure.groups], "ndof": system.ndof,
-              "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"], "converged": all(r["converged"] for r in timed),
-              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores", "coarsest_dofs")},
-              "tuning": tuning, "tr": rows[0]["value"], "lambda_max": rows[1]["value"],
-              "grad_mean": rows[0]["gradient"].cpu().numpy(), "grad_worst": rows[1]["gradient"].cpu().numpy()}
+    result = {"ms": ms, "launches_per_step": launches / (args.warmup + args.steps), "breakdown": breakdown,
+              "iterations_max": [int(np.max(r["iterations"])) for r in timed[-len(groups):]], "clocks": clocks,
+              "world": world, "rank": rank, "columns": [len(g["local"]) for g in measure.groups],
+              "ndof": system.ndof, "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"],
+              "converged": all(r["converged"] for r in timed),
+              "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores",
+                                                                          "coarsest_dofs", "precision", "pcg_precision")},
+              "tuning": tuning, "rows": rows}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     result["dominant"] = dominant
     if breakdown[dominant]["launches"]:
@@ -257,73 +304,42 @@ def ours(args):
     result["nodes"] = int(np.prod(np.asarray(mg.padded) + 1))
     result["cols"] = sum(result["columns"])
     if world == 1 and not args.no_e2e:
-        # (1) the public design-evaluation call: host densities in, host values and sensitivities out
+        # the reference-facing measure call: InterfaceCovariance.measure_device with a host density,
+        # both sensitivity fields read back to the host
         host_density = np.ascontiguousarray(density)
-        h2d = moduli_host.nbytes
 
         def e2e_step():
-            m = torch.as_tensor(system.moduli(host_density, 3.0, 1e-9)[0], device=device)
-            mg.update_device(m)
-            r, f = measure.measure(torch.as_tensor(-system.moduli(host_density, 3.0, 1e-9)[1], device=device))
-            return r[0]["value"], r[1]["value"], r[0]["gradient"].cpu().numpy(), r[1]["gradient"].cpu().numpy()
+            r = model.measure_device(host_density, 3.0, 1e-9)
+            return r[0]["gradient"].cpu().numpy(), r[1]["gradient"].cpu().numpy()
 
-        e2e_step()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.steps):
-            out = e2e_step()
-        e1.record()
-        torch.cuda.synchronize()
-        d2h = out[2].nbytes + out[3].nbytes + 16
-        result["e2e"] = {"ms": e0.elapsed_time(e1) / args.steps, "h2d_bytes_per_step": int(2 * h2d), "d2h_bytes_per_step": int(d2h)}
-        # (2) the reference solver seam: GeometricMultigrid.update / .solve with host forces and host solutions
-        host_forces = [(key, forces.T.cpu().numpy().copy()) for key, _, forces in groups]
-
-        def solve_api_step():
-            mg.update(moduli_host)
-            return [mg.solve(key, system.groups[key][0][1]["fixed"], f)[0] for key, f in host_forces]
-
-        solve_api_step()
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(args.steps):
-            solve_api_step()
-        e1.record()
-        torch.cuda.synchronize()
-        result["solve_api"] = {"ms": e0.elapsed_time(e1) / args.steps,
-                               "h2d_bytes_per_step": int(moduli_host.nbytes + sum(f.nbytes for _, f in host_forces)),
-                               "d2h_bytes_per_step": int(sum(f.nbytes for _, f in host_forces))}
-        # (3) the reference-facing measure call itself: InterfaceCovariance.measure_device with a host density,
-        # both sensitivity fields read back to the host
-        try:
-            def measure_api_step():
-                r = model.measure_device(host_density, 3.0, 1e-9)
-                return r[0]["gradient"].cpu().numpy(), r[1]["gradient"].cpu().numpy()
-
-            measure_api_step()
-            torch.cuda.synchronize()
-            e0.record()
-            for _ in range(args.steps):
-                grads = measure_api_step()
-            e1.record()
-            torch.cuda.synchronize()
-            result["measure_api"] = {"ms": e0.elapsed_time(e1) / args.steps, "h2d_bytes_per_step": int(moduli_host.nbytes),
-                                     "d2h_bytes_per_step": int(grads[0].nbytes + grads[1].nbytes + model.rank * model.rank * 8)}
-        except (RuntimeError, ValueError) as exc:
-            result["measure_api"] = {"error": f"{type(exc).__name__}: {exc}"}
+        e2e_steps = args.e2e_steps or min(args.steps, 3)
+        e_ms, grads, _ = timed_steps(e2e_step, e2e_steps, 1, 1, dist, device)
+        result["e2e"] = {"ms": e_ms, "steps": e2e_steps, "h2d_bytes_per_step": int(moduli_host.nbytes),
+                         "d2h_bytes_per_step": int(grads[0].nbytes + grads[1].nbytes + model.rank * model.rank * 8)}
+    if world == 1 and not args.no_plain:
+        # the plain FP64 GMG-PCG drop-in on the same GPU: FP64 V-cycle and FP64 PCG, the same smoother
+        # schedule, hierarchy depth and tolerance
+        rebuild_multigrid(system, PLAIN)
+        torch.cuda.empty_cache()
+        plain_mg, plain_step, _ = arm()
+        plain_first = len(plain_mg.statistics) + len(groups)
+        plain_steps = args.plain_steps or min(args.steps, 3)
+        p_ms, (p_rows, _), p_clocks = timed_steps(plain_step, plain_steps, 1, 1, dist, device, clocks_index=local)
+        p_timed = plain_mg.statistics[plain_first:]
+        result["plain"] = {"ms": p_ms, "steps": plain_steps, "rows": p_rows, "clocks": p_clocks,
+                           "iterations_max": [int(np.max(r["iterations"])) for r in p_timed[-len(groups):]],
+                           "converged": all(r["converged"] for r in p_timed)}
     if world > 1:
         dist.destroy_process_group()
     return result, system, model, density
-
-
-def cpu_samples(system, density, count=1, block=3, cores=None):
-    """The oracle's GMG-PCG on the host cores: ``count`` parallel evaluation samples (``oracle/baseline.py``).
+def cpu_samples(system, density, count=1, cores=None):
+    """The oracle's GMG-PCG on the host cores: ``count`` measured evaluations (``oracle/baseline.py``).
 
     One single-threaded spawn-started worker per usable core (at most one per column, and no more
-    than host memory holds at ~10 KB per dof each); in every sample each worker rebuilds its half's
-    hierarchy from the moduli and solves a block of its share of the columns to 1e-8 with the
-    reference's default smoother.  Returns ``[(step estimate in s, record), ...]``."""
+    than host memory holds at ~10 KB per dof each); in every evaluation each worker rebuilds its
+    half's hierarchy from the moduli and solves its whole share of the columns to 1e-8 with the
+    reference's default smoother, so every column of both halves is solved and nothing is scaled.
+    Returns ``[(evaluation seconds, record), ...]``."""
     from oracle.baseline import ParallelBaseline, sample_text, worker_count
     moduli, _ = system.moduli(density, 3.0, 1e-9)
     groups = [(members[0][1]["fixed"], np.stack([part["force"] for _, part in members], axis=1))
@@ -333,17 +349,28 @@ def cpu_samples(system, density, count=1, block=3, cores=None):
     out = []
     with ParallelBaseline(workers) as pool:
         for _ in range(count):
-            value, record = pool.sample(system.shape, system.ke, moduli, groups, settings, block=block)
+            value, record = pool.sample(system.shape, system.ke, moduli, groups, settings, block=None)
             record["text"] = sample_text(record, settings)
             out.append((value, record))
     return out
 
 
+def cpu_unavailable(ndof):
+    """Why the oracle's CPU GMG-PCG is not timed on a problem of ``ndof`` dofs, or None when it is."""
+    if ndof <= CPU_MAX_DOFS:
+        return None
+    return (f"oracle CPU GMG-PCG not run on {ndof} dofs: budget (about 10 KB of host memory per dof and worker, "
+            f"{ndof * 10e3 / 1e9:.0f} GB for one worker, and an estimated hour or more per evaluation on the host cores); "
+            f"the GPU line's cpu_baseline carries a full measured evaluation of the 96 x 96 x 16 plate")
+
+
 def reference(args):
     """--impl reference: the oracle's CPU restatement of the reference GMG-PCG path on all of this box's host cores.
 
-    Rank 0 alone runs (other ranks return at once); every step, warm-up included, is one parallel
-    sample of the evaluation, timed and scaled as ``cpu_samples`` describes."""
+    Rank 0 alone runs (other ranks return at once).  Every step is one full measured evaluation
+    (all columns of both halves solved to 1e-8, nothing scaled); a problem beyond the host's budget
+    prints an ``unavailable`` line instead.  The CPU arm runs at most one warm-up and three timed
+    steps, and its line says how many ran."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
@@ -351,13 +378,21 @@ def reference(args):
     from deep_frame_b200.elasticity import HexElasticity
     from deep_frame_b200.covariance import InterfaceCovariance
     spec = problems.CONFIGS[args.config]
-    domain, density, cov = problems.plate(spec["shape"], 0)
+    shape = spec["shape"]
+    ndof = 3 * int(np.prod(np.asarray(shape) + 1))
+    reason = cpu_unavailable(ndof)
+    if reason:
+        line = {"impl": "reference", "unavailable": reason, "config": {"workload": args.config, "ndof": ndof}}
+        print(json.dumps(line))
+        return line
+    domain, density, cov = problems.plate(shape, 0)
     system = HexElasticity(domain)
     InterfaceCovariance(system, cov, domain["interfaces"])
+    warmup, steps = min(args.warmup, 1), min(args.steps, 3)
     samples, cores = None, None
     while samples is None:
         try:
-            samples = cpu_samples(system, density, count=args.warmup + args.steps, cores=cores)[args.warmup:]
+            samples = cpu_samples(system, density, count=warmup + steps, cores=cores)[warmup:]
         except (OSError, MemoryError, RuntimeError) as exc:   # BrokenProcessPool is a RuntimeError
             from oracle.baseline import host_cores
             cores = (cores or host_cores()) // 2
@@ -366,7 +401,8 @@ def reference(args):
                 return None
     v = float(np.mean([value for value, _ in samples]))
     record = samples[-1][1]
-    line = {"metric": METRIC, "value": round(v, 3), "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+    line = {"metric": METRIC, "value": round(v, 3), "unit": "s", "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+            "steps_requested": args.steps, "warmup_requested": args.warmup,
             "ms_per_step": round(v * 1e3, 1), "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": system.ndof, "tolerance": 1e-8,
@@ -552,22 +588,71 @@ def learned_guess(args):
     print(json.dumps(line))
 
 
-def oracle_errors(config, result):
-    """Relative errors of the step's tr, lambda_max and sensitivity fields against the FP64 oracle
-    values of the same workload (tests/golden/<workload>.npz, from tests/golden/make_plate_oracle.py:
-    the oracle's GMG-PCG to a 1e-10 true relative residual); None when no such file exists."""
+def row_values(rows):
+    """tr, lambda_max, KS and both sensitivity fields (host arrays) of a measure's rows."""
+    return {"tr": rows[0]["value"], "lambda_max": rows[1]["value"], "ks": rows[1]["info"]["ks_n_mm"],
+            "grad_mean": rows[0]["gradient"].cpu().numpy(), "grad_worst": rows[1]["gradient"].cpu().numpy()}
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - b) / np.linalg.norm(b))
+
+
+def agreement(got, want):
+    """Relative differences of tr, lambda_max, KS and the two sensitivity fields (2-norm)."""
+    return {"tr_rel": rel(got["tr"], want["tr"]), "lambda_max_rel": rel(got["lambda_max"], want["lambda_max"]),
+            "ks_rel": rel(got["ks"], want["ks"]), "grad_mean_rel": rel(got["grad_mean"], want["grad_mean"]),
+            "grad_worst_rel": rel(got["grad_worst"], want["grad_worst"]),
+            "bars": {"tr": 1e-6, "lambda_max": 1e-6, "sensitivities": 1e-5}}
+
+
+def oracle_errors(config, values):
+    """Errors of the step's values against the FP64 oracle of the same workload
+    (tests/golden/<workload>.npz, from tests/golden/make_plate_oracle.py: the oracle's GMG-PCG to a
+    1e-10 true relative residual); None when no such file exists."""
     path = ROOT / "tests" / "golden" / f"{config}.npz"
     if not path.exists():
         return None
     ref = np.load(path)
+    out = agreement(values, {"tr": float(ref["tr"]), "lambda_max": float(ref["lambda_max"]), "ks": float(ref["ks"]),
+                             "grad_mean": ref["grad_mean"], "grad_worst": ref["grad_worst"]})
+    out["oracle"] = f"FP64 GMG-PCG to {float(ref['tolerance']):g} (tests/golden/{path.name})"
+    return out
 
-    def rel(a, b):
-        return float(np.linalg.norm(np.asarray(a) - b) / np.linalg.norm(b))
 
-    return {"oracle": f"FP64 GMG-PCG to {float(ref['tolerance']):g} (tests/golden/{path.name})",
-            "tr_rel": rel(result["tr"], ref["tr"]), "lambda_max_rel": rel(result["lambda_max"], ref["lambda_max"]),
-            "grad_mean_rel": rel(result["grad_mean"], ref["grad_mean"]), "grad_worst_rel": rel(result["grad_worst"], ref["grad_worst"]),
-            "bars": {"tr": 1e-6, "lambda_max": 1e-6, "sensitivities": 1e-5}}
+def roofline(args, result):
+    """Roofline of the step's dominant kernel class: algorithmic bytes of one launch over its
+    CUDA-event duration against the measured HBM copy bandwidth, with the compute side beside it."""
+    if "dominant_per_launch_ms" not in result:
+        return None
+    hbm, _, source = peaks()
+    # algorithmic bytes of one launch, per node and column: the words its mode must read and write
+    # (+ the element moduli, once per launch).  PCG operator: u read, y written (6).  Work-precision
+    # finest level with Chebyshev degree d: per V-cycle 2 residual applies (u, b read, y written: 9)
+    # and 2 (d - 1) Chebyshev steps (u, res, x read; y, res, x written: 18).
+    dominant = result["dominant"]
+    word = 8 if dominant == "fine_fp64" or args.precision == "float64" else 4
+    nodes, cols = result["nodes"], result["cols"]
+    per_launch_cols = cols / max(1, len(result["columns"]))
+    words = 6.0
+    sm = result["smoother"]
+    degree = int(sm.get("chebyshev_degree", 3))
+    if dominant == "fine_work" and sm.get("smoother", "chebyshev") == "chebyshev":
+        words = (2 * 9 + 2 * (degree - 1) * 18) / (2 * degree)
+    traffic_alg = nodes * per_launch_cols * (words * word) + nodes * word
+    traffic = None
+    if args.precision == "float32" and dominant == "fine_work" and sm.get("smoother", "chebyshev") == "chebyshev" \
+            and not sm.get("tensor_cores"):
+        # ncu capture of the 96 x 96 x 16 plate's launch, scaled by nodes x columns
+        traffic = FINE_TRAFFIC["resid" if degree == 1 else "cheb"] * nodes * per_launch_cols / (FINE_TRAFFIC_NODES * 42)
+    achieved = traffic_alg / (result["dominant_per_launch_ms"] * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+            "traffic": traffic, "kernel": dominant, "peak_source": source,
+            "per_launch_ms": round(result["dominant_per_launch_ms"], 4), "algorithmic_bytes_per_launch": int(traffic_alg)}
+    clk = result["clocks"] or {}
+    roof["compute"] = fma_roof("fp64" if word == 8 else "fp32", 1152.0 * nodes * per_launch_cols, result["dominant_per_launch_ms"],
+                               clk.get("sm_mhz"), clk.get("sm_max_mhz") or 1965.0)
+    return roof
 
 
 def main():
@@ -587,75 +672,66 @@ def main():
     result, system, model, density = ours(args)
     if result["rank"] != 0:
         return
-    hbm, bf16, source = peaks()
     ms = result["ms"]
-    # algorithmic bytes of one launch of the dominant kernel, per node and column: the words its mode
-    # must read and write (+ the element moduli, once per launch: a CTA stages them for its columns).  PCG operator: u read, y
-    # written (6).  Work-precision finest level with Chebyshev degree d: per V-cycle 2 residual applies
-    # (u, b read, y written: 9) and 2 (d - 1) Chebyshev steps (u, res, x read; y, res, x written: 18).
-    dominant = result["dominant"]
-    word = 8 if dominant == "fine_fp64" or args.precision == "float64" else 4
-    nodes, cols = result["nodes"], result["cols"]
-    per_launch_cols = cols / max(1, len(result["columns"]))
-    words = 6.0
-    sm = result["smoother"]
-    if dominant == "fine_work" and sm.get("smoother", "chebyshev") == "chebyshev":
-        d = int(sm.get("chebyshev_degree", 3))
-        words = (2 * 9 + 2 * (d - 1) * 18) / (2 * d)
-    traffic_alg = nodes * per_launch_cols * (words * word) + nodes * word
-    # DRAM bytes of one finest-level FP32 launch on this workload, from an ncu capture of that
-    # launch (dram__bytes_read.sum + dram__bytes_write.sum); None for other kernels
-    traffic = None
-    if args.config == CONFIG and args.precision == "float32" and dominant == "fine_work" and sm.get("smoother", "chebyshev") == "chebyshev":
-        # ncu captures on this workload: a residual apply (degree 1 schedules) and a Chebyshev step
-        traffic = FINE_TRAFFIC.get("resid" if int(sm.get("chebyshev_degree", 3)) == 1 else "cheb")
-    roof = None
-    if "dominant_per_launch_ms" in result:
-        achieved = traffic_alg / (result["dominant_per_launch_ms"] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                "traffic": traffic, "kernel": dominant, "peak_source": source,
-                "per_launch_ms": round(result["dominant_per_launch_ms"], 4), "algorithmic_bytes_per_launch": int(traffic_alg)}
-        # the same launch against the CUDA-core FMA pipe that bounds it: 576 FMA (1152 flop) per node and column
-        clk = result["clocks"] or {}
-        roof["compute"] = fma_roof("fp64" if word == 8 else "fp32", 1152.0 * nodes * per_launch_cols, result["dominant_per_launch_ms"],
-                                   clk.get("sm_mhz"), clk.get("sm_max_mhz") or 1965.0)
     cpu = None
     if not args.no_cpu and result["world"] == 1:
+        # a full measured evaluation of the 96 x 96 x 16 plate when this workload is beyond the host
+        sample_config = args.config
         try:
+            if cpu_unavailable(system.ndof):
+                sample_config = "plate_96x96x16"
+                _, system, _, density = cpu_problem(sample_config)
             value, sample = cpu_samples(system, density)[0]
-            cpu = {"value": round(value, 2), "unit": "s", "cores": sample["workers"], "kind": "port", "sample": sample["text"]}
+            cpu = {"value": round(value, 2), "unit": "s", "cores": sample["workers"], "kind": "port", "workload": sample_config,
+                   "sample": sample["text"] + ("" if sample_config == args.config else f"; workload {sample_config}, not {args.config}")}
         except (OSError, MemoryError, RuntimeError) as exc:   # the GPU line is kept whatever the CPU leg does
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "error": f"{type(exc).__name__}: {exc}"}
+    sm = result["smoother"]
+    fast = row_values(result["rows"])
     line = {"metric": METRIC, "value": round(ms / 1e3, 6), "unit": "s", "n_gpus": result["world"], "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.config, "rhs_per_half": 42, "halves": 2, "ndof": result["ndof"], "tolerance": 1e-8,
-                       "outer": "fp64 PCG", "vcycle": args.precision + (" (finest apply: tcgen05 TF32)" if result["smoother"].get("tensor_cores") else ""), "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"],
-                       "pcg_iterations": result["iterations_max"], "smoother": result["smoother"],
-                       "smoother_choice": (f"autotuned (fastest of {len(result['tuning'])} schedules / depths / finest-apply units, all to the same tolerance)"
-                                           if result["tuning"] else ("fixed by --schedule" if args.schedule else "reference default")),
-                       "l2": "working set > L2 (FP64 vector blocks of 161 MB per half)",
+                       "outer": "fp64 PCG" if sm.get("pcg_precision", "float64") == "float64" else "fp32 PCG, fp64 reliable residual updates",
+                       "vcycle": args.precision + (" (finest apply: tcgen05)" if sm.get("tensor_cores") else ""),
+                       "levels": result["levels"], "coarsest_dofs": result["coarsest_dofs"], "pcg_iterations": result["iterations_max"],
+                       "smoother": sm,
+                       "smoother_choice": (f"autotuned (fastest of {len(result['tuning'])} schedules / depths / finest-apply units)"
+                                           if result["tuning"] else "fixed: the autotuner's pick on the 96 x 96 x 16 plate"),
+                       "l2": "working set > L2 (FP64 vector blocks of %.0f MB per half)" % (result["ndof"] * 42 * 8 / 1e6),
+                       "learned_guess": "off: dropped by its policy (no iteration gain measured)",
                        "parallelism": f"rhs-sharded x{result['world']}"},
             "clocks": result["clocks"], "gpu_launches": int(result["launches_per_step"] * args.steps),
-            "roofline": roof, "cpu_baseline": cpu, "breakdown_ms": result["breakdown"], "converged": result["converged"]}
+            "roofline": roofline(args, result), "cpu_baseline": cpu, "breakdown_ms": result["breakdown"], "converged": result["converged"]}
     if "e2e" in result:
         e = result["e2e"]
         line["e2e"] = {"value": round(e["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": e["h2d_bytes_per_step"],
-                       "d2h_bytes_per_step": e["d2h_bytes_per_step"], "call": "InterfaceCovariance-style measure: host density in, host tr / lambda_max / sensitivities out"}
-        a = result["solve_api"]
-        line["e2e_solve_api"] = {"value": round(a["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": a["h2d_bytes_per_step"],
-                                 "d2h_bytes_per_step": a["d2h_bytes_per_step"], "call": "GeometricMultigrid.update + .solve per half with host NumPy forces and solutions"}
-        m = result.get("measure_api")
-        if m is not None:
-            line["e2e_measure_api"] = ({"error": m["error"]} if "error" in m else
-                                       {"value": round(m["ms"] / 1e3, 6), "unit": "s", "h2d_bytes_per_step": m["h2d_bytes_per_step"],
-                                        "d2h_bytes_per_step": m["d2h_bytes_per_step"],
-                                        "call": "InterfaceCovariance.measure_device(host density), both sensitivity fields to the host"})
-    line["results"] = {"tr_K_inv_sigma": result["tr"], "lambda_max": result["lambda_max"]}
-    parity = oracle_errors(args.config, result)
+                       "d2h_bytes_per_step": e["d2h_bytes_per_step"], "steps": e["steps"],
+                       "call": "InterfaceCovariance.measure_device(host density): SIMP moduli, update, both halves solved, "
+                               "F, tr, lambda_max, both sensitivity fields to the host"}
+    line["results"] = {"tr_K_inv_sigma": fast["tr"], "lambda_max": fast["lambda_max"], "ks": fast["ks"]}
+    if "plain" in result:
+        plain = result["plain"]
+        line["results"]["plain_fp64"] = {
+            "s": round(plain["ms"] / 1e3, 6), "steps": plain["steps"], "speedup_of_value": round(plain["ms"] / ms, 3),
+            "pcg_iterations": plain["iterations_max"], "converged": plain["converged"], "clocks": plain["clocks"],
+            "path": "FP64 V-cycle, FP64 PCG, CUDA-core operators, same schedule and tolerance",
+            "fast_vs_plain": agreement(fast, row_values(plain["rows"]))}
+    parity = oracle_errors(args.config, fast)
     if parity:
         line["results"]["vs_fp64_oracle"] = parity
     print(json.dumps(line))
+
+
+def cpu_problem(config):
+    from deep_frame_b200 import problems
+    from deep_frame_b200.covariance import InterfaceCovariance
+    from deep_frame_b200.elasticity import HexElasticity
+    spec = problems.CONFIGS[config]
+    domain, density, cov = problems.plate(spec["shape"], 0)
+    system = HexElasticity(domain)
+    model = InterfaceCovariance(system, cov, domain["interfaces"])
+    return spec, system, model, density
 
 
 if __name__ == "__main__":

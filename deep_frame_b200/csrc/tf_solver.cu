@@ -1418,6 +1418,23 @@ extern "C" int tf_apply(tf_handle* h, uint64_t key, int32_t use_mask, const doub
   });
 }
 
+extern "C" int tf_apply_level(tf_handle* h, uint64_t key, int32_t level, const double* u_dev, int32_t nrhs, double* y_dev,
+                              void* stream) {
+  if (!h) return TF_INVALID;
+  return guard(h, [&] {
+    require(nrhs >= 0 && (nrhs == 0 || (u_dev && y_dev)), "invalid operator arguments");
+    require(level >= 0 && level < h->nlev, "level out of range");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Hierarchy& hy = get_hierarchy(h, key, s);
+    if (nrhs == 0) return;
+    LevelArgs<double> a = level_args<double>(h, hy, level, nrhs, nullptr);
+    a.E = level_E<double>(h, hy, level, true);
+    a.u = u_dev;
+    a.y = y_dev;
+    launch_level<double>(h, level, a, MODE_APPLY, s);
+  });
+}
+
 namespace {
 // y = mask * (sum_e mass_e M0 u_e + lumped * u) on the padded finest grid, u already masked; one thread
 // per (node, column), 8 elements x 8 corners x 9 FMA per node in a fixed order (deterministic).

@@ -287,6 +287,16 @@ class GeometricMultigrid:
                                      _lib.ptr(out), self._stream()), self.handle, "tf_apply")
         return out
 
+    def apply_level_device(self, key, fixed, level, columns, out=None):
+        """y = mask_l * A_l (mask_l * u) on [R, 3 * nodes_l] device columns of the padded level-l grid:
+        the level operators of the hierarchy of ``key`` in FP64 (level 0 the masked finest operator,
+        deeper levels the Galerkin operators; topology_multigrid.py:110-117)."""
+        ident = self._key((key, False), fixed)
+        out = self.torch.empty_like(columns) if out is None else out
+        _lib.check(self.lib.tf_apply_level(self.handle, ident, int(level), _lib.ptr(columns), columns.shape[0], _lib.ptr(out),
+                                           self._stream()), self.handle, "tf_apply_level")
+        return out
+
     def operator(self, grid, moduli=None, mask=None):
         """y = mask * K (mask * u) on a grid [R, 3, padded nodes] (topology_multigrid.py:105-109)."""
         if moduli is not None:

@@ -149,6 +149,14 @@ TF_API int tf_precondition(tf_handle* h, uint64_t key, const double* r_dev, int3
 TF_API int tf_apply(tf_handle* h, uint64_t key, int32_t use_mask, const double* u_dev, int32_t nrhs, double* y_dev,
              void* stream);
 
+/* One level operator of the hierarchy of `key` in FP64 (the reference's _apply, topology_multigrid.py:110-117):
+ * level 0 the masked finest operator, level l >= 1 the Galerkin operator P^T A_{l-1} P of
+ * :145-208 as assembled by this library, y = mask_l * A_l (mask_l * u).  u_dev, y_dev are
+ * [nrhs][3 * nodes_l] device FP64 vectors on the PADDED level grid of
+ * (padded[0] >> l) x (padded[1] >> l) x (padded[2] >> l) elements (tf_levels gives `padded`). */
+TF_API int tf_apply_level(tf_handle* h, uint64_t key, int32_t level, const double* u_dev, int32_t nrhs, double* y_dev,
+                          void* stream);
+
 /* GeometricMultigrid.element_energy (topology_multigrid.py:458-459) and the
  * sensitivity sums of HexElasticity._collect (topology_optimization.py:721-734) /
  * InterfaceCovariance.energy (topology_problem.py:647-652):

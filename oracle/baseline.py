@@ -11,12 +11,11 @@ the G groups gets W / G single-threaded workers; a worker builds its group's hie
 solves its share of that group's columns as one batched block.
 
 The sample.  A spawn-started pool of W workers runs concurrently, so the cores contend for memory
-bandwidth as they would in a full evaluation.  Each worker does one hierarchy set-up and solves a
-block of at most ``block`` of its share's columns to convergence.  The step estimate is, per
-group, the slowest worker's set-up plus its block time scaled by share / block, and the maximum
-over groups.  Per-column cost falls as a batched block grows, so when share > block the linear
-scaling overstates the CPU time somewhat; with at least as many workers per group as columns
-(share = 1 <= block) nothing is scaled.
+bandwidth as they would in a full evaluation.  Each worker does one hierarchy set-up and solves
+its whole share of the columns to convergence (the benchmark's default, a complete measured
+evaluation), or a block of at most ``block`` of them.  The step time is, per group, the slowest
+worker's set-up plus its solve time (scaled by share / block when a block is smaller than the
+share), and the maximum over groups.
 """
 import multiprocessing as mp
 import os
@@ -167,17 +166,19 @@ class ParallelBaseline:
     def __exit__(self, *exc):
         self.close()
 
-    def sample(self, shape, ke, moduli, groups, settings, block=3):
+    def sample(self, shape, ke, moduli, groups, settings, block=None):
         """Time one parallel evaluation sample.
 
-        ``groups``: per fixture group ``(fixed dofs, forces [ndof, R])``.  Returns the step estimate
-        in seconds and a record of what was measured."""
+        ``groups``: per fixture group ``(fixed dofs, forces [ndof, R])``; ``block`` caps the columns a
+        worker solves (None: its whole share, so the sample is a complete evaluation).  Returns the
+        step time in seconds (an estimate when a block is smaller than its share) and a record of
+        what was measured."""
         plan = assignment([f.shape[1] for _, f in groups], self.workers)
         tasks, owner = [], []
         for g, ((fixed, forces), (count, shares)) in enumerate(zip(groups, plan)):
             start = 0
             for share in shares:
-                width = min(share, block)
+                width = share if block is None else min(share, block)
                 tasks.append((tuple(shape), ke, moduli, fixed, np.ascontiguousarray(forces[:, start:start + width]), settings))
                 owner.append((g, share))
                 start += share
@@ -197,7 +198,7 @@ class ParallelBaseline:
                           "column_s": float(np.mean([r["solve_s"] / r["columns"] for r in results])),
                           "sampled_columns": int(sum(r["columns"] for r in results)),
                           "columns": int(sum(f.shape[1] for _, f in groups)),
-                          "max_share": int(max(s for _, s in owner)), "block": int(block),
+                          "max_share": int(max(s for _, s in owner)), "block": int(block) if block is not None else None,
                           "iterations_mean": float(np.mean(iterations)), "iterations_max": int(max(iterations)),
                           "relative_max": float(max(x for r in results for x in r["relative"])),
                           "rss_bytes_max": int(max(r["rss_bytes"] for r in results))}
@@ -205,8 +206,9 @@ class ParallelBaseline:
 
 def sample_text(record, settings):
     """One-line description of a sample for the benchmark's ``cpu_baseline.sample``."""
-    scaled = (f"each worker's block of {record['block']} columns scaled to its share of {record['max_share']}"
-              if record["max_share"] > record["block"] else "nothing scaled (every worker solved its whole share)")
+    block = record["block"]
+    scaled = (f"each worker's block of {block} columns scaled to its share of {record['max_share']}"
+              if block is not None and record["max_share"] > block else "nothing scaled (every worker solved its whole share)")
     return (f"oracle GMG-PCG (NumPy/SciPy, one single-threaded process per core, {record['workers']} processes run "
             f"concurrently): per worker one hierarchy set-up of its mirror half plus a batched block of its columns "
             f"solved to {settings.get('tolerance', 1e-8):g} ({record['sampled_columns']} of {record['columns']} columns, "

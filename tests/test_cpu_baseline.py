@@ -44,3 +44,20 @@ def test_parallel_sample_converges():
     assert record["max_share"] == 3 and record["relative_max"] < 1e-8
     assert value >= max(record["group_s"]) - 1e-12 and value > 0
     assert "scaled to its share of 3" in sample_text(record, settings)
+
+
+def test_full_share_sample_scales_nothing():
+    shape = (6, 4, 4)
+    k0 = hex8.element_matrices((1.0, 1.0, 1.0), 0.3)[0]
+    nodes = tuple(n + 1 for n in shape)
+    rng = np.random.default_rng(1)
+    moduli = rng.uniform(0.1, 1.0, int(np.prod(shape)))
+    clamp = np.flatnonzero(np.indices(nodes).reshape(3, -1)[0] == 0)
+    fixed = (3 * clamp[:, None] + np.arange(3)).ravel()
+    forces = rng.standard_normal((3 * int(np.prod(nodes)), 3))
+    forces[fixed] = 0.0
+    settings = {"tolerance": 1e-8}
+    with ParallelBaseline(2) as pool:
+        value, record = pool.sample(shape, k0, moduli, [(fixed, forces)], settings)
+    assert record["sampled_columns"] == record["columns"] == 3 and record["block"] is None
+    assert "nothing scaled" in sample_text(record, settings) and value == max(record["group_s"])
