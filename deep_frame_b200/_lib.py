@@ -25,7 +25,7 @@ SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_
             "tf_chol_create", "tf_chol_factor_csr", "tf_chol_solve", "tf_chol_destroy", "tf_chol_last_error")
 SYMBOLS += ("tf_nn_last_error", "tf_nn_gemm", "tf_nn_im2col", "tf_nn_col2im", "tf_nn_bias_act", "tf_nn_act_back", "tf_nn_pool",
             "tf_nn_resample", "tf_nn_mse", "tf_nn_mse_scratch_doubles", "tf_nn_adam")
-TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy")
+TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy", "fine_pcg32")
 
 
 class TfSettings(ctypes.Structure):
@@ -35,7 +35,7 @@ class TfSettings(ctypes.Structure):
                 ("retries", ctypes.c_int32), ("batch", ctypes.c_int32), ("tensor_cores", ctypes.c_int32),
                 ("coarsest_dofs", ctypes.c_int64), ("damping", ctypes.c_double), ("chebyshev_ratio", ctypes.c_double),
                 ("growth", ctypes.c_double), ("tolerance", ctypes.c_double), ("dead_ratio", ctypes.c_double),
-                ("zero_rhs", ctypes.c_double)]
+                ("zero_rhs", ctypes.c_double), ("reliable", ctypes.c_double), ("pcg_precision", ctypes.c_int32)]
 
 
 class TfGrid(ctypes.Structure):

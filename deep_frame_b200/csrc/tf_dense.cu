@@ -441,10 +441,12 @@ void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, 
 }  // namespace tfb
 
 // ---------------------------------------------------------------------------
-// Dense FP64 direct solver of a small sparse SPD system (the drop-in for the
-// reference's CudaDirectSolver, deep_frame/topology_optimization.py:80-244):
-// the CSR matrix is scattered into a dense n x n array, symmetrised, factored
-// (A = L L^T), and L is inverted once; each solve is x = L^-T (L^-1 b).
+// FP64 direct solver of a sparse SPD system (the drop-in for the reference's
+// CudaDirectSolver, deep_frame/topology_optimization.py:80-244).  A matrix whose
+// band is much smaller than the dense matrix (a voxel grid's reduced stiffness)
+// is factored banded (tf_band.cu); otherwise the CSR matrix is scattered into a
+// dense n x n array, symmetrised, factored (A = L L^T), and L is inverted once;
+// each solve is x = L^-T (L^-1 b).
 // ---------------------------------------------------------------------------
 #include <algorithm>
 #include <string>
@@ -465,7 +467,9 @@ __global__ void csr_to_dense_kernel(int n, const int32_t* __restrict__ indptr, c
 
 struct tf_chol {
   int n = 0;
-  tfb::DevBuf A, X, tmp, info, work, fwork;
+  int bw = -1;          // bandwidth of the last factored matrix
+  bool band = false;    // the last factorisation is banded (else dense with the explicit inverse factor)
+  tfb::DevBuf A, X, tmp, info, work, fwork, AB, scratch;
   bool factored = false;
   std::string err;
 };
@@ -484,7 +488,8 @@ int chol_guard(tf_chol* h, F&& f) {
     return tfb::TF_INTERNAL;
   }
 }
-constexpr int64_t CHOL_MAX_N = 32768;
+constexpr int64_t CHOL_DENSE_MAX_N = 32768;          // dense factor and inverse: 2 n^2 doubles
+constexpr double CHOL_BAND_MAX_BYTES = 96.0 * (1 << 30);  // band storage (bw + 1) n doubles
 }  // namespace
 
 extern "C" int tf_chol_create(int64_t n, tf_chol** out) {
@@ -492,11 +497,10 @@ extern "C" int tf_chol_create(int64_t n, tf_chol** out) {
   *out = nullptr;
   tf_chol* h = new tf_chol();
   const int rc = chol_guard(h, [&] {
-    tfb::require(n >= 1 && n <= CHOL_MAX_N, "the dense direct solver handles 1 to 32768 unknowns");
+    tfb::require(n >= 1 && n < (1LL << 31), "the direct solver handles 1 to 2^31 - 1 unknowns");
     h->n = static_cast<int>(n);
-    h->A.alloc(sizeof(double) * n * n);
-    h->X.alloc(sizeof(double) * n * n);
     h->info.alloc(sizeof(int));
+    h->scratch.alloc(sizeof(int));
   });
   if (rc != tfb::TF_OK) {
     tfb::record_unhandled_error(h->err);
@@ -515,6 +519,26 @@ extern "C" int tf_chol_factor_csr(tf_chol* h, const int32_t* indptr_dev, const i
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int n = h->n;
     h->factored = false;
+    // a banded factor when the band is much smaller than the dense matrix (a grid's stiffness in
+    // its natural order), the dense factor with its explicit inverse otherwise
+    h->bw = tfb::band_width(n, indptr_dev, indices_dev, h->scratch.as<int>(), s);
+    h->band = n > CHOL_DENSE_MAX_N || (double)(h->bw + 1) * 8.0 <= (double)n;
+    if (h->band) {
+      const double bytes = 8.0 * (h->bw + 1) * (double)n;
+      tfb::require(bytes <= CHOL_BAND_MAX_BYTES, "the band of this matrix needs " + std::to_string(bytes / 1e9) +
+                                                     " GB; reorder it to a smaller bandwidth or use the multigrid solver");
+      h->AB.ensure(static_cast<size_t>(bytes));
+      tfb::band_assemble(n, indptr_dev, indices_dev, data_dev, h->bw, h->AB.as<double>(), s);
+      tfb::band_cholesky(h->AB.as<double>(), n, h->bw, h->info.as<int>(), s);
+      int info = 0;
+      TF_CUDA_CHECK(cudaMemcpyAsync(&info, h->info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      TF_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (info != 0) throw tfb::Error(tfb::TF_NUMERIC, "matrix is not positive definite (pivot " + std::to_string(info) + ")");
+      h->factored = true;
+      return;
+    }
+    h->A.ensure(sizeof(double) * n * n);
+    h->X.ensure(sizeof(double) * n * n);
     TF_CUDA_CHECK(cudaMemsetAsync(h->A.p, 0, h->A.bytes, s));
     csr_to_dense_kernel<<<tfb::grid_for(n, 128), 128, 0, s>>>(n, indptr_dev, indices_dev, data_dev, h->A.as<double>());
     TF_LAUNCH_CHECK("csr_to_dense_kernel");
@@ -536,6 +560,10 @@ extern "C" int tf_chol_solve(tf_chol* h, const double* b_dev, int32_t nrhs, doub
     tfb::require(h->factored, "tf_chol_solve: no factorisation (call tf_chol_factor_csr first)");
     tfb::require(nrhs >= 1 && b_dev && x_dev, "tf_chol_solve: invalid right-hand sides");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (h->band) {
+      tfb::band_solve(h->AB.as<double>(), h->n, h->bw, b_dev, x_dev, nrhs, s);
+      return;
+    }
     const size_t need = sizeof(double) * (size_t)h->n * nrhs;
     if (h->tmp.bytes < need) h->tmp.alloc(need);
     h->work.ensure(std::max(h->work.bytes, tfb::dense_trimul_work(h->n, nrhs)));

@@ -1,6 +1,7 @@
 // Dense FP64 helpers for the coarsest multigrid level.
 #pragma once
 #include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
 
 namespace tfb {
@@ -16,4 +17,14 @@ size_t dense_factor_work(int n);
 void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active, double* work,
                   cudaStream_t s);
 size_t dense_trimul_work(int n, int ncol);
+
+// Banded FP64 Cholesky (tf_band.cu).  Band storage AB[j * (bw + 1) + d] = A[j + d][j], 0 <= d <= bw.
+// bandwidth of a CSR matrix (max |i - j| over its entries); scratch_dev holds one int
+int band_width(int n, const int32_t* indptr, const int32_t* indices, int* scratch_dev, cudaStream_t s);
+// AB <- the band of (A + A^T) / 2
+void band_assemble(int n, const int32_t* indptr, const int32_t* indices, const double* data, int bw, double* AB, cudaStream_t s);
+// AB <- L (A = L L^T) in place; *info_dev = 1 + the first non-positive pivot's column (0 on success)
+void band_cholesky(double* AB, int n, int bw, int* info_dev, cudaStream_t s);
+// x = A^-1 b for nrhs columns stored [nrhs][n]
+void band_solve(const double* AB, int n, int bw, const double* b, double* x, int nrhs, cudaStream_t s);
 }  // namespace tfb

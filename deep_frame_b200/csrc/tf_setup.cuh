@@ -14,6 +14,7 @@ struct PcgState {
   double* rzo;
   double* beta;
   double* wscale;          // scale the preconditioner output w was formed with: z = wscale * w
+  double* rtrue;           // true relative residual at the last FP64 residual recomputation
   int* active;
   int* cand;
   int* iters;
@@ -440,13 +441,16 @@ __global__ void pcg_norm_kernel(const double* __restrict__ b, long long n, PcgSt
   if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) out[col] = take_sqrt ? sqrt(a) : a;
 }
 
-// alpha = rho / (p . q)
-__global__ void pcg_alpha_kernel(const double* __restrict__ p, const double* __restrict__ q, long long n, PcgState st) {
+// alpha = rho / (p . q).  R is the type of the PCG vectors: double for the FP64 PCG, float for the
+// FP32 iterations of the mixed PCG (dot products accumulate in double either way).
+template <typename R>
+__global__ void pcg_alpha_kernel(const R* __restrict__ p, const R* __restrict__ q, long long n, PcgState st) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   double a = 0.0, z = 0.0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a += p[off + t] * q[off + t];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    a += static_cast<double>(p[off + t]) * static_cast<double>(q[off + t]);
   block_reduce2<0, 0>(a, z);
   if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) st.alpha[col] = st.rho[col] / a;
 }
@@ -454,11 +458,13 @@ __global__ void pcg_alpha_kernel(const double* __restrict__ p, const double* __r
 // x += alpha p; r -= alpha q; rel = ||r|| / ||b||; candidate when rel < tol (topology_multigrid.py:424-430).
 // The same pass forms the next preconditioner inputs, scale = max|r| (clamped at 1e-300) and
 // rzo = r . z_old (topology_multigrid.py:320, :446), with z_old = wscale * w rebuilt from the
-// work-precision preconditioner output: z itself is never stored.
-template <typename T>
-__global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
-                                  const double* __restrict__ q, const T* __restrict__ w, long long n, PcgState st, double tol,
-                                  int step) {
+// work-precision preconditioner output: z itself is never stored.  x is always FP64.  With
+// reliable > 0 (the mixed PCG) a column whose iterated residual fell below reliable times its
+// last true residual also asks for the FP64 residual recomputation (a reliable update).
+template <typename T, typename R>
+__global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, const R* __restrict__ p,
+                                  const R* __restrict__ q, const T* __restrict__ w, long long n, PcgState st, double tol,
+                                  int step, double reliable) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
@@ -466,12 +472,13 @@ __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r
   const double zs = st.wscale[col];
   double a = 0.0, mx = 0.0, d = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    x[off + t] += al * p[off + t];
-    const double rv = r[off + t] - al * q[off + t];
+    x[off + t] += al * static_cast<double>(p[off + t]);
+    const R rv = static_cast<R>(static_cast<double>(r[off + t]) - al * static_cast<double>(q[off + t]));
     r[off + t] = rv;
-    a += rv * rv;
-    mx = fmax(mx, fabs(rv));
-    d += rv * (static_cast<double>(w[off + t]) * zs);
+    const double rd = static_cast<double>(rv);
+    a += rd * rd;
+    mx = fmax(mx, fabs(rd));
+    d += rd * (static_cast<double>(w[off + t]) * zs);
   }
   block_reduce3<0, 1, 0>(a, mx, d);
   if (last_block_combine3<0, 1, 0>(a, mx, d, st.partial, st.count, col)) {
@@ -480,15 +487,14 @@ __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r
     st.scale[col] = fmax(mx, 1e-300);
     st.rzo[col] = d;
     atomicMax(&st.hist[step - 1], static_cast<unsigned long long>(__double_as_longlong(rel)));
-    if (rel < tol) { st.cand[col] = 1; atomicExch(&st.flags[0], 1); }
+    if (rel < tol || (reliable > 0.0 && rel < reliable * st.rtrue[col])) { st.cand[col] = 1; atomicExch(&st.flags[0], 1); }
   }
 }
 
 // True-residual recheck (topology_multigrid.py:431-437): when any column is a
 // candidate, every active column's residual is recomputed as t = b - K x; a
 // column converges when ||t|| / ||b|| < tol, the others continue from t.
-__global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, double* __restrict__ r, long long n, PcgState st,
-                                     double tol, int step) {
+__global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, long long n, PcgState st, double tol, int step) {
   const int col = blockIdx.y;
   if (!st.flags[0] || !st.active[col]) return;
   const long long off = (long long)col * n;
@@ -501,14 +507,15 @@ __global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, double* _
   if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) {
     const double rel = sqrt(a) / st.bnorm[col];
     st.rel[col] = rel;
+    st.rtrue[col] = rel;
     st.cand[col] = (rel < tol) ? 2 : 3;   // 2 = converged, 3 = continue from the true residual
   }
 }
 
 // Columns that continue from the true residual (cand 3): r <- t, and the preconditioner inputs
 // scale = max|t| and rzo = t . z_old are formed again from the new r.
-template <typename T>
-__global__ void pcg_retire_kernel(const double* __restrict__ t_res, double* __restrict__ r, const T* __restrict__ w, long long n,
+template <typename T, typename R>
+__global__ void pcg_retire_kernel(const double* __restrict__ t_res, R* __restrict__ r, const T* __restrict__ w, long long n,
                                   PcgState st) {
   const int col = blockIdx.y;
   if (!st.active[col] || st.cand[col] != 3) return;
@@ -517,7 +524,7 @@ __global__ void pcg_retire_kernel(const double* __restrict__ t_res, double* __re
   double mx = 0.0, d = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const double v = t_res[off + t];
-    r[off + t] = v;
+    r[off + t] = static_cast<R>(v);
     mx = fmax(mx, fabs(v));
     d += v * (static_cast<double>(w[off + t]) * zs);
   }
@@ -552,32 +559,55 @@ __global__ void pcg_flags_kernel(PcgState st, int step) {
   }
 }
 
+// The starting residual: r = t (t = b, or b - K x0 for a warm start), scale = max|t| (clamped at
+// 1e-300; topology_multigrid.py:320) and rtrue = ||t|| / ||b||, the reference of the first
+// reliable update.
+template <typename R>
+__global__ void pcg_take_kernel(const double* __restrict__ t_res, R* __restrict__ r, long long n, PcgState st) {
+  const int col = blockIdx.y;
+  if (!st.active[col]) return;
+  const long long off = (long long)col * n;
+  double mx = 0.0, a = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double v = t_res[off + t];
+    r[off + t] = static_cast<R>(v);
+    mx = fmax(mx, fabs(v));
+    a += v * v;
+  }
+  block_reduce2<1, 0>(mx, a);
+  if (last_block_combine<1, 0>(mx, a, st.partial, st.count, col)) {
+    st.scale[col] = fmax(mx, 1e-300);
+    st.rtrue[col] = sqrt(a) / st.bnorm[col];
+  }
+}
+
 // scale = max|r| (clamped at 1e-300) before the first preconditioner application (topology_multigrid.py:320)
-__global__ void pcg_prep_kernel(const double* __restrict__ r, long long n, PcgState st) {
+template <typename R>
+__global__ void pcg_prep_kernel(const R* __restrict__ r, long long n, PcgState st) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   double mx = 0.0, d = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    mx = fmax(mx, fabs(r[off + t]));
+    mx = fmax(mx, fabs(static_cast<double>(r[off + t])));
   block_reduce2<1, 0>(mx, d);
   if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) st.scale[col] = fmax(mx, 1e-300);
 }
 
-template <typename T>
-__global__ void pcg_to_work_kernel(const double* __restrict__ r, long long n, PcgState st, T* __restrict__ w) {
+template <typename T, typename R>
+__global__ void pcg_to_work_kernel(const R* __restrict__ r, long long n, PcgState st, T* __restrict__ w) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   const double s = 1.0 / st.scale[col];
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    w[off + t] = static_cast<T>(r[off + t] * s);
+    w[off + t] = static_cast<T>(static_cast<double>(r[off + t]) * s);
 }
 
 // rz = r . z with z = scale * w (w: the work-precision preconditioner output); beta = (rz - rzo) / rho
 // (flexible Polak-Ribiere, topology_multigrid.py:445-448).  z is written out only when asked for (z != nullptr).
-template <typename T>
-__global__ void pcg_from_work_kernel(const T* __restrict__ w, const double* __restrict__ r, double* __restrict__ z, long long n,
+template <typename T, typename R>
+__global__ void pcg_from_work_kernel(const T* __restrict__ w, const R* __restrict__ r, double* __restrict__ z, long long n,
                                      PcgState st, int initial) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
@@ -587,7 +617,7 @@ __global__ void pcg_from_work_kernel(const T* __restrict__ w, const double* __re
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const double v = static_cast<double>(w[off + t]) * s;
     if (z) z[off + t] = v;
-    d += r[off + t] * v;
+    d += static_cast<double>(r[off + t]) * v;
   }
   block_reduce2<0, 0>(d, zz);
   if (last_block_combine<0, 0>(d, zz, st.partial, st.count, col)) {
@@ -598,15 +628,15 @@ __global__ void pcg_from_work_kernel(const T* __restrict__ w, const double* __re
 }
 
 // p = z + beta p, z = wscale * w
-template <typename T>
-__global__ void pcg_direction_kernel(const T* __restrict__ w, double* __restrict__ p, long long n, PcgState st, int initial) {
+template <typename T, typename R>
+__global__ void pcg_direction_kernel(const T* __restrict__ w, R* __restrict__ p, long long n, PcgState st, int initial) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   const double be = st.beta[col], s = st.wscale[col];
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const double z = static_cast<double>(w[off + t]) * s;
-    p[off + t] = initial ? z : z + be * p[off + t];
+    p[off + t] = static_cast<R>(initial ? z : z + be * static_cast<double>(p[off + t]));
   }
 }
 

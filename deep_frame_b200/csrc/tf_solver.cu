@@ -96,7 +96,8 @@ enum TimerClass : int {
   TIMER_COARSEST = 5,  // dense coarsest solve
   TIMER_SETUP = 6,     // hierarchy build (masks, Galerkin blocks, lambda_max, factor)
   TIMER_ENERGY = 7,    // element energies
-  TIMER_CLASSES = 8
+  TIMER_PCG32 = 8,     // FP32 finest-level operator of the mixed PCG's iterations
+  TIMER_CLASSES = 9
 };
 
 struct Timers {
@@ -236,7 +237,7 @@ void ensure_vbufs(tf_handle* h, int ncol) {
 void ensure_pcg(tf_handle* h, int ncol) {
   ensure_scratch(h, ncol);
   if (h->pcg_cap < ncol) {
-    h->pcg_d.alloc(sizeof(double) * 8 * ncol);
+    h->pcg_d.alloc(sizeof(double) * 9 * ncol);
     h->pcg_i.alloc(sizeof(int) * (4 * ncol + 8));
     h->colmap.alloc(sizeof(int) * ncol);
     TF_CUDA_CHECK(cudaMemset(h->pcg_d.p, 0, h->pcg_d.bytes));
@@ -271,6 +272,7 @@ PcgState pcg_state(tf_handle* h, int ncol) {
   st.rzo = d + 5 * c;
   st.beta = d + 6 * c;
   st.wscale = d + 7 * c;
+  st.rtrue = d + 8 * c;
   int* i = h->pcg_i.as<int>();
   st.active = i + 0 * c;
   st.cand = i + 1 * c;
@@ -801,29 +803,32 @@ void ensure_coarse_work(tf_handle* h, Hierarchy& hy, int ncol) {
 // ----------------------------------------------------------------- PCG ------
 
 // z = M r for the active columns: r scaled by its column max into the work precision, one cycle,
-// and the new search direction p.  Before the first application (initial) the scale is formed here;
-// afterwards pcg_update_kernel / pcg_retire_kernel have formed it.  z is stored only with store_z.
-template <typename T>
-void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int initial, bool store_z, cudaStream_t s) {
+// and the new search direction p.  With `prep` the scale is formed here; otherwise pcg_take_kernel /
+// pcg_update_kernel / pcg_retire_kernel have formed it.  z is stored only with store_z.  R is the
+// type of the PCG vectors r and p (double, or float in the mixed PCG).
+template <typename T, typename R>
+void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int initial, bool store_z, cudaStream_t s,
+                  bool prep = false) {
   const long long n = 3 * h->geo[0].nnode;
   VBufs<T>& vb = vbufs<T>(h);
+  R* r = static_cast<R*>(h->vr.p);
   dim3 gr(grid_for(n, RED_THREADS, PCG_BLOCKS), ncol);
   {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  if (initial) {
-    pcg_prep_kernel<<<gr, RED_THREADS, 0, s>>>(h->vr.as<double>(), n, st);
+  if (prep) {
+    pcg_prep_kernel<R><<<gr, RED_THREADS, 0, s>>>(r, n, st);
     TF_LAUNCH_CHECK("pcg_prep_kernel");
   }
-  pcg_to_work_kernel<T><<<cols_grid(n, ncol), 256, 0, s>>>(h->vr.as<double>(), n, st, vb.b[0].template as<T>());
+  pcg_to_work_kernel<T, R><<<cols_grid(n, ncol), 256, 0, s>>>(r, n, st, vb.b[0].template as<T>());
   TF_LAUNCH_CHECK("pcg_to_work_kernel");
   }
   vcycle<T>(h, hy, vb, 0, ncol, st.active, s);
   {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  pcg_from_work_kernel<T><<<gr, RED_THREADS, 0, s>>>(vb.x[0].template as<T>(), h->vr.as<double>(),
-                                                    store_z ? h->vz.as<double>() : nullptr, n, st, initial);
+  pcg_from_work_kernel<T, R><<<gr, RED_THREADS, 0, s>>>(vb.x[0].template as<T>(), r, store_z ? h->vz.as<double>() : nullptr, n, st,
+                                                        initial);
   TF_LAUNCH_CHECK("pcg_from_work_kernel");
-  pcg_direction_kernel<T><<<cols_grid(n, ncol), 256, 0, s>>>(vb.x[0].template as<T>(), h->vp.as<double>(), n, st, initial);
+  pcg_direction_kernel<T, R><<<cols_grid(n, ncol), 256, 0, s>>>(vb.x[0].template as<T>(), static_cast<R*>(h->vp.p), n, st, initial);
   TF_LAUNCH_CHECK("pcg_direction_kernel");
   }
 }
@@ -845,6 +850,26 @@ void fine_apply64(tf_handle* h, Hierarchy& hy, const double* u, const double* b,
   launch_level<double>(h, 0, a, mode, s, TIMER_FINE64);
 }
 
+// FP32 fine operator with mask: the operator of the mixed PCG's FP32 iterations, on the CUDA-core
+// stencil whatever the smoother uses (its accuracy bounds how far an FP32 stretch can reduce the
+// residual between two FP64 recomputations).
+void fine_apply32(tf_handle* h, Hierarchy& hy, const float* u, float* y, int ncol, const int* active, cudaStream_t s) {
+  LevelArgs<float> a{};
+  a.g = h->geo[0];
+  a.E = h->modulif.as<float>();
+  a.mask = hy.lv[0].mask.as<uint8_t>();
+  a.u = u;
+  a.y = y;
+  a.colstride = 3 * a.g.nnode;
+  a.ncol = ncol;
+  a.active = active;
+  TimedRange tr(h->timers, TIMER_PCG32, s);
+  const int tc = h->s.tensor_cores;
+  h->s.tensor_cores = 0;
+  struct Restore { tf_handle* h; int v; ~Restore() { h->s.tensor_cores = v; } } restore{h, tc};
+  launch_fine<float>(h, a, MODE_APPLY, s);
+}
+
 struct PcgResult {
   std::vector<int> iters;
   std::vector<double> rel;
@@ -854,14 +879,27 @@ struct PcgResult {
 
 // Batched flexible PCG over `ncol` columns held in h->vb (rhs) / h->vx (solution).
 // `run` selects the columns; with `warm` the current h->vx is the start vector.
-template <typename T>
+//
+// R = double: the reference's FP64 PCG (FP64 operator, FP64 vectors).  R = float: the mixed PCG.
+// Its iterations run in FP32 (r, p, q and the operator), while x accumulates in FP64 and the
+// residual is recomputed in FP64 (b - K x, the FP64 operator) whenever a column's iterated
+// residual fell by the factor settings.reliable since its last recomputation, or below the
+// tolerance; the recomputed residual replaces the FP32 one (a reliable update) and decides
+// convergence, so every column still converges on its FP64 true residual like the reference.
+template <typename T, typename R>
 PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run, bool warm, cudaStream_t s) {
+  constexpr bool mixed = std::is_same<R, float>::value;
   const long long n = 3 * h->geo[0].nnode;
   ensure_vbufs<T>(h, ncol);
   ensure_coarse_work(h, hy, ncol);
   PcgState st = pcg_state(h, ncol);
   const double tol = h->s.tolerance;
+  const double reliable = mixed ? h->s.reliable : 0.0;
   const int limit = h->s.max_iterations;
+  R* r = static_cast<R*>(h->vr.p);
+  R* p = static_cast<R*>(h->vp.p);
+  R* q = mixed ? static_cast<R*>(h->vz.p) : static_cast<R*>(h->vq.p);
+  double* t = h->vq.as<double>();   // b - K x in FP64 (shares vq with q in the FP64 PCG: q is consumed first)
   std::vector<int> zeros(ncol, 0);
   TF_CUDA_CHECK(cudaMemcpyAsync(st.active, run.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, s));
   TF_CUDA_CHECK(cudaMemcpyAsync(st.cand, zeros.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, s));
@@ -872,34 +910,41 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
   dim3 ge = cols_grid(n, ncol);
   pcg_norm_kernel<<<gr, RED_THREADS, 0, s>>>(h->vb.as<double>(), n, st, st.bnorm, 1);
   TF_LAUNCH_CHECK("pcg_norm_kernel");
+  const double* start = h->vb.as<double>();
   if (warm) {
-    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vr.as<double>(), MODE_RESID, ncol, st.active, nullptr, s);
+    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), t, MODE_RESID, ncol, st.active, nullptr, s);
+    start = t;
   } else {
     zero_cols_kernel<double><<<ge, 256, 0, s>>>(h->vx.as<double>(), n, st.active);
     TF_LAUNCH_CHECK("zero_cols_kernel");
-    TF_CUDA_CHECK(cudaMemcpyAsync(h->vr.p, h->vb.p, sizeof(double) * n * ncol, cudaMemcpyDeviceToDevice, s));
   }
-  precondition<T>(h, hy, ncol, st, 1, false, s);
+  {
+    TimedRange tr_(h->timers, TIMER_VECTOR, s);
+    pcg_take_kernel<R><<<gr, RED_THREADS, 0, s>>>(start, r, n, st);
+    TF_LAUNCH_CHECK("pcg_take_kernel");
+  }
+  precondition<T, R>(h, hy, ncol, st, 1, false, s);
   int step = 0;
   int n_active = 0;
   for (int c = 0; c < ncol; ++c) n_active += run[c];
   while (n_active > 0 && step < limit) {
-    fine_apply64(h, hy, h->vp.as<double>(), nullptr, h->vq.as<double>(), MODE_APPLY, ncol, st.active, nullptr, s);
+    if constexpr (mixed) fine_apply32(h, hy, p, q, ncol, st.active, s);
+    else fine_apply64(h, hy, p, nullptr, q, MODE_APPLY, ncol, st.active, nullptr, s);
     {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  pcg_alpha_kernel<<<gr, RED_THREADS, 0, s>>>(h->vp.as<double>(), h->vq.as<double>(), n, st);
+  pcg_alpha_kernel<R><<<gr, RED_THREADS, 0, s>>>(p, q, n, st);
     TF_LAUNCH_CHECK("pcg_alpha_kernel");
     ++step;
-    pcg_update_kernel<T><<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), h->vr.as<double>(), h->vp.as<double>(),
-                                                    h->vq.as<double>(), vbufs<T>(h).x[0].template as<T>(), n, st, tol, step);
+    pcg_update_kernel<T, R><<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), r, p, q, vbufs<T>(h).x[0].template as<T>(), n, st, tol,
+                                                       step, reliable);
     TF_LAUNCH_CHECK("pcg_update_kernel");
   }
-    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vq.as<double>(), MODE_RESID, ncol, st.active, st.flags, s);
+    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), t, MODE_RESID, ncol, st.active, st.flags, s);
     {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  pcg_truecheck_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), n, st, tol, step);
+  pcg_truecheck_kernel<<<gr, RED_THREADS, 0, s>>>(t, n, st, tol, step);
     TF_LAUNCH_CHECK("pcg_truecheck_kernel");
-    pcg_retire_kernel<T><<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), h->vr.as<double>(), vbufs<T>(h).x[0].template as<T>(), n, st);
+    pcg_retire_kernel<T, R><<<gr, RED_THREADS, 0, s>>>(t, r, vbufs<T>(h).x[0].template as<T>(), n, st);
     TF_LAUNCH_CHECK("pcg_retire_kernel");
     pcg_flags_kernel<<<1, 256, 0, s>>>(st, step);
     TF_LAUNCH_CHECK("pcg_flags_kernel");
@@ -908,14 +953,14 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
     n_active = h->host_flags[0];
     if (n_active == 0) break;
-    precondition<T>(h, hy, ncol, st, 0, false, s);
+    precondition<T, R>(h, hy, ncol, st, 0, false, s);
   }
   PcgResult res;
   res.steps = step;
   if (n_active > 0) {
     // iteration limit: final true residual of the columns still running (topology_multigrid.py:450-453)
-    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), h->vq.as<double>(), MODE_RESID, ncol, st.active, nullptr, s);
-    pcg_norm_kernel<<<gr, RED_THREADS, 0, s>>>(h->vq.as<double>(), n, st, st.rzo, 1);
+    fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), t, MODE_RESID, ncol, st.active, nullptr, s);
+    pcg_norm_kernel<<<gr, RED_THREADS, 0, s>>>(t, n, st, st.rzo, 1);
     TF_LAUNCH_CHECK("pcg_norm_kernel");
   }
   std::vector<int> act(ncol), it(ncol);
@@ -951,7 +996,7 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
 
 // Precise FP64 re-run of the columns that missed the tolerance (topology_multigrid.py:376-406).
 PcgResult pcg_precise(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run, cudaStream_t s) {
-  return pcg<double>(h, hy, ncol, run, true, s);
+  return pcg<double, double>(h, hy, ncol, run, true, s);
 }
 
 template <typename F>
@@ -986,6 +1031,11 @@ void validate_settings(const tf_settings& s) {
   require(std::isfinite(s.tolerance) && s.tolerance > 0, "tolerance must be positive");
   require(std::isfinite(s.dead_ratio) && s.dead_ratio >= 0, "dead_ratio must be non-negative");
   require(std::isfinite(s.zero_rhs) && s.zero_rhs >= 0, "zero_rhs must be non-negative");
+  require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.pcg_precision == TF_PRECISION_FLOAT32,
+          "pcg_precision must be float64 or float32");
+  require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.precision == TF_PRECISION_FLOAT32,
+          "float32 PCG iterations need the float32 work precision");
+  require(std::isfinite(s.reliable) && s.reliable > 0 && s.reliable < 1, "reliable must be in (0, 1)");
 }
 
 }  // namespace
@@ -1019,6 +1069,8 @@ extern "C" int tf_default_settings(tf_settings* s) {
   s->tolerance = 1e-8;
   s->dead_ratio = 1e-12;
   s->zero_rhs = 1e-12;
+  s->reliable = 0.01;
+  s->pcg_precision = TF_PRECISION_FLOAT64;
   return TF_OK;
 }
 
@@ -1261,7 +1313,9 @@ int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, do
         TF_LAUNCH_CHECK("pad_kernel");
       }
       std::vector<int> run(nc, 1);
-      PcgResult r = work_is_double(h) ? pcg<double>(h, hy, nc, run, warm, s) : pcg<float>(h, hy, nc, run, warm, s);
+      PcgResult r = work_is_double(h) ? pcg<double, double>(h, hy, nc, run, warm, s)
+                    : (h->s.pcg_precision == TF_PRECISION_FLOAT32 ? pcg<float, float>(h, hy, nc, run, warm, s)
+                                                                  : pcg<float, double>(h, hy, nc, run, warm, s));
       history.insert(history.end(), r.history.begin(), r.history.end());
       steps += r.steps;
       for (int attempt = 0; attempt < h->s.retries; ++attempt) {
@@ -1375,10 +1429,10 @@ extern "C" int tf_precondition(tf_handle* h, uint64_t key, const double* r_dev, 
     TF_LAUNCH_CHECK("pad_kernel");
     if (work_is_double(h)) {
       ensure_vbufs<double>(h, nrhs);
-      precondition<double>(h, hy, nrhs, st, 1, true, s);
+      precondition<double, double>(h, hy, nrhs, st, 1, true, s, true);
     } else {
       ensure_vbufs<float>(h, nrhs);
-      precondition<float>(h, hy, nrhs, st, 1, true, s);
+      precondition<float, double>(h, hy, nrhs, st, 1, true, s, true);
     }
     unpad_kernel<<<cols_grid(h->un.nnode, nrhs), 256, 0, s>>>(h->vz.as<double>(), h->un, h->geo[0], z_dev, nun, nullptr);
     TF_LAUNCH_CHECK("unpad_kernel");

@@ -1,15 +1,17 @@
-"""Drop-in ``CudaDirectSolver`` (dense FP64 Cholesky on the device).
+"""Drop-in ``CudaDirectSolver`` (FP64 Cholesky on the device).
 
 Same constructor, methods and attributes as the reference's cuDSS wrapper
 (deep_frame/topology_optimization.py:80-244): ``CudaDirectSolver(matrix,
 rhs)`` runs the structure analysis, ``solve(matrix, rhs)`` refactors the
 values and solves, ``substitute(rhs)`` reuses the factor, ``same_structure``,
 ``diagnostics`` and ``close() -> list of cleanup errors``; device buffers are
-exposed as ``rhs_device`` / ``solution_device``.  The factorisation is a dense
-blocked Cholesky of the (symmetrised) matrix in libtfb200.so, so it serves
-systems up to 32768 unknowns; larger systems belong on the multigrid solver.
-Invalid input raises ValueError like the reference; a non-positive-definite
-matrix raises RuntimeError.
+exposed as ``rhs_device`` / ``solution_device``.  The factorisation runs in
+libtfb200.so on the (symmetrised) matrix: banded when its band is much smaller
+than the dense matrix (a voxel grid's reduced stiffness in its natural order,
+bandwidth about 3 (ny + 1)(nz + 1); the band may take up to 96 GB), dense with
+an explicit inverse factor otherwise (at most 32768 unknowns).  Invalid input
+raises ValueError like the reference; a non-positive-definite matrix raises
+RuntimeError.
 """
 import ctypes
 from time import perf_counter
@@ -37,8 +39,6 @@ class CudaDirectSolver:
             raise ValueError("direct solver requires a nonempty two-dimensional RHS matching the matrix")
         if not np.all(np.isfinite(matrix.data)) or not np.all(np.isfinite(rhs)):
             raise ValueError("direct solver matrix and RHS must be finite")
-        if matrix.shape[0] > 32768:
-            raise ValueError("the dense device factorisation handles at most 32768 unknowns; use linear_solver='multigrid'")
         self.lib = _lib.load()
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.shape = matrix.shape
@@ -104,7 +104,7 @@ class CudaDirectSolver:
 
     def diagnostics(self):
         props = self.torch.cuda.get_device_properties(self.device)
-        return {"precision": "float64", "numeric_factorization": "dense blocked Cholesky with explicit inverse factor (sm_100a)",
+        return {"precision": "float64", "numeric_factorization": "banded or dense blocked Cholesky (sm_100a), chosen by the bandwidth",
                 "device_name": props.name, "analysis_s": self.analysis_s, "shape": list(self.shape), "nnz": len(self.indices),
                 "device_total_bytes": props.total_memory, "solves": self.timings}
 

@@ -72,6 +72,11 @@ typedef struct tf_settings {
   double tolerance;           /* relative residual of the recomputed true residual */
   double dead_ratio;          /* coarse dofs with diag <= dead_ratio * max(diag) are dropped */
   double zero_rhs;            /* columns with norm <= zero_rhs * max norm are skipped */
+  double reliable;            /* mixed PCG: the FP64 residual is recomputed once a column's iterated residual fell by this
+                                 factor since the last recomputation (0 < reliable < 1) */
+  int32_t pcg_precision;      /* TF_PRECISION_FLOAT64: the reference's FP64 PCG.  TF_PRECISION_FLOAT32 (with the FP32 work
+                                 precision): FP32 PCG iterations and operator, x in FP64, FP64 true residuals replacing the
+                                 iterated one (reliable updates) and deciding convergence; no counterpart in the reference */
 } tf_settings;
 
 /* Solve report (deep_frame/topology_multigrid.py:367-373).  Arrays are caller-owned. */

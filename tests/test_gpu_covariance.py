@@ -82,8 +82,8 @@ def test_combine_matches_host_product(cuda):
     assert np.max(np.abs(out.cpu().numpy() - expected)) < 1e-12 * np.max(np.abs(expected))
 
 
-@pytest.mark.parametrize("precision", ["float32", "float64"])
-def test_benchmark_plate_matches_fp64_oracle(cuda, precision):
+@pytest.mark.parametrize("precision,pcg", [("float32", "float64"), ("float64", "float64"), ("float32", "float32")])
+def test_benchmark_plate_matches_fp64_oracle(cuda, precision, pcg):
     """The benchmark workload itself (96 x 96 x 16 plate, seed 0, 2 x 42 columns solved to the
     benchmark's 1e-8) against the FP64 oracle of tests/golden/plate_96x96x16.npz (the oracle's
     GMG-PCG to 1e-10; made by tests/golden/make_plate_oracle.py): tr and lambda_max within 1e-6
@@ -94,7 +94,7 @@ def test_benchmark_plate_matches_fp64_oracle(cuda, precision):
     from deep_frame_b200.elasticity import HexElasticity
     ref = np.load(Path(__file__).resolve().parent / "golden" / "plate_96x96x16.npz")
     domain, density, cov = problems.plate((96, 96, 16), 0)
-    system = HexElasticity(domain, multigrid={"precision": precision, "tolerance": 1e-8})
+    system = HexElasticity(domain, multigrid={"precision": precision, "pcg_precision": pcg, "tolerance": 1e-8})
     model = InterfaceCovariance(system, cov, domain["interfaces"])
     rows = {row["name"]: row for row in model.measure_device(density, 3.0, 1e-9)}
     assert rows["load_mean"]["value"] == pytest.approx(float(ref["tr"]), rel=1e-6)

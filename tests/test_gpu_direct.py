@@ -109,3 +109,54 @@ def test_system_solve_matches_reference_superlu_golden(cuda):
     assert np.linalg.norm(result["derivative"] - g["derivative"]) < 1e-5 * np.linalg.norm(g["derivative"])
     assert result["max_displacement_mm"] == pytest.approx(float(g["max_displacement"]), rel=1e-6)
     system.close()
+
+
+def test_direct_system_solve_of_config_one_matches_reference_superlu(cuda):
+    """linear_solver="cuda_cudss" on the config-1 cantilever (48 x 24 x 24, 91 875 dofs: the banded
+    factorisation, bandwidth about 3 x 25 x 25): compliance within 1e-6 and sensitivities within
+    1e-5 of the reference's SuperLU golden."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "cantilever_48x24x24.npz")
+    system, _ = _system((48, 24, 24), 0, "cuda_cudss")
+    result = system.solve(g["density"], 3.0, 1e-9, metrics=True)["tip"]
+    assert result["compliance_n_mm"] == pytest.approx(float(g["compliance"]), rel=1e-6)
+    assert np.linalg.norm(result["derivative"] - g["derivative"]) < 1e-5 * np.linalg.norm(g["derivative"])
+    assert result["max_displacement_mm"] == pytest.approx(float(g["max_displacement"]), rel=1e-6)
+    assert system.diagnostics()["gpu_solver_details"][0]["shape"][0] > 32768
+    assert system.close() == []
+
+
+@pytest.mark.parametrize("n,bw", [(200, 3), (600, 64), (1000, 65), (4000, 130)])
+def test_banded_factorisation_sizes_around_block_edges(cuda, n, bw):
+    """Band matrices whose bandwidth is below, at and beyond the 64-wide block columns, with a last
+    partial block: the banded path against NumPy, three right-hand sides."""
+    from scipy.sparse import diags
+    from deep_frame_b200.direct import CudaDirectSolver
+    rng = np.random.default_rng(n + bw)
+    bands = [rng.standard_normal(n - k) for k in range(bw + 1)]
+    lower = diags(bands, [-k for k in range(bw + 1)], shape=(n, n)).toarray()
+    a = lower @ lower.T + 0.1 * np.eye(n)
+    a[np.abs(np.subtract.outer(np.arange(n), np.arange(n))) > bw] = 0.0
+    a += np.diag(np.abs(a).sum(axis=1))          # diagonally dominant: SPD with the band kept
+    from scipy.sparse import csr_matrix
+    rhs = rng.standard_normal((n, 3))
+    solver = CudaDirectSolver(csr_matrix(a), rhs)
+    x = solver.solve(csr_matrix(a), rhs)
+    want = np.linalg.solve(a, rhs)
+    assert np.linalg.norm(x - want) <= 1e-10 * np.linalg.norm(want)
+    assert solver.close() == []
+
+
+def test_banded_factorisation_reports_the_failing_pivot(cuda):
+    """A diagonally dominant tridiagonal matrix with one negative diagonal entry at row 150 (third
+    block column of the banded path): "not positive definite (pivot 151)"."""
+    from scipy.sparse import diags
+    from deep_frame_b200.direct import CudaDirectSolver
+    n = 300
+    main = np.full(n, 4.0)
+    main[150] = -1.0
+    a = diags([np.full(n - 1, 0.5), main, np.full(n - 1, 0.5)], [-1, 0, 1], shape=(n, n)).tocsr()
+    solver = CudaDirectSolver(a, np.ones((n, 1)))
+    with pytest.raises(RuntimeError, match=r"pivot 151\)"):
+        solver.solve(a, np.ones((n, 1)))
+    solver.close()

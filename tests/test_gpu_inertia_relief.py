@@ -26,3 +26,20 @@ def test_relief_solves_match_reference(cuda, name, solver):
         assert np.linalg.norm(entry["derivative"] - ref) <= 1e-7 * np.linalg.norm(ref)
         assert entry["max_displacement_mm"] == pytest.approx(float(GOLDEN[f"{name}_{case_name}_max_displacement"]), rel=1e-7)
     assert not system.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_support_reactions_vanish_with_the_default_device_solver(cuda, name):
+    """HexElasticity.support_reactions with its default solver (the device direct solver, banded
+    for these grids): the d'Alembert loads balance every free-flying case, so the largest support
+    reaction is negligible against the applied nodal forces (the reference's check,
+    topology_optimization.py:570-580)."""
+    from deep_frame_b200.elasticity import HexElasticity
+    system = HexElasticity(domain_of(name))
+    for case_name in GOLDEN[f"{name}_cases"]:
+        case = next(c for c in system.cases if c["name"] == str(case_name))
+        if "inertia_relief" not in case:
+            continue
+        for part in system.support_reactions(GOLDEN[f"{name}_density"], str(case_name)):
+            assert part["max_reaction_n"] <= 1e-8 * part["nodal_force_sum_n"], part
+    assert not system.close()

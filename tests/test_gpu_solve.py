@@ -156,3 +156,40 @@ def test_tensor_core_vcycle_matches_cuda_core_vcycle(cuda, shape):
     assert max(runs[True]["iterations"]) <= 1.3 * max(runs[False]["iterations"]) + 2
     lam_tc, lam_cc = np.asarray(runs[True]["lambda_max"]), np.asarray(runs[False]["lambda_max"])
     assert np.max(np.abs(lam_tc / lam_cc - 1)) < 1e-2
+
+
+@pytest.mark.parametrize("shape,tolerance", [((24, 12, 10), 1e-10), ((16, 8, 16), 1e-8)])
+def test_mixed_pcg_converges_on_the_fp64_true_residual(cuda, shape, tolerance):
+    """pcg_precision = float32: FP32 iterations and operator with FP64 reliable residual updates.
+    Convergence is still decided on the FP64 true residual, so every column meets the tolerance and
+    equals the direct solution as closely as the FP64 PCG's; the iteration count stays close to the
+    FP64 PCG's on the same hierarchy."""
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    k0, _, moduli, fixed, force = cantilever(shape, 3)
+    rng = np.random.default_rng(5)
+    forces = np.column_stack([force, rng.normal(size=(force.size, 5))])
+    forces[fixed] = 0
+    expected = direct(shape, k0, moduli, fixed, forces)
+    runs = {}
+    for pcg in ("float64", "float32"):
+        mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 300, "precision": "float32", "tolerance": tolerance,
+                                                        "pcg_precision": pcg})
+        mg.update(moduli)
+        solution, report = mg.solve("c", fixed, forces)
+        assert report["converged"] and max(report["relative_residual"]) < tolerance, report
+        bar = 1e-7 if tolerance < 1e-9 else 1e-5
+        for c in range(forces.shape[1]):
+            assert np.linalg.norm(solution[:, c] - expected[:, c]) < bar * np.linalg.norm(expected[:, c])
+        residual = op.assemble(shape, k0, moduli) @ solution - forces
+        live = op.live_dofs(shape, moduli, fixed)
+        assert np.all(np.linalg.norm(residual[live], axis=0) < 1.01 * tolerance * np.linalg.norm(forces[live], axis=0))
+        runs[pcg] = report
+        mg.close()
+    assert max(runs["float32"]["iterations"]) <= 1.25 * max(runs["float64"]["iterations"]) + 2
+
+
+def test_mixed_pcg_rejects_a_float64_vcycle(cuda):
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    k0 = hex8.element_matrices((1, 1, 1), 0.3)[0]
+    with pytest.raises(ValueError, match="float32 work precision"):
+        GeometricMultigrid((8, 4, 4), (1, 1, 1), k0, {"precision": "float64", "pcg_precision": "float32"})
