@@ -56,6 +56,9 @@ def parse(argv=None):
     ap.add_argument("--tensor-cores", action="store_true", help="fast path's finest-level V-cycle applies on tcgen05")
     ap.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 arm (default min(steps, 3))")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 arm")
+    ap.add_argument("--storage-trial", default="", metavar="P1,P2",
+                    help="also time the fast path with these V-cycle storage precisions (bfloat16, float16: vectors rounded "
+                         "to 16 bits when stored) and report their PCG iterations")
     ap.add_argument("--e2e-steps", type=int, default=None, help="timed steps of the end-to-end leg (default min(steps, 3))")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -316,6 +319,22 @@ def ours(args):
         e_ms, grads, _ = timed_steps(e2e_step, e2e_steps, 1, 1, dist, device)
         result["e2e"] = {"ms": e_ms, "steps": e2e_steps, "h2d_bytes_per_step": int(moduli_host.nbytes),
                          "d2h_bytes_per_step": int(grads[0].nbytes + grads[1].nbytes + model.rank * model.rank * 8)}
+    if world == 1 and args.storage_trial:
+        # the same step with 16-bit V-cycle storage (the same schedule, tolerance and outer PCG)
+        result["storage_trial"] = {}
+        for precision in [p for p in args.storage_trial.split(",") if p]:
+            rebuild_multigrid(system, {**fast_settings(args), "precision": precision, "tensor_cores": False})
+            torch.cuda.empty_cache()
+            trial_mg, trial_step, _ = arm()
+            first = len(trial_mg.statistics) + len(groups)
+            try:
+                t_ms, (t_rows, _), _ = timed_steps(trial_step, min(args.steps, 2), 1, 1, dist, device)
+                stats = trial_mg.statistics[first:]
+                result["storage_trial"][precision] = {"s": round(t_ms / 1e3, 6), "pcg_iterations": [int(np.max(r["iterations"])) for r in stats[-len(groups):]],
+                                                      "converged": all(r["converged"] for r in stats),
+                                                      "tr": t_rows[0]["value"], "lambda_max": t_rows[1]["value"]}
+            except (RuntimeError, ValueError) as exc:
+                result["storage_trial"][precision] = {"error": f"{type(exc).__name__}: {exc}"}
     if world == 1 and not args.no_plain:
         # the plain FP64 GMG-PCG drop-in on the same GPU: FP64 V-cycle and FP64 PCG, the same smoother
         # schedule, hierarchy depth and tolerance
@@ -717,6 +736,10 @@ def main():
             "pcg_iterations": plain["iterations_max"], "converged": plain["converged"], "clocks": plain["clocks"],
             "path": "FP64 V-cycle, FP64 PCG, CUDA-core operators, same schedule and tolerance",
             "fast_vs_plain": agreement(fast, row_values(plain["rows"]))}
+    if "storage_trial" in result:
+        line["results"]["storage_trial"] = {
+            "what": "V-cycle vectors rounded to 16 bits when stored (FP32 buffers and arithmetic), FP64 outer PCG; same schedule",
+            **{p: ({**r, "tr_rel_to_value": abs(r["tr"] / fast["tr"] - 1)} if "tr" in r else r) for p, r in result["storage_trial"].items()}}
     parity = oracle_errors(args.config, fast)
     if parity:
         line["results"]["vs_fp64_oracle"] = parity

@@ -8,6 +8,8 @@
 // elements around it, so no atomics and no scatter conflicts are needed and
 // every write is coalesced along z.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -142,6 +144,18 @@ __device__ __forceinline__ void fine_node(const K0Param<T>& K, const Geo& g, con
   }
 }
 
+// Storage rounding of the work-precision V-cycle vectors: 0 none, 1 bfloat16, 2 float16.  With a
+// 16-bit storage precision every V-cycle vector value is rounded to that format (round to nearest)
+// when it is stored, while the arithmetic stays FP32: the vectors then hold exactly what 16-bit
+// buffers would, so the solver's iteration counts are those of 16-bit storage (the buffers
+// themselves stay FP32).
+__device__ __forceinline__ float round_store(float v, int mode) {
+  if (mode == 1) return __bfloat162float(__float2bfloat16_rn(v));
+  if (mode == 2) return __half2float(__float2half_rn(v));
+  return v;
+}
+__device__ __forceinline__ double round_store(double v, int) { return v; }
+
 // Epilogue modes of the level operators.
 enum ApplyMode : int {
   MODE_APPLY = 0,   // y = mask * A u
@@ -166,6 +180,7 @@ struct LevelArgs {
   const int* active;     // optional per-column flag; inactive columns are skipped
   const int* gate;       // optional device flag; the whole launch is skipped while *gate == 0
   T s, c1, c2;           // epilogue scalars
+  int round;             // storage rounding of the outputs (round_store mode)
 };
 
 template <typename T>
@@ -177,17 +192,17 @@ __device__ __forceinline__ void epilogue(const LevelArgs<T>& a, int mode, long l
     const bool live = (m >> q) & 1u;
     const long long d = d0 + q;
     if (mode == MODE_APPLY) {
-      a.y[d] = live ? av[q] : T(0);
+      a.y[d] = round_store(live ? av[q] : T(0), a.round);
     } else if (mode == MODE_RESID) {
-      a.y[d] = live ? (a.b[d] - av[q]) : T(0);
+      a.y[d] = round_store(live ? (a.b[d] - av[q]) : T(0), a.round);
     } else if (mode == MODE_JACOBI) {
-      a.y[d] = a.u[d] + a.s * a.inv[3 * node + q] * (a.b[d] - (live ? av[q] : T(0)));
+      a.y[d] = round_store(a.u[d] + a.s * a.inv[3 * node + q] * (a.b[d] - (live ? av[q] : T(0))), a.round);
     } else {  // MODE_CHEB
-      const T r = a.res[d] - (live ? av[q] : T(0));
-      const T dn = a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r;
+      const T r = round_store(a.res[d] - (live ? av[q] : T(0)), a.round);
+      const T dn = round_store(a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r, a.round);
       a.res[d] = r;
       a.y[d] = dn;
-      a.x[d] += dn;
+      a.x[d] = round_store(a.x[d] + dn, a.round);
     }
   }
 }
@@ -224,17 +239,17 @@ __device__ __forceinline__ void epilogue_pre(const LevelArgs<T>& a, int mode, lo
     const bool live = (m >> q) & 1u;
     const long long d = d0 + q;
     if (mode == MODE_APPLY) {
-      a.y[d] = live ? av[q] : T(0);
+      a.y[d] = round_store(live ? av[q] : T(0), a.round);
     } else if (mode == MODE_RESID) {
-      a.y[d] = live ? (in.v[0][q] - av[q]) : T(0);
+      a.y[d] = round_store(live ? (in.v[0][q] - av[q]) : T(0), a.round);
     } else if (mode == MODE_JACOBI) {
-      a.y[d] = a.u[d] + a.s * a.inv[3 * node + q] * (in.v[0][q] - (live ? av[q] : T(0)));
+      a.y[d] = round_store(a.u[d] + a.s * a.inv[3 * node + q] * (in.v[0][q] - (live ? av[q] : T(0))), a.round);
     } else {  // MODE_CHEB
-      const T r = in.v[0][q] - (live ? av[q] : T(0));
-      const T dn = a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r;
+      const T r = round_store(in.v[0][q] - (live ? av[q] : T(0)), a.round);
+      const T dn = round_store(a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r, a.round);
       a.res[d] = r;
       a.y[d] = dn;
-      a.x[d] = in.v[1][q] + dn;
+      a.x[d] = round_store(in.v[1][q] + dn, a.round);
     }
   }
 }
@@ -661,7 +676,7 @@ __global__ void __launch_bounds__(128) energy_kernel(const __grid_constant__ K0P
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void restrict_kernel(Geo fine, Geo coarse, const T* __restrict__ r, long long fstride, T* __restrict__ out,
-                                long long cstride, const uint8_t* __restrict__ cmask, const int* __restrict__ active) {
+                                long long cstride, const uint8_t* __restrict__ cmask, const int* __restrict__ active, int round) {
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const T* rc = r + col * fstride;
@@ -689,16 +704,16 @@ __global__ void restrict_kernel(Geo fine, Geo coarse, const T* __restrict__ r, l
       }
     }
     const unsigned m = cmask ? cmask[n] : 7u;
-    oc[3 * n + 0] = (m & 1u) ? acc0 : T(0);
-    oc[3 * n + 1] = (m & 2u) ? acc1 : T(0);
-    oc[3 * n + 2] = (m & 4u) ? acc2 : T(0);
+    oc[3 * n + 0] = (m & 1u) ? round_store(acc0, round) : T(0);
+    oc[3 * n + 1] = (m & 2u) ? round_store(acc1, round) : T(0);
+    oc[3 * n + 2] = (m & 4u) ? round_store(acc2, round) : T(0);
   }
 }
 
 // x_fine += mask * P c  (P = transpose of the restriction)
 template <typename T>
 __global__ void prolong_add_kernel(Geo fine, Geo coarse, const T* __restrict__ c, long long cstride, T* __restrict__ x,
-                                   long long fstride, const uint8_t* __restrict__ fmask, const int* __restrict__ active) {
+                                   long long fstride, const uint8_t* __restrict__ fmask, const int* __restrict__ active, int round) {
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const T* cc = c + col * cstride;
@@ -739,9 +754,9 @@ __global__ void prolong_add_kernel(Geo fine, Geo coarse, const T* __restrict__ c
       }
     }
     const unsigned m = fmask ? fmask[n] : 7u;
-    if (m & 1u) xc[3 * n + 0] += acc0;
-    if (m & 2u) xc[3 * n + 1] += acc1;
-    if (m & 4u) xc[3 * n + 2] += acc2;
+    if (m & 1u) xc[3 * n + 0] = round_store(xc[3 * n + 0] + acc0, round);
+    if (m & 2u) xc[3 * n + 1] = round_store(xc[3 * n + 1] + acc1, round);
+    if (m & 4u) xc[3 * n + 2] = round_store(xc[3 * n + 2] + acc2, round);
   }
 }
 

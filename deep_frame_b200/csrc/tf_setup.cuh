@@ -378,11 +378,11 @@ __global__ void coarsest_gather_kernel(const T* __restrict__ src, long long stri
 
 template <typename T>
 __global__ void coarsest_scatter_kernel(const double* __restrict__ src, const long long* __restrict__ live, int n,
-                                        T* __restrict__ dst, long long stride, const int* __restrict__ active) {
+                                        T* __restrict__ dst, long long stride, const int* __restrict__ active, int round) {
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    dst[col * stride + live[t]] = static_cast<T>(src[(long long)col * n + t]);
+    dst[col * stride + live[t]] = round_store(static_cast<T>(src[(long long)col * n + t]), round);
 }
 
 // ----------------------------------------------------------- elementwise ----
@@ -398,12 +398,12 @@ __global__ void zero_cols_kernel(T* __restrict__ v, long long stride, const int*
 // x = s * inv * b   (first Jacobi sweep from a zero guess)
 template <typename T>
 __global__ void jacobi_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x, T s,
-                                    const int* __restrict__ active) {
+                                    const int* __restrict__ active, int round) {
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const long long off = (long long)col * ndof;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x)
-    x[off + t] = s * inv[t] * b[off + t];
+    x[off + t] = round_store(s * inv[t] * b[off + t], round);
 }
 
 // Chebyshev start from a zero guess: res = b, d = inv * res / theta, x = d (with has_x: x += d, res
@@ -411,18 +411,18 @@ __global__ void jacobi_first_kernel(long long ndof, const T* __restrict__ inv, c
 template <typename T>
 __global__ void cheb_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ res,
                                   T* __restrict__ d, T* __restrict__ x, T inv_theta, int has_x, int write_rd,
-                                  const int* __restrict__ active) {
+                                  const int* __restrict__ active, int round) {
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const long long off = (long long)col * ndof;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x) {
     const T r = has_x ? res[off + t] : b[off + t];
-    const T dv = inv[t] * r * inv_theta;
+    const T dv = round_store(inv[t] * r * inv_theta, round);
     if (write_rd) {
       res[off + t] = r;
       d[off + t] = dv;
     }
-    x[off + t] = has_x ? x[off + t] + dv : dv;
+    x[off + t] = has_x ? round_store(x[off + t] + dv, round) : dv;
   }
 }
 
@@ -595,13 +595,13 @@ __global__ void pcg_prep_kernel(const R* __restrict__ r, long long n, PcgState s
 }
 
 template <typename T, typename R>
-__global__ void pcg_to_work_kernel(const R* __restrict__ r, long long n, PcgState st, T* __restrict__ w) {
+__global__ void pcg_to_work_kernel(const R* __restrict__ r, long long n, PcgState st, T* __restrict__ w, int round) {
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
   const double s = 1.0 / st.scale[col];
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    w[off + t] = static_cast<T>(static_cast<double>(r[off + t]) * s);
+    w[off + t] = round_store(static_cast<T>(static_cast<double>(r[off + t]) * s), round);
 }
 
 // rz = r . z with z = scale * w (w: the work-precision preconditioner output); beta = (rz - rzo) / rho

@@ -198,6 +198,11 @@ struct tf_handle {
 namespace {
 
 bool work_is_double(const tf_handle* h) { return h->s.precision == TF_PRECISION_FLOAT64; }
+// Storage rounding of the V-cycle vectors (round_store): 16-bit storage precisions keep FP32 buffers
+// and arithmetic and round every stored value to the 16-bit format.
+int store_round(const tf_handle* h) {
+  return h->s.precision == TF_PRECISION_BFLOAT16 ? 1 : (h->s.precision == TF_PRECISION_FLOAT16 ? 2 : 0);
+}
 
 // ------------------------------------------------------------ buffers -------
 
@@ -481,6 +486,7 @@ LevelArgs<T> level_args(tf_handle* h, Hierarchy& hy, int l, int ncol, const int*
   a.ncol = ncol;
   a.active = active;
   a.gate = nullptr;
+  a.round = std::is_same<T, float>::value ? store_round(h) : 0;
   return a;
 }
 
@@ -505,7 +511,7 @@ void coarsest_solve(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int ncol, const i
   if (h->trimul_work.bytes < need) h->trimul_work.alloc(need);
   dense_trimul(hy.X.as<double>(), h->cb.as<double>(), h->cy.as<double>(), n, ncol, 0, active, h->trimul_work.as<double>(), st);
   dense_trimul(hy.X.as<double>(), h->cy.as<double>(), h->cb.as<double>(), n, ncol, 1, active, h->trimul_work.as<double>(), st);
-  coarsest_scatter_kernel<T><<<g1, 256, 0, st>>>(h->cb.as<double>(), hy.live.as<long long>(), n, x, nd, active);
+  coarsest_scatter_kernel<T><<<g1, 256, 0, st>>>(h->cb.as<double>(), hy.live.as<long long>(), n, x, nd, active, store_round(h));
   TF_LAUNCH_CHECK("coarsest_scatter_kernel");
 }
 
@@ -523,7 +529,8 @@ void smooth(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, bool first, int nc
     const T step = static_cast<T>(s.damping / lam);
     int start = 0;
     if (first) {
-      jacobi_first_kernel<T><<<ge, 256, 0, st>>>(nd, a.inv, vb.b[l].template as<T>(), vb.x[l].template as<T>(), step, active);
+      jacobi_first_kernel<T><<<ge, 256, 0, st>>>(nd, a.inv, vb.b[l].template as<T>(), vb.x[l].template as<T>(), step, active,
+                                                  store_round(h));
       TF_LAUNCH_CHECK("jacobi_first_kernel");
       start = 1;
     }
@@ -550,7 +557,7 @@ void smooth(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, bool first, int nc
   // with one sweep nothing reads res or d afterwards (the V-cycle's next residual apply rewrites res)
   cheb_first_kernel<T><<<ge, 256, 0, st>>>(nd, a.inv, vb.b[l].template as<T>(), vb.res[l].template as<T>(),
                                            vb.d[l].template as<T>(), vb.x[l].template as<T>(), static_cast<T>(1.0 / theta),
-                                           first ? 0 : 1, count > 1 ? 1 : 0, active);
+                                           first ? 0 : 1, count > 1 ? 1 : 0, active, store_round(h));
   TF_LAUNCH_CHECK("cheb_first_kernel");
   for (int k = 1; k < count; ++k) {
     const double rn = 1.0 / (2.0 * sigma - rho);
@@ -586,14 +593,14 @@ void vcycle(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, int ncol, const in
     TimedRange tr(h->timers, TIMER_TRANSFER, st);
     restrict_kernel<T><<<cols_grid(cg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.res[l].template as<T>(), 3 * fg.nnode,
                                                                   vb.b[l + 1].template as<T>(), 3 * cg.nnode,
-                                                                  hy.lv[l + 1].mask.as<uint8_t>(), active);
+                                                                  hy.lv[l + 1].mask.as<uint8_t>(), active, store_round(h));
     TF_LAUNCH_CHECK("restrict_kernel");
     }
     vcycle<T>(h, hy, vb, l + 1, ncol, active, st);
     TimedRange tr(h->timers, TIMER_TRANSFER, st);
     prolong_add_kernel<T><<<cols_grid(fg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.x[l + 1].template as<T>(), 3 * cg.nnode,
                                                                      vb.x[l].template as<T>(), 3 * fg.nnode,
-                                                                     hy.lv[l].mask.as<uint8_t>(), active);
+                                                                     hy.lv[l].mask.as<uint8_t>(), active, store_round(h));
     TF_LAUNCH_CHECK("prolong_add_kernel");
   }
   smooth<T>(h, hy, vb, l, false, ncol, active, st);
@@ -819,7 +826,7 @@ void precondition(tf_handle* h, Hierarchy& hy, int ncol, const PcgState& st, int
     pcg_prep_kernel<R><<<gr, RED_THREADS, 0, s>>>(r, n, st);
     TF_LAUNCH_CHECK("pcg_prep_kernel");
   }
-  pcg_to_work_kernel<T, R><<<cols_grid(n, ncol), 256, 0, s>>>(r, n, st, vb.b[0].template as<T>());
+  pcg_to_work_kernel<T, R><<<cols_grid(n, ncol), 256, 0, s>>>(r, n, st, vb.b[0].template as<T>(), store_round(h));
   TF_LAUNCH_CHECK("pcg_to_work_kernel");
   }
   vcycle<T>(h, hy, vb, 0, ncol, st.active, s);
@@ -1015,7 +1022,8 @@ int guard(tf_handle* h, F&& f) {
 
 void validate_settings(const tf_settings& s) {
   require(s.precision >= TF_PRECISION_FLOAT64 && s.precision <= TF_PRECISION_FLOAT16, "invalid precision");
-  require(s.precision <= TF_PRECISION_FLOAT32, "bfloat16/float16 work precision is not available in this library");
+  require(s.precision <= TF_PRECISION_FLOAT32 || !s.tensor_cores,
+          "bfloat16/float16 storage runs on the CUDA-core operators (tensor_cores must be off)");
   require(s.smoother == TF_SMOOTHER_JACOBI || s.smoother == TF_SMOOTHER_CHEBYSHEV, "invalid smoother");
   require(s.cycle == TF_CYCLE_V || s.cycle == TF_CYCLE_W, "invalid cycle");
   require(s.coarse == TF_COARSE_GALERKIN, "only Galerkin coarse operators are available in this library");
@@ -1033,7 +1041,7 @@ void validate_settings(const tf_settings& s) {
   require(std::isfinite(s.zero_rhs) && s.zero_rhs >= 0, "zero_rhs must be non-negative");
   require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.pcg_precision == TF_PRECISION_FLOAT32,
           "pcg_precision must be float64 or float32");
-  require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.precision == TF_PRECISION_FLOAT32,
+  require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.precision != TF_PRECISION_FLOAT64,
           "float32 PCG iterations need the float32 work precision");
   require(std::isfinite(s.reliable) && s.reliable > 0 && s.reliable < 1, "reliable must be in (0, 1)");
 }

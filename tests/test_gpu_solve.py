@@ -193,3 +193,32 @@ def test_mixed_pcg_rejects_a_float64_vcycle(cuda):
     k0 = hex8.element_matrices((1, 1, 1), 0.3)[0]
     with pytest.raises(ValueError, match="float32 work precision"):
         GeometricMultigrid((8, 4, 4), (1, 1, 1), k0, {"precision": "float64", "pcg_precision": "float32"})
+
+
+@pytest.mark.parametrize("precision", ["bfloat16", "float16"])
+def test_sixteen_bit_vcycle_storage_still_converges_to_the_fp64_answer(cuda, precision):
+    """bfloat16 / float16 work precision: every V-cycle vector rounded to the 16-bit format when
+    stored (FP32 arithmetic, FP64 outer PCG).  The preconditioner is weaker, never the answer: the
+    solution still equals the direct solve to the tolerance."""
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    shape = (24, 12, 10)
+    k0, _, moduli, fixed, force = cantilever(shape, 3)
+    rng = np.random.default_rng(9)
+    forces = np.column_stack([force, rng.normal(size=(force.size, 2))])
+    forces[fixed] = 0
+    expected = direct(shape, k0, moduli, fixed, forces)
+    mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 300, "precision": precision, "tolerance": 1e-10,
+                                                    "max_iterations": 3000})
+    mg.update(moduli)
+    solution, report = mg.solve("c", fixed, forces)
+    assert report["converged"], report
+    for c in range(forces.shape[1]):
+        assert np.linalg.norm(solution[:, c] - expected[:, c]) < 1e-7 * np.linalg.norm(expected[:, c])
+    mg.close()
+
+
+def test_sixteen_bit_storage_refuses_the_tensor_core_apply(cuda):
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    k0 = hex8.element_matrices((1, 1, 1), 0.3)[0]
+    with pytest.raises(ValueError, match="tensor_cores"):
+        GeometricMultigrid((8, 4, 4), (1, 1, 1), k0, {"precision": "bfloat16", "tensor_cores": True})
