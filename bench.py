@@ -191,7 +191,7 @@ def rebuild_multigrid(system, multigrid):
     if system.multigrid is not None:
         system.multigrid.close()
         system.multigrid = None
-    system.multigrid_settings = {**(system.multigrid_settings or {}), **multigrid}
+    system.multigrid_settings = {**(system.multigrid_settings or {}), "max_iterations": 2000, "retries": 2, **multigrid}
     system.multigrid_settings.pop("_tuned", None)
 
 
@@ -323,7 +323,9 @@ def ours(args):
         # the same step with 16-bit V-cycle storage (the same schedule, tolerance and outer PCG)
         result["storage_trial"] = {}
         for precision in [p for p in args.storage_trial.split(",") if p]:
-            rebuild_multigrid(system, {**fast_settings(args), "precision": precision, "tensor_cores": False})
+            # capped: a storage precision that stalls the PCG is reported unconverged instead of running 2000 iterations
+            rebuild_multigrid(system, {**fast_settings(args), "precision": precision, "tensor_cores": False, "max_iterations": 300,
+                                       "retries": 0})
             torch.cuda.empty_cache()
             trial_mg, trial_step, _ = arm()
             first = len(trial_mg.statistics) + len(groups)

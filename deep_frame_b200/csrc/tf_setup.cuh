@@ -486,6 +486,10 @@ __global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, con
     st.rel[col] = rel;
     st.scale[col] = fmax(mx, 1e-300);
     st.rzo[col] = d;
+    if (!isfinite(rel)) {
+      st.cand[col] = 4;   // breakdown (a non-finite residual): the column stops and is reported unconverged
+      return;
+    }
     atomicMax(&st.hist[step - 1], static_cast<unsigned long long>(__double_as_longlong(rel)));
     if (rel < tol || (reliable > 0.0 && rel < reliable * st.rtrue[col])) { st.cand[col] = 1; atomicExch(&st.flags[0], 1); }
   }
@@ -496,7 +500,7 @@ __global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, con
 // column converges when ||t|| / ||b|| < tol, the others continue from t.
 __global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, long long n, PcgState st, double tol, int step) {
   const int col = blockIdx.y;
-  if (!st.flags[0] || !st.active[col]) return;
+  if (!st.flags[0] || !st.active[col] || st.cand[col] == 4) return;
   const long long off = (long long)col * n;
   double a = 0.0, z = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -540,7 +544,7 @@ __global__ void pcg_flags_kernel(PcgState st, int step) {
   int n_active = 0;
   for (int col = threadIdx.x; col < st.ncol; col += blockDim.x) {
     if (st.active[col]) {
-      if (st.cand[col] == 2) {
+      if (st.cand[col] == 2 || st.cand[col] == 4) {   // converged, or broken down (its rel stays non-finite)
         st.active[col] = 0;
         st.iters[col] = step;
       }
