@@ -1,8 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own Python code.
 
-Run in a container that has the reference source tree:
+Run where the reference source tree is available, passing its path (required):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py PATH_TO_REFERENCE [--only=NAME,...] [--skip-config1]
 
 The reference tree is copied to a scratch directory (its mount is read-only and
 pytest/pycache write files), imported, and run on the CPU: SciPy SuperLU for the
@@ -420,4 +420,6 @@ def main(source):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--") else "/root/reference")
+    if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
+        sys.exit("usage: python tests/golden/make_golden.py PATH_TO_REFERENCE [--only=NAME,...] [--skip-config1]")
+    main(sys.argv[1])

@@ -44,3 +44,22 @@ def test_static_scratch_gram_rejects_oversized_requests(cuda):
     out = torch.zeros((64, 64), dtype=torch.float64, device=cuda)
     assert lib.tf_gram_static(_lib.ptr(a), 64, _lib.ptr(a), 64, 8, _lib.ptr(out), None) == 1
     assert b"exceeds the static scratch limit" in lib.tf_last_error(None)
+
+
+def test_static_scratch_gram_allocates_no_device_memory(cuda):
+    """After its first call on the device (which resolves the static array's address), further calls
+    leave the device's free memory unchanged: the entry point allocates nothing."""
+    import torch
+    from deep_frame_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(3)
+    a = torch.as_tensor(rng.normal(size=(42, 65537)), device=cuda)
+    out = torch.empty((42, 42), dtype=torch.float64, device=cuda)
+    assert lib.tf_gram_static(_lib.ptr(a), 42, _lib.ptr(a), 42, 65537, _lib.ptr(out), None) == 0
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert lib.tf_gram_static(_lib.ptr(a), 42, _lib.ptr(a), 42, 65537, _lib.ptr(out), None) == 0
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
