@@ -263,7 +263,7 @@ def ours(args):
             if rank != 0:
                 tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
                               candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps",
-                                                                                        "tensor_cores", "coarsest_dofs")}], repeats=1)
+                                                                                        "tensor_cores", "coarsest_dofs", "cycle")}], repeats=1)
 
     def arm():
         mg = system._multigrid()
@@ -298,7 +298,7 @@ def ours(args):
               "ndof": system.ndof, "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"],
               "converged": all(r["converged"] for r in timed),
               "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores",
-                                                                          "coarsest_dofs", "precision", "pcg_precision")},
+                                                                          "coarsest_dofs", "precision", "pcg_precision", "cycle")},
               "tuning": tuning, "rows": rows}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     result["dominant"] = dominant

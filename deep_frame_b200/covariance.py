@@ -247,7 +247,8 @@ class InterfaceCovariance:
 
     def measure_from(self, solved, scale, gradients=True, worst_gradient=True):
         """Rows of the reference's measure (topology_problem.py:657-684) from device solutions; the
-        sensitivities are sums of element energies formed on the device (``tf_element_energy``)."""
+        sensitivities are sums of element energies formed on the device (``tf_combine`` for the
+        eigenvector combinations, ``tf_element_energy`` for the energies)."""
         mg = self.system._multigrid()
         torch = mg.torch
         limits = self._limits()
@@ -260,8 +261,10 @@ class InterfaceCovariance:
             for _, ks, _, u, _ in solved:
                 mg.energy_device(u, coefficients=np.full(len(ks), self.factor), scale=scale, out=grad_mean, accumulate=True)
                 if worst_gradient:
-                    mg.energy_device(u, combination=spectrum.vectors[np.ix_(ks, kept)], coefficients=spectrum.weights[kept] * self.factor,
-                                     scale=scale, out=grad_worst, accumulate=True)
+                    # the KS-weighted eigenvector combinations U v_i formed once (tf_combine), then their energies
+                    combined = mg.combine_device(u, spectrum.vectors[np.ix_(ks, kept)])
+                    mg.energy_device(combined, coefficients=spectrum.weights[kept] * self.factor, scale=scale, out=grad_worst,
+                                     accumulate=True)
             mean_limit, worst_limit = limits["mean_n_mm"] or 1.0, limits["worst_n_mm"] or 1.0
             rows[0].update(g=spectrum.trace / mean_limit - 1, gradient=grad_mean / mean_limit)
             rows[1].update(g=float(spectrum.ks / worst_limit - 1), gradient=grad_worst / worst_limit if worst_gradient else None)

@@ -155,6 +155,12 @@ __device__ __forceinline__ float round_store(float v, int mode) {
   return v;
 }
 __device__ __forceinline__ double round_store(double v, int) { return v; }
+// compile-time form for the level operators: RND = 0 compiles to a plain store
+template <int RND, typename T>
+__device__ __forceinline__ T rs(T v) {
+  if constexpr (RND == 0) return v;
+  else return round_store(v, RND);
+}
 
 // Epilogue modes of the level operators.
 enum ApplyMode : int {
@@ -180,10 +186,10 @@ struct LevelArgs {
   const int* active;     // optional per-column flag; inactive columns are skipped
   const int* gate;       // optional device flag; the whole launch is skipped while *gate == 0
   T s, c1, c2;           // epilogue scalars
-  int round;             // storage rounding of the outputs (round_store mode)
+  int round;             // storage rounding of the outputs (round_store mode; selects the RND instantiation)
 };
 
-template <typename T>
+template <typename T, int RND>
 __device__ __forceinline__ void epilogue(const LevelArgs<T>& a, int mode, long long col_off, long long node,
                                          unsigned m, const T av[3]) {
   const long long d0 = col_off + 3 * node;
@@ -192,17 +198,17 @@ __device__ __forceinline__ void epilogue(const LevelArgs<T>& a, int mode, long l
     const bool live = (m >> q) & 1u;
     const long long d = d0 + q;
     if (mode == MODE_APPLY) {
-      a.y[d] = round_store(live ? av[q] : T(0), a.round);
+      a.y[d] = rs<RND>(live ? av[q] : T(0));
     } else if (mode == MODE_RESID) {
-      a.y[d] = round_store(live ? (a.b[d] - av[q]) : T(0), a.round);
+      a.y[d] = rs<RND>(live ? (a.b[d] - av[q]) : T(0));
     } else if (mode == MODE_JACOBI) {
-      a.y[d] = round_store(a.u[d] + a.s * a.inv[3 * node + q] * (a.b[d] - (live ? av[q] : T(0))), a.round);
+      a.y[d] = rs<RND>(a.u[d] + a.s * a.inv[3 * node + q] * (a.b[d] - (live ? av[q] : T(0))));
     } else {  // MODE_CHEB
-      const T r = round_store(a.res[d] - (live ? av[q] : T(0)), a.round);
-      const T dn = round_store(a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r, a.round);
+      const T r = rs<RND>(a.res[d] - (live ? av[q] : T(0)));
+      const T dn = rs<RND>(a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r);
       a.res[d] = r;
       a.y[d] = dn;
-      a.x[d] = round_store(a.x[d] + dn, a.round);
+      a.x[d] = rs<RND>(a.x[d] + dn);
     }
   }
 }
@@ -230,7 +236,7 @@ __device__ __forceinline__ void epilogue_load(const LevelArgs<T>& a, int mode, l
 }
 
 // epilogue() from prefetched inputs (the same arithmetic)
-template <typename T>
+template <typename T, int RND>
 __device__ __forceinline__ void epilogue_pre(const LevelArgs<T>& a, int mode, long long col_off, long long node, unsigned m,
                                              const T av[3], const EpiPre<T>& in) {
   const long long d0 = col_off + 3 * node;
@@ -239,17 +245,17 @@ __device__ __forceinline__ void epilogue_pre(const LevelArgs<T>& a, int mode, lo
     const bool live = (m >> q) & 1u;
     const long long d = d0 + q;
     if (mode == MODE_APPLY) {
-      a.y[d] = round_store(live ? av[q] : T(0), a.round);
+      a.y[d] = rs<RND>(live ? av[q] : T(0));
     } else if (mode == MODE_RESID) {
-      a.y[d] = round_store(live ? (in.v[0][q] - av[q]) : T(0), a.round);
+      a.y[d] = rs<RND>(live ? (in.v[0][q] - av[q]) : T(0));
     } else if (mode == MODE_JACOBI) {
-      a.y[d] = round_store(a.u[d] + a.s * a.inv[3 * node + q] * (in.v[0][q] - (live ? av[q] : T(0))), a.round);
+      a.y[d] = rs<RND>(a.u[d] + a.s * a.inv[3 * node + q] * (in.v[0][q] - (live ? av[q] : T(0))));
     } else {  // MODE_CHEB
-      const T r = round_store(in.v[0][q] - (live ? av[q] : T(0)), a.round);
-      const T dn = round_store(a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r, a.round);
+      const T r = rs<RND>(in.v[0][q] - (live ? av[q] : T(0)));
+      const T dn = rs<RND>(a.c1 * a.u[d] + a.c2 * a.inv[3 * node + q] * r);
       a.res[d] = r;
       a.y[d] = dn;
-      a.x[d] = round_store(in.v[1][q] + dn, a.round);
+      a.x[d] = rs<RND>(in.v[1][q] + dn);
     }
   }
 }
@@ -388,7 +394,7 @@ __device__ __forceinline__ void fine_tile_nodes(const KC& K, const T* __restrict
 // the halo's global indices and live bits are staged once; while column c is
 // computed from shared memory, column c+1's halo is already loading into
 // registers, so the global-load latency overlaps the FMAs.
-template <typename T, int SLOT, bool REFLECT, int TZ, int NPT>
+template <typename T, int SLOT, bool REFLECT, int TZ, int NPT, int RND>
 __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm, int cpb) {
   constexpr int FMAXH = NPT == 1 ? 3 : 4;   // halo nodes staged per thread and column
   constexpr int TXN = FTXT * NPT;                 // tile nodes along x
@@ -503,7 +509,7 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
           const int i = x0 + lx * NPT + q;
           if (i >= g.nx) continue;
           const long long n = ((long long)i * g.ny + j) * g.nz + k;
-          epilogue_pre(a, mode, off, n, mq[q], av[q], ep[q]);
+          epilogue_pre<T, RND>(a, mode, off, n, mq[q], av[q], ep[q]);
         }
       } else {
         T av[NPT][3];
@@ -514,7 +520,7 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
           if (i >= g.nx) continue;
           const long long n = ((long long)i * g.ny + j) * g.nz + k;
           const unsigned m = a.mask ? a.mask[n] : 7u;
-          epilogue(a, mode, off, n, m, av[q]);
+          epilogue<T, RND>(a, mode, off, n, m, av[q]);
         }
       }
     }
@@ -534,7 +540,7 @@ constexpr size_t fine_smem_bytes() {
 // Galerkin levels as assembled 27-point stencils: S[(d * 9 + 3 q + r)][node] is the 3 x 3 coupling of
 // the node with its neighbour node + d, summed over the elements holding both.  Per node and column
 // that is 243 FMA and 243 / CB coefficient loads, against 576 of each for the element blocks.
-template <typename T, int CB>
+template <typename T, int CB, int RND>
 __global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);   // [CB][HALO][3]
@@ -591,7 +597,7 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const Le
   }
 #pragma unroll
   for (int c = 0; c < CB; ++c) {
-    if (c < nc && (!a.active || a.active[c0 + c])) epilogue_pre(a, mode, off + c * a.colstride, n, m, out[c], ep[c]);
+    if (c < nc && (!a.active || a.active[c0 + c])) epilogue_pre<T, RND>(a, mode, off + c * a.colstride, n, m, out[c], ep[c]);
   }
 }
 

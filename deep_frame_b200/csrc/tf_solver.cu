@@ -368,13 +368,14 @@ int k0_slot(tf_handle* h) {
 
 // One finest-level launch: z tiles of 8 or 9 nodes (whichever wastes fewer
 // threads on this grid), two x-adjacent nodes per thread in FP32.
-template <typename T, int SLOT, bool REFLECT, int TZ>
-void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
+template <typename T, int SLOT, bool REFLECT, int TZ, int RND>
+void launch_fine_rounded(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   constexpr int NPT = (sizeof(T) == 4 && REFLECT) ? 2 : 1;
   constexpr size_t smem = fine_smem_bytes<T, TZ, NPT>();
   static bool configured = false;   // per variant and process; the attribute is per function
   if (!configured) {
-    TF_CUDA_CHECK(cudaFuncSetAttribute(fine_level_kernel<T, SLOT, REFLECT, TZ, NPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TF_CUDA_CHECK(cudaFuncSetAttribute(fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
     configured = true;
   }
   TileMap tm;
@@ -387,8 +388,20 @@ void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   int cpb = 1;
   while (cpb < a.ncol && (long long)tiles * ((a.ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
   dim3 grid((unsigned)tiles, (unsigned)((a.ncol + cpb - 1) / cpb));
-  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm, cpb);
+  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm, cpb);
   TF_LAUNCH_CHECK("fine_level_kernel");
+}
+
+// One finest-level launch: z tiles of 8 or 9 nodes (whichever wastes fewer
+// threads on this grid), two x-adjacent nodes per thread in FP32.  The storage
+// rounding of 16-bit precisions is a separate instantiation (FP32 only).
+template <typename T, int SLOT, bool REFLECT, int TZ>
+void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (a.round == 1) { launch_fine_rounded<T, SLOT, REFLECT, TZ, 1>(a, mode, st); return; }
+    if (a.round == 2) { launch_fine_rounded<T, SLOT, REFLECT, TZ, 2>(a, mode, st); return; }
+  }
+  launch_fine_rounded<T, SLOT, REFLECT, TZ, 0>(a, mode, st);
 }
 
 // Tensor-core finest level (FP32 work precision, settings.tensor_cores): tiles of 8 x 8 x tz nodes
@@ -465,12 +478,18 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
     dim3 grid(tiles, (a.ncol + cb - 1) / cb);
     const size_t smem = sizeof(T) * 3 * HALO * cb;
-    static bool configured = false;   // per instantiation and process; the attribute is per function
-    if (!configured) {
-      TF_CUDA_CHECK(cudaFuncSetAttribute(stencil_level_kernel<T, cb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      configured = true;
-    }
-    stencil_level_kernel<T, cb><<<grid, threads, smem, st>>>(a, mode, tm);
+    auto launch = [&](auto rnd) {
+      constexpr int RND = decltype(rnd)::value;
+      static bool configured = false;   // per instantiation and process; the attribute is per function
+      if (!configured) {
+        TF_CUDA_CHECK(cudaFuncSetAttribute(stencil_level_kernel<T, cb, RND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+      }
+      stencil_level_kernel<T, cb, RND><<<grid, threads, smem, st>>>(a, mode, tm);
+    };
+    if (std::is_same<T, float>::value && a.round == 1) launch(std::integral_constant<int, 1>{});
+    else if (std::is_same<T, float>::value && a.round == 2) launch(std::integral_constant<int, 2>{});
+    else launch(std::integral_constant<int, 0>{});
     TF_LAUNCH_CHECK("stencil_level_kernel");
   }
 }

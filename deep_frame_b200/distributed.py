@@ -68,12 +68,8 @@ class ShardedMeasure:
         coefficients = spectrum.weights[kept] * self.factor
         grad_worst = torch.zeros(nelem, dtype=torch.float64, device=device)
         for g, u in zip(self.groups, solved):
+            # this rank's partial combinations U_local v_i, completed by one all-reduce of [kept, ndof]
             mixing = spectrum.vectors[np.ix_(g["local_ks"], kept)]
-            if self.world == 1:
-                # every direction is local: the energy kernel forms the combinations U v_i itself
-                grad_worst += self.ops.energy(u, coefficients, scale, combination=mixing)
-                continue
-            # partial combinations of this rank's columns, completed by one all-reduce of [kept, ndof]
             partial = (self.ops.combine(u, mixing) if u is not None else
                        torch.zeros((len(kept), g["forces"].shape[1]), dtype=torch.float64, device=device))
             self._all_reduce(partial)
@@ -105,18 +101,9 @@ class DeviceOps:
                                mg._stream()), None, "tf_gram")
         return out
 
-    def energy(self, columns, coefficients, scale, combination=None):
-        return self.system._multigrid().energy_device(columns, combination=combination, coefficients=coefficients, scale=scale)
+    def energy(self, columns, coefficients, scale):
+        return self.system._multigrid().energy_device(columns, coefficients=coefficients, scale=scale)
 
     def combine(self, columns, mixing):
         """[k, ndof] = mixing^T columns, on the device (tf_combine)."""
-        import torch
-        from . import _lib
-        lib = _lib.load()
-        mg = self.system._multigrid()
-        m, n = columns.shape
-        k = mixing.shape[1]
-        coef = torch.as_tensor(np.ascontiguousarray(mixing), dtype=torch.float64, device=columns.device)
-        out = torch.empty((k, n), dtype=torch.float64, device=columns.device)
-        _lib.check(lib.tf_combine(_lib.ptr(columns), m, n, _lib.ptr(coef), k, _lib.ptr(out), mg._stream()), None, "tf_combine")
-        return out
+        return self.system._multigrid().combine_device(columns, mixing)

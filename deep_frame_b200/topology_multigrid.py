@@ -301,6 +301,18 @@ class GeometricMultigrid:
                                            self._stream()), self.handle, "tf_apply_level")
         return out
 
+    def combine_device(self, columns, mixing, out=None):
+        """[k, ndof] = mixing^T columns for device columns [m, ndof] and a host mixing matrix [m, k]
+        (tf_combine): the combinations U v whose energies the lambda_max sensitivity sums."""
+        torch = self.torch
+        mixing = np.ascontiguousarray(np.asarray(mixing, dtype=float))
+        m, n = columns.shape
+        coef = torch.as_tensor(mixing, device=columns.device)
+        out = torch.empty((mixing.shape[1], n), dtype=torch.float64, device=columns.device) if out is None else out
+        _lib.check(self.lib.tf_combine(_lib.ptr(columns), m, n, _lib.ptr(coef), mixing.shape[1], _lib.ptr(out), self._stream()),
+                   None, "tf_combine")
+        return out
+
     def operator(self, grid, moduli=None, mask=None):
         """y = mask * K (mask * u) on a grid [R, 3, padded nodes] (topology_multigrid.py:105-109)."""
         if moduli is not None:

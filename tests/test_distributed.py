@@ -51,10 +51,8 @@ class OracleOps:
     def gram(self, p_all, u_local):
         return p_all @ u_local.T
 
-    def energy(self, columns, coefficients, scale, combination=None):
+    def energy(self, columns, coefficients, scale):
         import torch
-        if combination is not None:
-            columns = torch.as_tensor(np.asarray(combination).T) @ columns
         e = self.op.element_energy(self.shape, self.system.ke, columns.numpy().T)
         e = e.reshape(len(coefficients), -1) if e.ndim == 2 else e[None]
         return torch.as_tensor(scale.numpy() * (np.asarray(coefficients) @ e))
@@ -110,17 +108,15 @@ def _oracle_reference():
     return ocov.measure(parts, model.factor, shape, system.ke, derivative)
 
 
-def test_unsharded_measure_forms_combinations_in_the_energy_call():
-    """One process (no process group): every direction is local, so the lambda_max gradient passes
-    the eigenvector combinations to the energy call instead of forming U v first."""
+def test_unsharded_measure_matches_the_oracle():
+    """One process (no process group): the exchange's all-reduces are no-ops and the measure equals
+    the oracle's single-process measure."""
     import torch
     from deep_frame_b200.distributed import ShardedMeasure
     ref = _oracle_reference()
     shape, system, model, density = _problem()
     moduli, derivative = system.moduli(density, 3.0, 1e-9)
-    ops = OracleOps(shape, system, moduli)
-    ops.combine = lambda *a: pytest.fail("one process must not form partial combinations")
-    rows, _ = ShardedMeasure(_groups(model), model.rank, model.factor, ops).measure(torch.as_tensor(-derivative))
+    rows, _ = ShardedMeasure(_groups(model), model.rank, model.factor, OracleOps(shape, system, moduli)).measure(torch.as_tensor(-derivative))
     assert rows[0]["value"] == pytest.approx(ref["load_mean"], rel=1e-12)
     assert rows[1]["value"] == pytest.approx(ref["load_worst"], rel=1e-12)
     assert rows[1]["info"]["ks_n_mm"] == pytest.approx(ref["ks"], rel=1e-12)
