@@ -54,6 +54,8 @@ def parse(argv=None):
     ap.add_argument("--pcg", default="float64", choices=["float64", "float32"],
                     help="fast path's PCG iterations: FP64, or FP32 with FP64 reliable residual updates")
     ap.add_argument("--tensor-cores", action="store_true", help="fast path's finest-level V-cycle applies on tcgen05")
+    ap.add_argument("--fine-tz", type=int, default=0, choices=[0, 8, 9],
+                    help="node-tile height of the finest-level operator in both arms (0: the one that wastes fewer threads)")
     ap.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 arm (default min(steps, 3))")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 arm")
     ap.add_argument("--storage-trial", default="", metavar="P1,P2",
@@ -168,7 +170,7 @@ def schedule_settings(text):
 
 
 def fast_settings(args):
-    return {"precision": args.precision, "pcg_precision": args.pcg, "tensor_cores": bool(args.tensor_cores)}
+    return {"precision": args.precision, "pcg_precision": args.pcg, "tensor_cores": bool(args.tensor_cores), "fine_tz": args.fine_tz}
 
 
 PLAIN = {"precision": "float64", "pcg_precision": "float64", "tensor_cores": False}
@@ -263,7 +265,7 @@ def ours(args):
             if rank != 0:
                 tune_smoother(system, [(key, forces) for key, _, forces in groups], moduli,
                               candidates=[{k: v for k, v in choice[0].items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps",
-                                                                                        "tensor_cores", "coarsest_dofs", "cycle")}], repeats=1)
+                                                                                        "tensor_cores", "coarsest_dofs", "cycle", "fine_tz")}], repeats=1)
 
     def arm():
         mg = system._multigrid()
@@ -298,7 +300,8 @@ def ours(args):
               "ndof": system.ndof, "levels": timed[-1]["levels"], "coarsest_dofs": timed[-1]["coarsest_dofs"],
               "converged": all(r["converged"] for r in timed),
               "smoother": {k: v for k, v in mg.settings.items() if k in ("smoother", "chebyshev_degree", "growth", "sweeps", "tensor_cores",
-                                                                          "coarsest_dofs", "precision", "pcg_precision", "cycle")},
+                                                                          "coarsest_dofs", "precision", "pcg_precision", "cycle",
+                                                                          "fine_tz")},
               "tuning": tuning, "rows": rows}
     dominant = max(("fine_fp64", "fine_work"), key=lambda k: breakdown[k]["ms"])
     result["dominant"] = dominant

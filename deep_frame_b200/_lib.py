@@ -35,7 +35,8 @@ class TfSettings(ctypes.Structure):
                 ("retries", ctypes.c_int32), ("batch", ctypes.c_int32), ("tensor_cores", ctypes.c_int32),
                 ("coarsest_dofs", ctypes.c_int64), ("damping", ctypes.c_double), ("chebyshev_ratio", ctypes.c_double),
                 ("growth", ctypes.c_double), ("tolerance", ctypes.c_double), ("dead_ratio", ctypes.c_double),
-                ("zero_rhs", ctypes.c_double), ("reliable", ctypes.c_double), ("pcg_precision", ctypes.c_int32)]
+                ("zero_rhs", ctypes.c_double), ("reliable", ctypes.c_double), ("pcg_precision", ctypes.c_int32),
+                ("fine_tz", ctypes.c_int32)]
 
 
 class TfGrid(ctypes.Structure):

@@ -1,8 +1,9 @@
 """Measured choice of the V-cycle smoother for a given problem.
 
 The smoother schedule (Chebyshev degree, growth of the sweep count per level,
-or damped Jacobi), the depth of the hierarchy and the finest-level apply (FP32
-CUDA cores or TF32 tensor cores) change the cost of a V-cycle and the number of PCG iterations, never
+or damped Jacobi), the cycle (V or W), the depth of the hierarchy and the
+finest-level apply (its node-tile height; FP32 CUDA cores or TF32 tensor cores)
+change the cost of a V-cycle and the number of PCG iterations, never
 the converged answer: every candidate solves to the same
 recomputed true relative residual.  ``tune_smoother`` times one full solve of
 every fixture group per candidate on the device and returns the fastest.
@@ -27,6 +28,8 @@ CANDIDATES = (
     # W-cycles: two coarse corrections per level (more Galerkin-level work, fewer PCG iterations)
     {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "cycle": "W"},
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.0, "cycle": "W"},
+    # the finest operator's node tiles 8 high (no register spills) where 9 would waste fewer threads
+    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "fine_tz": 8},
     # the finest-level V-cycle apply on the tensor cores (TF32 operands)
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5, "tensor_cores": True},
 )

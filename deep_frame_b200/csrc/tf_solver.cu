@@ -451,7 +451,7 @@ void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st)
   }
   const int slot = k0_slot(h);
   const int nz = a.g.nz;
-  const bool nine = h->k0_reflect && ((nz + 8) / 9) * 9 < ((nz + 7) / 8) * 8;
+  const bool nine = h->k0_reflect && (h->s.fine_tz == 9 || (h->s.fine_tz == 0 && ((nz + 8) / 9) * 9 < ((nz + 7) / 8) * 8));
   if (h->k0_reflect) {
     if (nine) {
       if (slot == 0) launch_fine_variant<T, 0, true, 9>(a, mode, st);
@@ -1063,6 +1063,7 @@ void validate_settings(const tf_settings& s) {
   require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.precision != TF_PRECISION_FLOAT64,
           "float32 PCG iterations need the float32 work precision");
   require(std::isfinite(s.reliable) && s.reliable > 0 && s.reliable < 1, "reliable must be in (0, 1)");
+  require(s.fine_tz == 0 || s.fine_tz == 8 || s.fine_tz == 9, "fine_tz must be 0, 8 or 9");
 }
 
 }  // namespace

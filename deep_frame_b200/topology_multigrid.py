@@ -26,7 +26,7 @@ MULTIGRID = {"coarse": "galerkin", "coarsest_dofs": 8000, "max_levels": 8, "smoo
              "power_iterations": 20, "precision": "float32", "tolerance": 1e-8, "max_iterations": 2000, "batch": 0,
              "projection": True, "coarsest_projection": True, "dead_ratio": 1e-12, "zero_rhs": 1e-12, "retries": 2,
              "device": "cuda", "eigen_tolerance": 1e-8, "eigen_iterations": 300, "eigen_guard": 2, "eigen_refresh": 10,
-             "eigen_drop": 1e-12, "eigen_seed": 0, "tensor_cores": False, "pcg_precision": "float64", "reliable": 0.01}
+             "eigen_drop": 1e-12, "eigen_seed": 0, "tensor_cores": False, "pcg_precision": "float64", "reliable": 0.01, "fine_tz": 0}
 PRECISIONS = ("float64", "float32", "bfloat16", "float16")
 
 
@@ -63,6 +63,7 @@ def _native_settings(settings):
         raise ValueError("Invalid multigrid settings")
     s.pcg_precision = _lib.PRECISION[settings["pcg_precision"]]
     s.reliable = float(settings["reliable"])
+    s.fine_tz = int(settings["fine_tz"])
     return s
 
 
