@@ -28,8 +28,8 @@ CANDIDATES = (
     # W-cycles: two coarse corrections per level (more Galerkin-level work, fewer PCG iterations)
     {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "cycle": "W"},
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.0, "cycle": "W"},
-    # the finest operator's node tiles 8 high (no register spills) where 9 would waste fewer threads
-    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "fine_tz": 8},
+    # the finest operator's node tiles 9 high (fewer padded threads on some grids, register spills)
+    {"smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0, "fine_tz": 9},
     # the finest-level V-cycle apply on the tensor cores (TF32 operands)
     {"smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5, "tensor_cores": True},
 )
@@ -38,43 +38,44 @@ CANDIDATES = (
 def tune_smoother(system, groups, moduli, base=None, candidates=CANDIDATES, repeats=2):
     """groups: [(key, forces [R, ndof] CUDA tensor)]; moduli: CUDA float64 tensor.
 
-    Rebuilds ``system.multigrid`` for every candidate; leaves the fastest in place
-    and returns (settings, timings)."""
+    Times every candidate on its own multigrid handle, closing each one before the next is built
+    (on the largest grids two handles do not fit in device memory together), and installs the
+    fastest converged settings in ``system`` (its handle is rebuilt on next use).  Returns
+    (settings, timings)."""
     import torch
     from .topology_multigrid import GeometricMultigrid
     base = dict(base or system.multigrid_settings or {})
+    if system.multigrid is not None:
+        system.multigrid.close()
+        system.multigrid = None
     timings = []
     best = None
     for cand in candidates:
         settings = {**base, **cand}
         mg = GeometricMultigrid(system.shape, system.spacing, system.ke, settings, system.me)
         seconds, iterations, ok = None, [], True
-        for rep in range(repeats + 1):
-            torch.cuda.synchronize()
-            t0 = perf_counter()
-            mg.update_device(moduli)
-            its = []
-            for key, forces in groups:
-                part = system.groups[key][0][1]
-                _, report = mg.solve_device(key, part["fixed"], forces)
-                ok &= report["converged"]
-                its.append(max(report["iterations"]))
-            torch.cuda.synchronize()
-            if rep:   # the first pass builds buffers
-                dt = perf_counter() - t0
-                seconds = dt if seconds is None else min(seconds, dt)
-                iterations = its
+        try:
+            for rep in range(repeats + 1):
+                torch.cuda.synchronize()
+                t0 = perf_counter()
+                mg.update_device(moduli)
+                its = []
+                for key, forces in groups:
+                    part = system.groups[key][0][1]
+                    _, report = mg.solve_device(key, part["fixed"], forces)
+                    ok &= report["converged"]
+                    its.append(max(report["iterations"]))
+                torch.cuda.synchronize()
+                if rep:   # the first pass builds buffers
+                    dt = perf_counter() - t0
+                    seconds = dt if seconds is None else min(seconds, dt)
+                    iterations = its
+        finally:
+            mg.close()
         timings.append({"settings": cand, "seconds": seconds, "iterations": iterations, "converged": bool(ok)})
         if ok and (best is None or seconds < best[0]):
-            if best is not None:
-                best[2].close()
-            best = (seconds, settings, mg)
-        else:
-            mg.close()
+            best = (seconds, settings)
     if best is None:
         raise RuntimeError("no smoother candidate converged")
-    if system.multigrid is not None and system.multigrid is not best[2]:
-        system.multigrid.close()
-    system.multigrid = best[2]
     system.multigrid_settings = best[1]
     return best[1], timings
