@@ -451,11 +451,12 @@ void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st)
   }
   const int slot = k0_slot(h);
   const int nz = a.g.nz;
-  // 8-high node tiles unless 9 is asked for: the 9-high variants spill registers at two CTAs per SM,
-  // and on the 352 x 352 x 48 plate the 8-high FP32 apply is 17 % faster although it pads 4 % more
-  // threads (the FP64 apply is as fast either way)
-  (void)nz;
-  const bool nine = h->k0_reflect && h->s.fine_tz == 9;
+  // 8-high node tiles unless 9-high ones pad at least 15 % fewer threads along z: the 9-high
+  // variants spill registers at two CTAs per SM.  Measured: on the 352 x 352 x 48 plate (49 node
+  // planes: 56 padded with 8, 54 with 9) the 8-high FP32 apply is 17 % faster; on the 96 x 96 x 16
+  // plate (17 planes: 24 against 18) the 9-high one is 10 % faster.
+  const bool nine = h->k0_reflect &&
+                    (h->s.fine_tz == 9 || (h->s.fine_tz == 0 && 100 * (((nz + 8) / 9) * 9) < 85 * (((nz + 7) / 8) * 8)));
   if (h->k0_reflect) {
     if (nine) {
       if (slot == 0) launch_fine_variant<T, 0, true, 9>(a, mode, st);
