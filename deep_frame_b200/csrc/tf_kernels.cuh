@@ -390,10 +390,12 @@ __device__ __forceinline__ void fine_tile_nodes(const KC& K, const T* __restrict
   }
 }
 
-// One CTA handles one tile for `cpb` consecutive columns: the element moduli,
-// the halo's global indices and live bits are staged once; while column c is
-// computed from shared memory, column c+1's halo is already loading into
-// registers, so the global-load latency overlaps the FMAs.
+// One CTA handles one tile for `cpb` (<= 64) consecutive columns: the element
+// moduli, the halo's global indices and live bits, the owned nodes' live bits and
+// the chunk's active-column mask are read once; while column c is computed from
+// one shared-memory halo buffer, column c+1's halo is loading into registers and
+// then goes to the other buffer, so the global-load latency overlaps the FMAs and
+// one barrier per column suffices.
 template <typename T, int SLOT, bool REFLECT, int TZ, int NPT, int RND>
 __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm, int cpb) {
   constexpr int FMAXH = NPT == 1 ? 3 : 4;   // halo nodes staged per thread and column
@@ -406,8 +408,8 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
   constexpr int HALO_N = SHX * SHY * (TZ + 2);
   static_assert(HALO_N <= FMAXH * NT, "halo exceeds the per-thread staging slots");
   extern __shared__ __align__(16) unsigned char fine_smem[];
-  T* su = reinterpret_cast<T*>(fine_smem);
-  T* sE = su + 3 * PLANE;
+  T* su = reinterpret_cast<T*>(fine_smem);   // two halo buffers of 3 * PLANE
+  T* sE = su + 6 * PLANE;
   const K0Const<T, SLOT, REFLECT> K;
   if (a.gate && !*a.gate) return;
   const int c_begin = blockIdx.y * cpb;
@@ -464,77 +466,86 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
       }
     }
   };
-  auto store = [&]() {
+  // two halo buffers: column c is computed from one while column c+1's halo is stored into the other,
+  // so one barrier per column separates them
+  auto store = [&](T* buf) {
 #pragma unroll
     for (int h = 0; h < FMAXH; ++h) {
       if (soff[h] >= 0) {
-        su[soff[h]] = pre[h][0];
-        su[soff[h] + PLANE] = pre[h][1];
-        su[soff[h] + 2 * PLANE] = pre[h][2];
+        buf[soff[h]] = pre[h][0];
+        buf[soff[h] + PLANE] = pre[h][1];
+        buf[soff[h] + 2 * PLANE] = pre[h][2];
       }
     }
   };
-  // skip to the first active column of the chunk
-  int c = c_begin;
-  while (c < c_end && a.active && !a.active[c]) ++c;
-  if (c >= c_end) return;
+  // the chunk's active columns as a bit mask (cpb <= 64), read once
+  unsigned long long act = 0ull;
+  for (int q = c_begin; q < c_end; ++q)
+    if (!a.active || a.active[q]) act |= 1ull << (q - c_begin);
+  if (!act) return;
+  auto next_active = [&](int from) {
+    const unsigned long long rest = from - c_begin < 64 ? act >> (from - c_begin) : 0ull;
+    return rest ? from + __ffsll(static_cast<long long>(rest)) - 1 : c_end;
+  };
+  int c = next_active(c_begin);
+  T* cur = su;
+  T* other = su + 3 * PLANE;
   fetch(c);
-  store();
+  store(cur);
   __syncthreads();
   const int j = y0 + ly, k = z0 + lz;
   const bool owner = j < g.ny && k < g.nz;
+  // per-node quantities that do not depend on the column: node index and live bits
+  long long node[NPT];
+  unsigned mq[NPT];
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) {
+    const int i = x0 + lx * NPT + q;
+    node[q] = -1;
+    mq[q] = 0u;
+    if (owner && i < g.nx) {
+      node[q] = ((long long)i * g.ny + j) * g.nz + k;
+      mq[q] = a.mask ? a.mask[node[q]] : 7u;
+    }
+  }
   while (c < c_end) {
-    int next = c + 1;
-    while (next < c_end && a.active && !a.active[next]) ++next;
+    const int next = next_active(c + 1);
     if (next < c_end) fetch(next);
     if (owner) {
       const long long off = (long long)c * a.colstride;
       if constexpr (sizeof(T) == 4) {
         // work-precision smoother: the epilogue inputs are fetched before the operator
         EpiPre<T> ep[NPT];
-        unsigned mq[NPT];
 #pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-          const int i = x0 + lx * NPT + q;
-          mq[q] = 0u;
-          if (i >= g.nx) continue;
-          const long long n = ((long long)i * g.ny + j) * g.nz + k;
-          mq[q] = a.mask ? a.mask[n] : 7u;
-          epilogue_load(a, mode, off, n, ep[q]);
-        }
+        for (int q = 0; q < NPT; ++q)
+          if (node[q] >= 0) epilogue_load(a, mode, off, node[q], ep[q]);
         T av[NPT][3];
-        fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+        fine_tile_nodes<T, NPT>(K, cur, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
 #pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-          const int i = x0 + lx * NPT + q;
-          if (i >= g.nx) continue;
-          const long long n = ((long long)i * g.ny + j) * g.nz + k;
-          epilogue_pre<T, RND>(a, mode, off, n, mq[q], av[q], ep[q]);
-        }
+        for (int q = 0; q < NPT; ++q)
+          if (node[q] >= 0) epilogue_pre<T, RND>(a, mode, off, node[q], mq[q], av[q], ep[q]);
       } else {
         T av[NPT][3];
-        fine_tile_nodes<T, NPT>(K, su, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
+        fine_tile_nodes<T, NPT>(K, cur, sE, PLANE, SHY, P, SEY, SEZ, lx, ly, lz, av);
 #pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-          const int i = x0 + lx * NPT + q;
-          if (i >= g.nx) continue;
-          const long long n = ((long long)i * g.ny + j) * g.nz + k;
-          const unsigned m = a.mask ? a.mask[n] : 7u;
-          epilogue<T, RND>(a, mode, off, n, m, av[q]);
-        }
+        for (int q = 0; q < NPT; ++q)
+          if (node[q] >= 0) epilogue<T, RND>(a, mode, off, node[q], mq[q], av[q]);
       }
     }
     if (next >= c_end) break;
+    store(other);
     __syncthreads();
-    store();
-    __syncthreads();
+    T* t = cur;
+    cur = other;
+    other = t;
     c = next;
   }
 }
 
 template <typename T, int TZ, int NPT>
 constexpr size_t fine_smem_bytes() {
-  return sizeof(T) * (3 * (FTXT * NPT + 2) * (TY + 2) * FineTile<T, TZ>::P + (FTXT * NPT + 1) * (TY + 1) * (TZ + 1));
+  // two halo buffers (3 component planes each) and the element moduli
+  return sizeof(T) * (2 * 3 * (FTXT * NPT + 2) * (TY + 2) * FineTile<T, TZ>::P + (FTXT * NPT + 1) * (TY + 1) * (TZ + 1));
 }
 
 // Galerkin levels as assembled 27-point stencils: S[(d * 9 + 3 q + r)][node] is the 3 x 3 coupling of

@@ -385,8 +385,9 @@ void launch_fine_rounded(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   tm.tiles_z = (a.g.nz + TZ - 1) / TZ;
   const int tiles = tm.tiles_x * tm.tiles_y * tm.tiles_z;
   // columns per CTA: enough CTAs for a few waves on 148 SMs, the rest looped inside
+  // (at most 64: the kernel keeps its chunk's active columns in a 64-bit mask)
   int cpb = 1;
-  while (cpb < a.ncol && (long long)tiles * ((a.ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
+  while (cpb < 64 && cpb < a.ncol && (long long)tiles * ((a.ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
   dim3 grid((unsigned)tiles, (unsigned)((a.ncol + cpb - 1) / cpb));
   fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm, cpb);
   TF_LAUNCH_CHECK("fine_level_kernel");
