@@ -551,18 +551,22 @@ constexpr size_t fine_smem_bytes() {
 // Galerkin levels as assembled 27-point stencils: S[(d * 9 + 3 q + r)][node] is the 3 x 3 coupling of
 // the node with its neighbour node + d, summed over the elements holding both.  Per node and column
 // that is 243 FMA and 243 / CB coefficient loads, against 576 of each for the element blocks.
+//
+// Launch order: with groups_first the column groups of one tile are consecutive blocks (blockIdx.x =
+// column group, blockIdx.y = tile), so the tile's coefficients come from HBM once and from L2 for the
+// other groups running beside it; otherwise blockIdx.x = tile, blockIdx.y = column group.
 template <typename T, int CB, int RND>
-__global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const LevelArgs<T> a, int mode, TileMap tm) {
+__global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const LevelArgs<T> a, int mode, TileMap tm, int groups_first) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);   // [CB][HALO][3]
-  const int c0 = blockIdx.y * CB;
+  const int c0 = (groups_first ? blockIdx.x : blockIdx.y) * CB;
   if (a.gate && !*a.gate) return;
   const int nc = min(CB, a.ncol - c0);
   bool any = false;
   for (int c = 0; c < nc; ++c) any |= (!a.active || a.active[c0 + c]);
   if (!any) return;
   const Geo& g = a.g;
-  const int b = blockIdx.x;
+  const int b = groups_first ? blockIdx.y : blockIdx.x;
   const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
   const int tz = tm.tz;
   const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;

@@ -482,7 +482,11 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     const int threads = TX * TY * tm.tz;
     const unsigned tiles = (unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z);
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
-    dim3 grid(tiles, (a.ncol + cb - 1) / cb);
+    // column groups of a tile launched side by side (its 27-point coefficients then stream from HBM
+    // once per tile instead of once per group), as long as the tiles fit the grid's y extent
+    const unsigned groups = (unsigned)((a.ncol + cb - 1) / cb);
+    const int groups_first = tiles <= 65535u ? 1 : 0;
+    dim3 grid = groups_first ? dim3(groups, tiles) : dim3(tiles, groups);
     const size_t smem = sizeof(T) * 3 * HALO * cb;
     auto launch = [&](auto rnd) {
       constexpr int RND = decltype(rnd)::value;
@@ -491,7 +495,7 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
         TF_CUDA_CHECK(cudaFuncSetAttribute(stencil_level_kernel<T, cb, RND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = true;
       }
-      stencil_level_kernel<T, cb, RND><<<grid, threads, smem, st>>>(a, mode, tm);
+      stencil_level_kernel<T, cb, RND><<<grid, threads, smem, st>>>(a, mode, tm, groups_first);
     };
     if (std::is_same<T, float>::value && a.round == 1) launch(std::integral_constant<int, 1>{});
     else if (std::is_same<T, float>::value && a.round == 2) launch(std::integral_constant<int, 2>{});
