@@ -1,13 +1,13 @@
-"""Parity at the benchmark's own configurations (too large for a CPU oracle solve).
+"""Parity on the benchmark's largest workloads (too large for a CPU oracle solve).
 
-* The 352 x 352 x 48 plate (config 5, 18.3 M dofs, 2 x 42 columns to 1e-8): the fast path (FP32
+* The 352 x 352 x 48 plate (18.3 M dofs, 2 x 42 columns to 1e-8): the fast path (FP32
   V-cycle) against the plain FP64 GMG-PCG (FP64 V-cycle) on the same device: tr, lambda_max and
   KS within 1e-6 relative, both sensitivity fields within 1e-5 relative (2-norm).  Each path
-  converges on its own FP64 true residual, so this is the north star's agreement bar between them.
-* The 128 x 128 x 24 plate (config 3's grid, volume fraction 0.15, cone filter 1.5, move 0.2):
+  converges on its own FP64 true residual; these are the agreement bars asked of the fast path.
+* The 128 x 128 x 24 plate (volume fraction 0.15, cone filter 1.5, move 0.2):
   a fixed number of SIMP + MMA iterations with the FP32 V-cycle and with the FP64 V-cycle give
   final physical densities within 1e-4 max-abs and the same tr history to 1e-6.
-The 96 x 96 x 16 plate (config 2) is held to the FP64 oracle fixture in test_gpu_covariance.py.
+The 96 x 96 x 16 plate is held to the FP64 oracle fixture in test_gpu_covariance.py.
 """
 import numpy as np
 import pytest

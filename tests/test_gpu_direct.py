@@ -98,7 +98,7 @@ def test_multigrid_system_solve_matches_direct_system_solve(cuda):
 
 
 def test_system_solve_matches_reference_superlu_golden(cuda):
-    """Config-1 cantilever (48 x 24 x 24): compliance 1e-6 and sensitivities 1e-5 vs the reference's SuperLU."""
+    """The 48 x 24 x 24 cantilever: compliance 1e-6 and sensitivities 1e-5 vs the reference's SuperLU."""
     from pathlib import Path
     g = np.load(Path(__file__).resolve().parent / "golden" / "cantilever_48x24x24.npz")
     system, _ = _system((48, 24, 24), 0, "multigrid", {"precision": "float64", "smoother": "jacobi", "sweeps": 2,
@@ -112,7 +112,7 @@ def test_system_solve_matches_reference_superlu_golden(cuda):
 
 
 def test_direct_system_solve_of_config_one_matches_reference_superlu(cuda):
-    """linear_solver="cuda_cudss" on the config-1 cantilever (48 x 24 x 24, 91 875 dofs: the banded
+    """linear_solver="cuda_cudss" on the 48 x 24 x 24 cantilever (91 875 dofs: the banded
     factorisation, bandwidth about 3 x 25 x 25): compliance within 1e-6 and sensitivities within
     1e-5 of the reference's SuperLU golden."""
     from pathlib import Path
