@@ -33,7 +33,7 @@ def _rows(precision):
     return out
 
 
-def test_config_five_fast_path_agrees_with_plain_fp64(cuda):
+def test_plate_352_fast_path_agrees_with_plain_fp64(cuda):
     fast = _rows("float32")
     plain = _rows("float64")
     for key in ("tr", "lambda_max", "ks"):
@@ -42,7 +42,7 @@ def test_config_five_fast_path_agrees_with_plain_fp64(cuda):
         assert np.linalg.norm(fast[key] - plain[key]) < 1e-5 * np.linalg.norm(plain[key]), key
 
 
-def test_config_three_simp_designs_agree_across_vcycle_precisions(cuda):
+def test_plate_128_simp_designs_agree_across_vcycle_precisions(cuda):
     import torch
     from deep_frame_b200 import problems
     from deep_frame_b200.optimize import CovarianceSimp
