@@ -499,15 +499,17 @@ def simp(args):
 
 def instances(args):
     """--instances N: N independent seeded plate instances (grids from 64 x 64 x 12 to 160 x 160 x 24,
-    6 to 42 load columns per half), each with its own solver handle and CUDA stream on its own host
-    thread, solved concurrently to 1e-8.  After one untimed round (buffers, hierarchies, constant
-    slots) the wall time of one concurrent round gives solves/s (one solve = all columns of both
-    halves of one instance) and column solves/s."""
+    6 to 42 load columns per half), each with its own solver handle, solved to 1e-8 three ways: as one
+    batch (tf_solve_batch: every PCG and V-cycle stage one launch over all instances; one batch per
+    mirror half), one after another on one stream, and concurrently on one host thread and CUDA
+    stream per instance.  After one untimed round of each (buffers, hierarchies, constant slots) the
+    time of one round gives solves/s (one solve = all columns of both halves of one instance)."""
     import threading
     import torch
     from deep_frame_b200 import problems
     from deep_frame_b200.covariance import InterfaceCovariance
     from deep_frame_b200.elasticity import HexElasticity
+    from deep_frame_b200.topology_multigrid import solve_batch_device
     rng = np.random.default_rng(2026)
     sizes = [(64, 64, 12), (80, 80, 12), (96, 96, 16), (112, 112, 16), (128, 128, 16), (128, 128, 24), (144, 144, 24), (160, 160, 24)]
     specs = []
@@ -523,13 +525,14 @@ def instances(args):
         moduli = torch.as_tensor(system.moduli(density, 3.0, 1e-9)[0], device="cuda")
         groups = [(key, forces[:rhs].contiguous()) for key, _, forces in model.groups()]
         work.append({"system": system, "moduli": moduli, "groups": groups, "stream": torch.cuda.Stream(), "shape": shape, "rhs": rhs})
+    for item in work:
+        item["system"]._multigrid().update_device(item["moduli"])
+    torch.cuda.synchronize()
     errors = []
 
     def solve(item):
         try:
             with torch.cuda.stream(item["stream"]):
-                mg = item["system"]._multigrid()
-                mg.update_device(item["moduli"])
                 its = []
                 for key, forces in item["groups"]:
                     _, report = item["system"].solve_group_device(key, forces)
@@ -539,7 +542,7 @@ def instances(args):
         except Exception as error:          # surfaced after the join
             errors.append(repr(error))
 
-    def round_():
+    def threaded():
         threads = [threading.Thread(target=solve, args=(item,)) for item in work]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -548,25 +551,63 @@ def instances(args):
         for t in threads:
             t.join()
         torch.cuda.synchronize()
+        if errors:
+            raise RuntimeError("; ".join(errors))
         return time.perf_counter() - t0
 
-    round_()                                  # untimed: allocations, hierarchies, constant slots
-    seconds = round_()
-    if errors:
-        raise RuntimeError("; ".join(errors))
-    columns = sum(2 * item["rhs"] for item in work)
-    serial = 0.0
-    for item in work:                          # the same instances one after another, for comparison
+    def serial():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        solve(item)
-        serial += time.perf_counter() - t0
-    line = {"metric": "independent uneven instances: solves/s", "value": round(len(work) / seconds, 4), "unit": "solves/s", "n_gpus": 1,
+        for item in work:
+            solve(item)
+        torch.cuda.synchronize()
+        if errors:
+            raise RuntimeError("; ".join(errors))
+        return time.perf_counter() - t0
+
+    def batched():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        results = []
+        for half in range(max(len(item["groups"]) for item in work)):
+            jobs = []
+            for item in work:
+                if half < len(item["groups"]):
+                    key, forces = item["groups"][half]
+                    mg = item["system"]._multigrid()
+                    jobs.append((mg, key, item["system"].groups[key][0][1]["fixed"], forces))
+            results.append(solve_batch_device(jobs))
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - t0
+        for half in results:
+            for (_, report) in half:
+                if not report["converged"]:
+                    raise RuntimeError(f"batched solve did not converge: {max(report['relative_residual'])}")
+        return seconds, results
+
+    batched()                                 # untimed: allocations, hierarchies, constant slots
+    batch_seconds, results = batched()
+    serial()
+    serial_seconds = serial()
+    # the batch against the instances' own solves (the serial round just ran them)
+    worst = 0.0
+    for half, outcome in enumerate(results):
+        for item, (u, report) in zip([w for w in work if half < len(w["groups"])], outcome):
+            key, forces = item["groups"][half]
+            single, _ = item["system"].solve_group_device(key, forces)
+            worst = max(worst, float(((u - single).norm(dim=1) / single.norm(dim=1).clamp_min(1e-300)).max()))
+    threaded()
+    threaded_seconds = threaded()
+    columns = sum(2 * item["rhs"] for item in work)
+    line = {"metric": "independent uneven instances: solves/s", "value": round(len(work) / batch_seconds, 4), "unit": "solves/s", "n_gpus": 1,
             "higher_is_better": True, "data": "synthetic",
             "config": {"instances": [{"shape": list(item["shape"]), "rhs_per_half": item["rhs"], "pcg_iterations": item.get("iterations")}
-                                     for item in work], "tolerance": 1e-8, "concurrency": "one host thread + CUDA stream + solver handle per instance"},
-            "seconds": round(seconds, 4), "column_solves_per_s": round(columns / seconds, 2), "serial_seconds": round(serial, 4),
-            "concurrency_speedup": round(serial / seconds, 3)}
+                                     for item in work], "tolerance": 1e-8,
+                       "batched": "tf_solve_batch: one launch per PCG / V-cycle stage over all instances, one batch per mirror half"},
+            "seconds": round(batch_seconds, 4), "column_solves_per_s": round(columns / batch_seconds, 2),
+            "serial_seconds": round(serial_seconds, 4), "speedup_vs_serial": round(serial_seconds / batch_seconds, 3),
+            "threaded_seconds": round(threaded_seconds, 4), "threaded_speedup_vs_serial": round(serial_seconds / threaded_seconds, 3),
+            "batch_vs_own_solves_max_rel": worst}
     for item in work:
         item["system"].close()
     print(json.dumps(line))

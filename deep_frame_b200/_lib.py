@@ -17,7 +17,7 @@ COARSE = {"galerkin": 0, "rediscretize": 1}
 
 # every symbol include/tf_b200.h declares (checked by the CPU test suite)
 SYMBOLS = ("tf_default_settings", "tf_create", "tf_levels", "tf_update", "tf_set_bc", "tf_prepare", "tf_precondition",
-           "tf_solve", "tf_solve_guess", "tf_apply", "tf_apply_level", "tf_mass_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_combine", "tf_timers", "tf_launch_count",
+           "tf_solve", "tf_solve_guess", "tf_solve_batch", "tf_apply", "tf_apply_level", "tf_mass_apply", "tf_element_energy", "tf_gram", "tf_gram_scratch_size", "tf_gram_static", "tf_combine", "tf_timers", "tf_launch_count",
            "tf_destroy", "tf_last_error")
 SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_project", "tf_filter_volume", "tf_oc_update",
             "tf_filter_destroy",
@@ -92,6 +92,7 @@ def load():
             "tf_precondition": [P, U64, P, I32, P, P],
             "tf_solve": [P, U64, P, I32, P, ctypes.POINTER(TfReport), P],
             "tf_solve_guess": [P, U64, P, I32, P, ctypes.POINTER(TfReport), P],
+            "tf_solve_batch": [P, P, I32, P, P, P, ctypes.POINTER(TfReport), P],
             "tf_mass_apply": [P, U64, P, P, P, I32, P, P],
             "tf_apply": [P, U64, I32, P, I32, P, P],
             "tf_apply_level": [P, U64, I32, P, I32, P, P],

@@ -9,6 +9,8 @@
 // dependent substitution steps.
 #include "tf_common.h"
 #include "tf_dense.h"
+#include "tf_batch.cuh"
+#include "tf_reduce.cuh"
 
 namespace tfb {
 
@@ -361,8 +363,9 @@ __device__ __forceinline__ bool trimul_chunk_live(int i0, int kc, int transpose)
   return transpose ? (kc + 1) * TM_KCH - 1 >= i0 : kc * TM_KCH <= i0 + TM_RB - 1;
 }
 
-__global__ void __launch_bounds__(TM_THREADS) trimul_split_kernel(const double* __restrict__ X, const double* __restrict__ B,
+__device__ __forceinline__ void trimul_split_body(const VGrid vg_,const double* __restrict__ X, const double* __restrict__ B,
                                                                   double* __restrict__ P, int n, int ncol, int transpose) {
+  TF_VGRID(vg_);
   __shared__ double Xs[TM_RB][TM_KS + 1];
   __shared__ double Bs[TM_CW][TM_KS + 1];
   const int i0 = blockIdx.x * TM_RB, kc = blockIdx.y, c0 = blockIdx.z * TM_CW;
@@ -409,9 +412,14 @@ __global__ void __launch_bounds__(TM_THREADS) trimul_split_kernel(const double* 
     }
   }
 }
+__global__ void __launch_bounds__(TM_THREADS) trimul_split_kernel(const double* __restrict__ X, const double* __restrict__ B,
+                                                                  double* __restrict__ P, int n, int ncol, int transpose) {
+  trimul_split_body(vgrid(), X, B, P, n, ncol, transpose);
+}
 
-__global__ void trimul_sum_kernel(const double* __restrict__ P, double* __restrict__ C, int n, int ncol, int nchunks, int transpose,
+__device__ __forceinline__ void trimul_sum_body(const VGrid vg_,const double* __restrict__ P, double* __restrict__ C, int n, int ncol, int nchunks, int transpose,
                                   const int* __restrict__ active) {
+  TF_VGRID(vg_);
   const long long total = (long long)n * ncol;
   for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
     const int col = static_cast<int>(idx / n), i = static_cast<int>(idx % n);
@@ -422,6 +430,33 @@ __global__ void trimul_sum_kernel(const double* __restrict__ P, double* __restri
       if (trimul_chunk_live(i0, kc, transpose)) s += P[((long long)kc * ncol + col) * n + i];
     C[(long long)col * n + i] = s;
   }
+}
+__global__ void trimul_sum_kernel(const double* __restrict__ P, double* __restrict__ C, int n, int ncol, int nchunks, int transpose,
+                                  const int* __restrict__ active) {
+  trimul_sum_body(vgrid(), P, C, n, ncol, nchunks, transpose, active);
+}
+
+struct TrimulSplitRec {
+  const double* X;
+  const double* B;
+  double* P;
+  int n, ncol, transpose;
+};
+__global__ void __launch_bounds__(TM_THREADS) trimul_split_batch(const __grid_constant__ Batch<TrimulSplitRec> b) {
+  VGrid vg;
+  const TrimulSplitRec& r = b.rec[batch_locate(b, vg)];
+  trimul_split_body(vg, r.X, r.B, r.P, r.n, r.ncol, r.transpose);
+}
+struct TrimulSumRec {
+  const double* P;
+  double* C;
+  int n, ncol, nchunks, transpose;
+  const int* active;
+};
+__global__ void trimul_sum_batch(const __grid_constant__ Batch<TrimulSumRec> b) {
+  VGrid vg;
+  const TrimulSumRec& r = b.rec[batch_locate(b, vg)];
+  trimul_sum_body(vg, r.P, r.C, r.n, r.ncol, r.nchunks, r.transpose, r.active);
 }
 
 size_t dense_trimul_work(int n, int ncol) {
@@ -436,6 +471,21 @@ void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, 
   TF_LAUNCH_CHECK("trimul_split_kernel");
   trimul_sum_kernel<<<grid_for((long long)n * ncol, 256), 256, 0, s>>>(work, C, n, ncol, nchunks, transpose, active);
   TF_LAUNCH_CHECK("trimul_sum_kernel");
+}
+
+void dense_trimul_batch(const TrimulJob* jobs, int count, int transpose, cudaStream_t s) {
+  std::vector<std::pair<dim3, TrimulSplitRec>> split;
+  std::vector<std::pair<dim3, TrimulSumRec>> sum;
+  for (int i = 0; i < count; ++i) {
+    const TrimulJob& j = jobs[i];
+    if (j.n <= 0 || j.ncol <= 0) continue;
+    const int nchunks = (j.n + TM_KCH - 1) / TM_KCH;
+    split.push_back({dim3((j.n + TM_RB - 1) / TM_RB, nchunks, (j.ncol + TM_CW - 1) / TM_CW),
+                     TrimulSplitRec{j.X, j.B, j.work, j.n, j.ncol, transpose}});
+    sum.push_back({dim3(grid_for((long long)j.n * j.ncol, 256)), TrimulSumRec{j.work, j.C, j.n, j.ncol, nchunks, transpose, j.active}});
+  }
+  launch_batched<TrimulSplitRec>(trimul_split_batch, split, dim3(TM_THREADS), 0, s, "trimul_split_batch");
+  launch_batched<TrimulSumRec>(trimul_sum_batch, sum, dim3(256), 0, s, "trimul_sum_batch");
 }
 
 }  // namespace tfb

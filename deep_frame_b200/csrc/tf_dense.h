@@ -17,6 +17,16 @@ size_t dense_factor_work(int n);
 void dense_trimul(const double* X, const double* B, double* C, int n, int ncol, int transpose, const int* active, double* work,
                   cudaStream_t s);
 size_t dense_trimul_work(int n, int ncol);
+// dense_trimul of several independent systems, one launch per stage for all of them
+struct TrimulJob {
+  const double* X;
+  const double* B;
+  double* C;
+  double* work;
+  int n, ncol;
+  const int* active;
+};
+void dense_trimul_batch(const TrimulJob* jobs, int count, int transpose, cudaStream_t s);
 
 // Banded FP64 Cholesky (tf_band.cu).  Band storage AB[j * (bw + 1) + d] = A[j + d][j], 0 <= d <= bw.
 // bandwidth of a CSR matrix (max |i - j| over its entries); scratch_dev holds one int

@@ -12,6 +12,8 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
+#include "tf_reduce.cuh"
 
 namespace tfb {
 
@@ -187,6 +189,9 @@ struct LevelArgs {
   const int* gate;       // optional device flag; the whole launch is skipped while *gate == 0
   T s, c1, c2;           // epilogue scalars
   int round;             // storage rounding of the outputs (round_store mode; selects the RND instantiation)
+  // Fused PCG curvature (finest level, FP64 operator, MODE_APPLY): every warp writes the sum of
+  // u . y over its nodes of column c to dot_out[(c * gridDim.x + blockIdx.x) * warps + warp]
+  double* dot_out;
 };
 
 template <typename T, int RND>
@@ -287,6 +292,11 @@ __host__ inline TileMap tile_map(const Geo& g) {
   m.tiles_y = (g.ny + TY - 1) / TY;
   m.tiles_z = (g.nz + m.tz - 1) / m.tz;
   return m;
+}
+
+template <typename T, int CB>
+constexpr size_t stencil_smem_bytes() {
+  return sizeof(T) * 3 * (size_t)HALO * CB;
 }
 
 // Stage the masked input tiles of nc <= CB columns in one pass over the halo: the mask is read once
@@ -396,8 +406,13 @@ __device__ __forceinline__ void fine_tile_nodes(const KC& K, const T* __restrict
 // one shared-memory halo buffer, column c+1's halo is loading into registers and
 // then goes to the other buffer, so the global-load latency overlaps the FMAs and
 // one barrier per column suffices.
-template <typename T, int SLOT, bool REFLECT, int TZ, int NPT, int RND>
-__global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const LevelArgs<T> a, int mode, TileMap tm, int cpb) {
+//
+// PCG (FP64 only, MODE_APPLY): the curvature partials of LevelArgs::dot_out, in their own
+// instantiation so that the plain applies keep their registers.
+template <typename T, int SLOT, bool REFLECT, int TZ, int NPT, int RND, bool PCG>
+__device__ __forceinline__ void fine_level_body(const VGrid vg_, const LevelArgs<T>& a, int mode, TileMap tm, int cpb) {
+  TF_VGRID(vg_);
+  static_assert(!PCG || sizeof(T) == 8, "the fused PCG step is an FP64 operator");
   constexpr int FMAXH = NPT == 1 ? 3 : 4;   // halo nodes staged per thread and column
   constexpr int TXN = FTXT * NPT;                 // tile nodes along x
   constexpr int SHX = TXN + 2, SHY = TY + 2;      // staged halo extents
@@ -508,6 +523,7 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
       mq[q] = a.mask ? a.mask[node[q]] : 7u;
     }
   }
+  double dot = 0.0;
   while (c < c_end) {
     const int next = next_active(c + 1);
     if (next < c_end) fetch(next);
@@ -530,7 +546,24 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
 #pragma unroll
         for (int q = 0; q < NPT; ++q)
           if (node[q] >= 0) epilogue<T, RND>(a, mode, off, node[q], mq[q], av[q]);
+        if constexpr (PCG) {
+#pragma unroll
+          for (int q = 0; q < NPT; ++q) {
+            if (node[q] < 0) continue;
+            const int sc = ((lx * NPT + q + 1) * SHY + (ly + 1)) * P + (lz + 1);
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+              if ((mq[q] >> e) & 1u) dot += static_cast<double>(cur[sc + e * PLANE]) * static_cast<double>(av[q][e]);
+          }
+        }
       }
+    }
+    if constexpr (PCG) {
+      // every lane takes part (non-owners add 0), so the warp's partial is always written
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
+      if ((tid & 31) == 0) a.dot_out[((long long)c * gridDim.x + blockIdx.x) * ((NT + 31) / 32) + (tid >> 5)] = dot;
+      dot = 0.0;
     }
     if (next >= c_end) break;
     store(other);
@@ -540,6 +573,10 @@ __global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const Lev
     other = t;
     c = next;
   }
+}
+template <typename T, int SLOT, bool REFLECT, int TZ, int NPT, int RND, bool PCG>
+__global__ void __launch_bounds__(FTXT * TY * TZ, 2) fine_level_kernel(const __grid_constant__ LevelArgs<T> a, int mode, TileMap tm, int cpb) {
+  fine_level_body<T, SLOT, REFLECT, TZ, NPT, RND, PCG>(vgrid(), a, mode, tm, cpb);
 }
 
 template <typename T, int TZ, int NPT>
@@ -552,27 +589,26 @@ constexpr size_t fine_smem_bytes() {
 // the node with its neighbour node + d, summed over the elements holding both.  Per node and column
 // that is 243 FMA and 243 / CB coefficient loads, against 576 of each for the element blocks.
 //
-// Launch order: with groups_first the column groups of one tile are consecutive blocks (blockIdx.x =
-// column group, blockIdx.y = tile), so the tile's coefficients come from HBM once and from L2 for the
-// other groups running beside it; otherwise blockIdx.x = tile, blockIdx.y = column group.
 template <typename T, int CB, int RND>
-__global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const LevelArgs<T> a, int mode, TileMap tm, int groups_first) {
+__device__ __forceinline__ void stencil_level_body(const VGrid vg_, const LevelArgs<T>& a, int mode, TileMap tm) {
+  TF_VGRID(vg_);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);   // [CB][HALO][3]
-  const int c0 = (groups_first ? blockIdx.x : blockIdx.y) * CB;
+  const int c0 = blockIdx.y * CB;
   if (a.gate && !*a.gate) return;
   const int nc = min(CB, a.ncol - c0);
   bool any = false;
   for (int c = 0; c < nc; ++c) any |= (!a.active || a.active[c0 + c]);
   if (!any) return;
   const Geo& g = a.g;
-  const int b = groups_first ? blockIdx.y : blockIdx.x;
+  const int b = blockIdx.x;
   const int bz = b % tm.tiles_z, r = b / tm.tiles_z, by = r % tm.tiles_y, bx = r / tm.tiles_y;
   const int tz = tm.tz;
   const int x0 = bx * TX, y0 = by * TY, z0 = bz * tz;
   const long long off = (long long)c0 * a.colstride;
   stage_tiles<T, CB>(su, g, a.u + off, a.colstride, nc, a.mask, x0, y0, z0, tz);
   __syncthreads();
+  if ((int)threadIdx.x >= TX * TY * tz) return;   // a batched launch sizes its blocks for the tallest tile
   const int lz = threadIdx.x % tz, rr = threadIdx.x / tz, ly = rr % TY, lx = rr / TY;
   const int i = x0 + lx, j = y0 + ly, k = z0 + lz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -614,6 +650,10 @@ __global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const Le
   for (int c = 0; c < CB; ++c) {
     if (c < nc && (!a.active || a.active[c0 + c])) epilogue_pre<T, RND>(a, mode, off + c * a.colstride, n, m, out[c], ep[c]);
   }
+}
+template <typename T, int CB, int RND>
+__global__ void __launch_bounds__(TX * TY * TZMAX) stencil_level_kernel(const __grid_constant__ LevelArgs<T> a, int mode, TileMap tm) {
+  stencil_level_body<T, CB, RND>(vgrid(), a, mode, tm);
 }
 
 // ---------------------------------------------------------------------------
@@ -696,8 +736,9 @@ __global__ void __launch_bounds__(128) energy_kernel(const __grid_constant__ K0P
 // prolongation (:316).  Columns on blockIdx.y.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void restrict_kernel(Geo fine, Geo coarse, const T* __restrict__ r, long long fstride, T* __restrict__ out,
+__device__ __forceinline__ void restrict_body(const VGrid vg_,Geo fine, Geo coarse, const T* __restrict__ r, long long fstride, T* __restrict__ out,
                                 long long cstride, const uint8_t* __restrict__ cmask, const int* __restrict__ active, int round) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const T* rc = r + col * fstride;
@@ -730,11 +771,17 @@ __global__ void restrict_kernel(Geo fine, Geo coarse, const T* __restrict__ r, l
     oc[3 * n + 2] = (m & 4u) ? round_store(acc2, round) : T(0);
   }
 }
+template <typename T>
+__global__ void restrict_kernel(Geo fine, Geo coarse, const T* __restrict__ r, long long fstride, T* __restrict__ out,
+                                long long cstride, const uint8_t* __restrict__ cmask, const int* __restrict__ active, int round) {
+  restrict_body<T>(vgrid(), fine, coarse, r, fstride, out, cstride, cmask, active, round);
+}
 
 // x_fine += mask * P c  (P = transpose of the restriction)
 template <typename T>
-__global__ void prolong_add_kernel(Geo fine, Geo coarse, const T* __restrict__ c, long long cstride, T* __restrict__ x,
+__device__ __forceinline__ void prolong_add_body(const VGrid vg_,Geo fine, Geo coarse, const T* __restrict__ c, long long cstride, T* __restrict__ x,
                                    long long fstride, const uint8_t* __restrict__ fmask, const int* __restrict__ active, int round) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const T* cc = c + col * cstride;
@@ -779,6 +826,11 @@ __global__ void prolong_add_kernel(Geo fine, Geo coarse, const T* __restrict__ c
     if (m & 2u) xc[3 * n + 1] = round_store(xc[3 * n + 1] + acc1, round);
     if (m & 4u) xc[3 * n + 2] = round_store(xc[3 * n + 2] + acc2, round);
   }
+}
+template <typename T>
+__global__ void prolong_add_kernel(Geo fine, Geo coarse, const T* __restrict__ c, long long cstride, T* __restrict__ x,
+                                   long long fstride, const uint8_t* __restrict__ fmask, const int* __restrict__ active, int round) {
+  prolong_add_body<T>(vgrid(), fine, coarse, c, cstride, x, fstride, fmask, active, round);
 }
 
 }  // namespace tfb

@@ -368,50 +368,74 @@ __global__ void coarsest_assemble_kernel(Geo g, const double* __restrict__ B, co
 
 // gather live coarsest dofs of the active columns into FP64 [ncol][n]
 template <typename T>
-__global__ void coarsest_gather_kernel(const T* __restrict__ src, long long stride, const long long* __restrict__ live, int n,
+__device__ __forceinline__ void coarsest_gather_body(const VGrid vg_,const T* __restrict__ src, long long stride, const long long* __restrict__ live, int n,
                                        double* __restrict__ dst, const int* __restrict__ active) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     dst[(long long)col * n + t] = static_cast<double>(src[col * stride + live[t]]);
 }
+template <typename T>
+__global__ void coarsest_gather_kernel(const T* __restrict__ src, long long stride, const long long* __restrict__ live, int n,
+                                       double* __restrict__ dst, const int* __restrict__ active) {
+  coarsest_gather_body<T>(vgrid(), src, stride, live, n, dst, active);
+}
 
 template <typename T>
-__global__ void coarsest_scatter_kernel(const double* __restrict__ src, const long long* __restrict__ live, int n,
+__device__ __forceinline__ void coarsest_scatter_body(const VGrid vg_,const double* __restrict__ src, const long long* __restrict__ live, int n,
                                         T* __restrict__ dst, long long stride, const int* __restrict__ active, int round) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     dst[col * stride + live[t]] = round_store(static_cast<T>(src[(long long)col * n + t]), round);
 }
+template <typename T>
+__global__ void coarsest_scatter_kernel(const double* __restrict__ src, const long long* __restrict__ live, int n,
+                                        T* __restrict__ dst, long long stride, const int* __restrict__ active, int round) {
+  coarsest_scatter_body<T>(vgrid(), src, live, n, dst, stride, active, round);
+}
 
 // ----------------------------------------------------------- elementwise ----
 
 template <typename T>
-__global__ void zero_cols_kernel(T* __restrict__ v, long long stride, const int* __restrict__ active) {
+__device__ __forceinline__ void zero_cols_body(const VGrid vg_,T* __restrict__ v, long long stride, const int* __restrict__ active) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   T* p = v + col * stride;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < stride; t += (long long)gridDim.x * blockDim.x) p[t] = T(0);
 }
+template <typename T>
+__global__ void zero_cols_kernel(T* __restrict__ v, long long stride, const int* __restrict__ active) {
+  zero_cols_body<T>(vgrid(), v, stride, active);
+}
 
 // x = s * inv * b   (first Jacobi sweep from a zero guess)
 template <typename T>
-__global__ void jacobi_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x, T s,
+__device__ __forceinline__ void jacobi_first_body(const VGrid vg_,long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x, T s,
                                     const int* __restrict__ active, int round) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const long long off = (long long)col * ndof;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ndof; t += (long long)gridDim.x * blockDim.x)
     x[off + t] = round_store(s * inv[t] * b[off + t], round);
 }
+template <typename T>
+__global__ void jacobi_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x, T s,
+                                    const int* __restrict__ active, int round) {
+  jacobi_first_body<T>(vgrid(), ndof, inv, b, x, s, active, round);
+}
 
 // Chebyshev start from a zero guess: res = b, d = inv * res / theta, x = d (with has_x: x += d, res
 // kept).  Without write_rd only x is written: a one-sweep smoother reads neither res nor d again.
 template <typename T>
-__global__ void cheb_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ res,
+__device__ __forceinline__ void cheb_first_body(const VGrid vg_,long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ res,
                                   T* __restrict__ d, T* __restrict__ x, T inv_theta, int has_x, int write_rd,
                                   const int* __restrict__ active, int round) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (active && !active[col]) return;
   const long long off = (long long)col * ndof;
@@ -425,20 +449,30 @@ __global__ void cheb_first_kernel(long long ndof, const T* __restrict__ inv, con
     x[off + t] = has_x ? round_store(x[off + t] + dv, round) : dv;
   }
 }
+template <typename T>
+__global__ void cheb_first_kernel(long long ndof, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ res,
+                                  T* __restrict__ d, T* __restrict__ x, T inv_theta, int has_x, int write_rd,
+                                  const int* __restrict__ active, int round) {
+  cheb_first_body<T>(vgrid(), ndof, inv, b, res, d, x, inv_theta, has_x, write_rd, active, round);
+}
 
 // --------------------------------------------------------------- PCG -------
 
 constexpr int PCG_BLOCKS = 64;   // reduction blocks per column
 
 // bnorm = ||b||; r = b; x = 0 (or r = b - A x computed elsewhere)
-__global__ void pcg_norm_kernel(const double* __restrict__ b, long long n, PcgState st, double* out, int take_sqrt) {
+__device__ __forceinline__ void pcg_norm_body(const VGrid vg_,const double* __restrict__ b, long long n, PcgState st, double* out, int take_sqrt) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const double* p = b + (long long)col * n;
   double a = 0.0, z = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a += p[t] * p[t];
   block_reduce2<0, 0>(a, z);
-  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) out[col] = take_sqrt ? sqrt(a) : a;
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col, blockIdx.x, gridDim.x)) out[col] = take_sqrt ? sqrt(a) : a;
+}
+__global__ void pcg_norm_kernel(const double* __restrict__ b, long long n, PcgState st, double* out, int take_sqrt) {
+  pcg_norm_body(vgrid(), b, n, st, out, take_sqrt);
 }
 
 // alpha = rho / (p . q).  R is the type of the PCG vectors: double for the FP64 PCG, float for the
@@ -452,7 +486,24 @@ __global__ void pcg_alpha_kernel(const R* __restrict__ p, const R* __restrict__ 
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     a += static_cast<double>(p[off + t]) * static_cast<double>(q[off + t]);
   block_reduce2<0, 0>(a, z);
-  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) st.alpha[col] = st.rho[col] / a;
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col, blockIdx.x, gridDim.x)) st.alpha[col] = st.rho[col] / a;
+}
+
+// alpha = rho / (p . K p) from the per-warp partials that the FP64 finest-level operator wrote while
+// it formed q = K p (LevelArgs::dot_out): one block per column sums its partials in a fixed order,
+// so the result does not depend on scheduling.
+__device__ __forceinline__ void pcg_alpha_sum_body(const VGrid vg_,const double* __restrict__ part, long long per_col, PcgState st) {
+  TF_VGRID(vg_);
+  const int col = blockIdx.x;
+  if (!st.active[col]) return;
+  const double* pc = part + (long long)col * per_col;
+  double a = 0.0, z = 0.0;
+  for (long long t = threadIdx.x; t < per_col; t += blockDim.x) a += pc[t];
+  block_reduce2<0, 0>(a, z);
+  if (threadIdx.x == 0) st.alpha[col] = st.rho[col] / a;
+}
+__global__ void pcg_alpha_sum_kernel(const double* __restrict__ part, long long per_col, PcgState st) {
+  pcg_alpha_sum_body(vgrid(), part, per_col, st);
 }
 
 // x += alpha p; r -= alpha q; rel = ||r|| / ||b||; candidate when rel < tol (topology_multigrid.py:424-430).
@@ -462,9 +513,10 @@ __global__ void pcg_alpha_kernel(const R* __restrict__ p, const R* __restrict__ 
 // reliable > 0 (the mixed PCG) a column whose iterated residual fell below reliable times its
 // last true residual also asks for the FP64 residual recomputation (a reliable update).
 template <typename T, typename R>
-__global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, const R* __restrict__ p,
+__device__ __forceinline__ void pcg_update_body(const VGrid vg_,double* __restrict__ x, R* __restrict__ r, const R* __restrict__ p,
                                   const R* __restrict__ q, const T* __restrict__ w, long long n, PcgState st, double tol,
                                   int step, double reliable) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
@@ -481,7 +533,7 @@ __global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, con
     d += rd * (static_cast<double>(w[off + t]) * zs);
   }
   block_reduce3<0, 1, 0>(a, mx, d);
-  if (last_block_combine3<0, 1, 0>(a, mx, d, st.partial, st.count, col)) {
+  if (last_block_combine3<0, 1, 0>(a, mx, d, st.partial, st.count, col, blockIdx.x, gridDim.x)) {
     const double rel = sqrt(a) / st.bnorm[col];
     st.rel[col] = rel;
     st.scale[col] = fmax(mx, 1e-300);
@@ -494,11 +546,18 @@ __global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, con
     if (rel < tol || (reliable > 0.0 && rel < reliable * st.rtrue[col])) { st.cand[col] = 1; atomicExch(&st.flags[0], 1); }
   }
 }
+template <typename T, typename R>
+__global__ void pcg_update_kernel(double* __restrict__ x, R* __restrict__ r, const R* __restrict__ p,
+                                  const R* __restrict__ q, const T* __restrict__ w, long long n, PcgState st, double tol,
+                                  int step, double reliable) {
+  pcg_update_body<T, R>(vgrid(), x, r, p, q, w, n, st, tol, step, reliable);
+}
 
 // True-residual recheck (topology_multigrid.py:431-437): when any column is a
 // candidate, every active column's residual is recomputed as t = b - K x; a
 // column converges when ||t|| / ||b|| < tol, the others continue from t.
-__global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, long long n, PcgState st, double tol, int step) {
+__device__ __forceinline__ void pcg_truecheck_body(const VGrid vg_,const double* __restrict__ t_res, long long n, PcgState st, double tol, int step) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.flags[0] || !st.active[col] || st.cand[col] == 4) return;
   const long long off = (long long)col * n;
@@ -508,19 +567,23 @@ __global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, long long
     a += v * v;
   }
   block_reduce2<0, 0>(a, z);
-  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col)) {
+  if (last_block_combine<0, 0>(a, z, st.partial, st.count, col, blockIdx.x, gridDim.x)) {
     const double rel = sqrt(a) / st.bnorm[col];
     st.rel[col] = rel;
     st.rtrue[col] = rel;
     st.cand[col] = (rel < tol) ? 2 : 3;   // 2 = converged, 3 = continue from the true residual
   }
 }
+__global__ void pcg_truecheck_kernel(const double* __restrict__ t_res, long long n, PcgState st, double tol, int step) {
+  pcg_truecheck_body(vgrid(), t_res, n, st, tol, step);
+}
 
 // Columns that continue from the true residual (cand 3): r <- t, and the preconditioner inputs
 // scale = max|t| and rzo = t . z_old are formed again from the new r.
 template <typename T, typename R>
-__global__ void pcg_retire_kernel(const double* __restrict__ t_res, R* __restrict__ r, const T* __restrict__ w, long long n,
+__device__ __forceinline__ void pcg_retire_body(const VGrid vg_,const double* __restrict__ t_res, R* __restrict__ r, const T* __restrict__ w, long long n,
                                   PcgState st) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col] || st.cand[col] != 3) return;
   const long long off = (long long)col * n;
@@ -533,13 +596,19 @@ __global__ void pcg_retire_kernel(const double* __restrict__ t_res, R* __restric
     d += v * (static_cast<double>(w[off + t]) * zs);
   }
   block_reduce2<1, 0>(mx, d);
-  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) {
+  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col, blockIdx.x, gridDim.x)) {
     st.scale[col] = fmax(mx, 1e-300);
     st.rzo[col] = d;
   }
 }
+template <typename T, typename R>
+__global__ void pcg_retire_kernel(const double* __restrict__ t_res, R* __restrict__ r, const T* __restrict__ w, long long n,
+                                  PcgState st) {
+  pcg_retire_body<T, R>(vgrid(), t_res, r, w, n, st);
+}
 
-__global__ void pcg_flags_kernel(PcgState st, int step) {
+__device__ __forceinline__ void pcg_flags_body(const VGrid vg_,PcgState st, int step) {
+  TF_VGRID(vg_);
   // single block: finalize column states for this step
   int n_active = 0;
   for (int col = threadIdx.x; col < st.ncol; col += blockDim.x) {
@@ -562,12 +631,16 @@ __global__ void pcg_flags_kernel(PcgState st, int step) {
     st.flags[0] = 0;
   }
 }
+__global__ void pcg_flags_kernel(PcgState st, int step) {
+  pcg_flags_body(vgrid(), st, step);
+}
 
 // The starting residual: r = t (t = b, or b - K x0 for a warm start), scale = max|t| (clamped at
 // 1e-300; topology_multigrid.py:320) and rtrue = ||t|| / ||b||, the reference of the first
 // reliable update.
 template <typename R>
-__global__ void pcg_take_kernel(const double* __restrict__ t_res, R* __restrict__ r, long long n, PcgState st) {
+__device__ __forceinline__ void pcg_take_body(const VGrid vg_,const double* __restrict__ t_res, R* __restrict__ r, long long n, PcgState st) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
@@ -579,10 +652,14 @@ __global__ void pcg_take_kernel(const double* __restrict__ t_res, R* __restrict_
     a += v * v;
   }
   block_reduce2<1, 0>(mx, a);
-  if (last_block_combine<1, 0>(mx, a, st.partial, st.count, col)) {
+  if (last_block_combine<1, 0>(mx, a, st.partial, st.count, col, blockIdx.x, gridDim.x)) {
     st.scale[col] = fmax(mx, 1e-300);
     st.rtrue[col] = sqrt(a) / st.bnorm[col];
   }
+}
+template <typename R>
+__global__ void pcg_take_kernel(const double* __restrict__ t_res, R* __restrict__ r, long long n, PcgState st) {
+  pcg_take_body<R>(vgrid(), t_res, r, n, st);
 }
 
 // scale = max|r| (clamped at 1e-300) before the first preconditioner application (topology_multigrid.py:320)
@@ -595,11 +672,12 @@ __global__ void pcg_prep_kernel(const R* __restrict__ r, long long n, PcgState s
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     mx = fmax(mx, fabs(static_cast<double>(r[off + t])));
   block_reduce2<1, 0>(mx, d);
-  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col)) st.scale[col] = fmax(mx, 1e-300);
+  if (last_block_combine<1, 0>(mx, d, st.partial, st.count, col, blockIdx.x, gridDim.x)) st.scale[col] = fmax(mx, 1e-300);
 }
 
 template <typename T, typename R>
-__global__ void pcg_to_work_kernel(const R* __restrict__ r, long long n, PcgState st, T* __restrict__ w, int round) {
+__device__ __forceinline__ void pcg_to_work_body(const VGrid vg_,const R* __restrict__ r, long long n, PcgState st, T* __restrict__ w, int round) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
@@ -607,12 +685,17 @@ __global__ void pcg_to_work_kernel(const R* __restrict__ r, long long n, PcgStat
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     w[off + t] = round_store(static_cast<T>(static_cast<double>(r[off + t]) * s), round);
 }
+template <typename T, typename R>
+__global__ void pcg_to_work_kernel(const R* __restrict__ r, long long n, PcgState st, T* __restrict__ w, int round) {
+  pcg_to_work_body<T, R>(vgrid(), r, n, st, w, round);
+}
 
 // rz = r . z with z = scale * w (w: the work-precision preconditioner output); beta = (rz - rzo) / rho
 // (flexible Polak-Ribiere, topology_multigrid.py:445-448).  z is written out only when asked for (z != nullptr).
 template <typename T, typename R>
-__global__ void pcg_from_work_kernel(const T* __restrict__ w, const R* __restrict__ r, double* __restrict__ z, long long n,
+__device__ __forceinline__ void pcg_from_work_body(const VGrid vg_,const T* __restrict__ w, const R* __restrict__ r, double* __restrict__ z, long long n,
                                      PcgState st, int initial) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
@@ -624,16 +707,22 @@ __global__ void pcg_from_work_kernel(const T* __restrict__ w, const R* __restric
     d += static_cast<double>(r[off + t]) * v;
   }
   block_reduce2<0, 0>(d, zz);
-  if (last_block_combine<0, 0>(d, zz, st.partial, st.count, col)) {
+  if (last_block_combine<0, 0>(d, zz, st.partial, st.count, col, blockIdx.x, gridDim.x)) {
     st.beta[col] = initial ? 0.0 : (d - st.rzo[col]) / st.rho[col];
     st.rho[col] = d;
     st.wscale[col] = s;
   }
 }
+template <typename T, typename R>
+__global__ void pcg_from_work_kernel(const T* __restrict__ w, const R* __restrict__ r, double* __restrict__ z, long long n,
+                                     PcgState st, int initial) {
+  pcg_from_work_body<T, R>(vgrid(), w, r, z, n, st, initial);
+}
 
 // p = z + beta p, z = wscale * w
 template <typename T, typename R>
-__global__ void pcg_direction_kernel(const T* __restrict__ w, R* __restrict__ p, long long n, PcgState st, int initial) {
+__device__ __forceinline__ void pcg_direction_body(const VGrid vg_,const T* __restrict__ w, R* __restrict__ p, long long n, PcgState st, int initial) {
+  TF_VGRID(vg_);
   const int col = blockIdx.y;
   if (!st.active[col]) return;
   const long long off = (long long)col * n;
@@ -642,6 +731,10 @@ __global__ void pcg_direction_kernel(const T* __restrict__ w, R* __restrict__ p,
     const double z = static_cast<double>(w[off + t]) * s;
     p[off + t] = static_cast<R>(initial ? z : z + be * static_cast<double>(p[off + t]));
   }
+}
+template <typename T, typename R>
+__global__ void pcg_direction_kernel(const T* __restrict__ w, R* __restrict__ p, long long n, PcgState st, int initial) {
+  pcg_direction_body<T, R>(vgrid(), w, p, n, st, initial);
 }
 
 // ------------------------------------------------------- layout copies ----

@@ -25,6 +25,7 @@
 #include "tf_dense.h"
 #include "tf_setup.cuh"
 #include "tf_tc.cuh"
+#include "tf_batch.cuh"
 
 using namespace tfb;
 
@@ -32,7 +33,7 @@ namespace {
 
 thread_local std::string g_last_create_error;
 
-constexpr int CB32 = 4;                  // columns per CTA of the FP32 Galerkin-level operator
+constexpr int CB32 = 6;                  // columns per CTA of the FP32 Galerkin-level operator
 constexpr int CB64 = 2;                  // columns per CTA of the FP64 Galerkin-level operator
 constexpr long long DENSE_LIMIT = 24000;  // largest dense coarsest factor (4.6 GB in FP64)
 
@@ -164,8 +165,8 @@ struct tf_handle {
   bool have_moduli = false;
   std::map<uint64_t, std::vector<int64_t>> bcs;
   std::map<uint64_t, Hierarchy> hier;
-  // reduction scratch
-  DevBuf partial, count, scal;
+  // reduction scratch; dotp holds the FP64 operator's per-warp curvature partials
+  DevBuf partial, count, scal, dotp;
   // PCG state
   DevBuf pcg_d, pcg_i, hist, colmap;
   int pcg_cap = 0, hist_cap = 0;
@@ -368,28 +369,34 @@ int k0_slot(tf_handle* h) {
 
 // One finest-level launch: z tiles of 8 or 9 nodes (whichever wastes fewer
 // threads on this grid), two x-adjacent nodes per thread in FP32.
-template <typename T, int SLOT, bool REFLECT, int TZ, int RND>
+// Tiles of a finest-level launch and its columns per CTA: enough CTAs for a few waves on 148 SMs,
+// the rest looped inside (at most 64: the kernel keeps its chunk's active columns in a 64-bit mask).
+template <int TZ, int NPT>
+dim3 fine_shape(const Geo& g, int ncol, TileMap& tm, int& cpb) {
+  tm.tz = TZ;
+  tm.tiles_x = (g.nx + FTXT * NPT - 1) / (FTXT * NPT);
+  tm.tiles_y = (g.ny + TY - 1) / TY;
+  tm.tiles_z = (g.nz + TZ - 1) / TZ;
+  const int tiles = tm.tiles_x * tm.tiles_y * tm.tiles_z;
+  cpb = 1;
+  while (cpb < 64 && cpb < ncol && (long long)tiles * ((ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
+  return dim3((unsigned)tiles, (unsigned)((ncol + cpb - 1) / cpb));
+}
+
+template <typename T, int SLOT, bool REFLECT, int TZ, int RND, bool PCG = false>
 void launch_fine_rounded(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   constexpr int NPT = (sizeof(T) == 4 && REFLECT) ? 2 : 1;
   constexpr size_t smem = fine_smem_bytes<T, TZ, NPT>();
   static bool configured = false;   // per variant and process; the attribute is per function
   if (!configured) {
-    TF_CUDA_CHECK(cudaFuncSetAttribute(fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TF_CUDA_CHECK(cudaFuncSetAttribute(fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND, PCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
     configured = true;
   }
   TileMap tm;
-  tm.tz = TZ;
-  tm.tiles_x = (a.g.nx + FTXT * NPT - 1) / (FTXT * NPT);
-  tm.tiles_y = (a.g.ny + TY - 1) / TY;
-  tm.tiles_z = (a.g.nz + TZ - 1) / TZ;
-  const int tiles = tm.tiles_x * tm.tiles_y * tm.tiles_z;
-  // columns per CTA: enough CTAs for a few waves on 148 SMs, the rest looped inside
-  // (at most 64: the kernel keeps its chunk's active columns in a 64-bit mask)
-  int cpb = 1;
-  while (cpb < 64 && cpb < a.ncol && (long long)tiles * ((a.ncol + 2 * cpb - 1) / (2 * cpb)) >= 4 * 148 * 2) cpb *= 2;
-  dim3 grid((unsigned)tiles, (unsigned)((a.ncol + cpb - 1) / cpb));
-  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm, cpb);
+  int cpb;
+  const dim3 grid = fine_shape<TZ, NPT>(a.g, a.ncol, tm, cpb);
+  fine_level_kernel<T, SLOT, REFLECT, TZ, NPT, RND, PCG><<<grid, dim3(TZ, TY, FTXT), smem, st>>>(a, mode, tm, cpb);
   TF_LAUNCH_CHECK("fine_level_kernel");
 }
 
@@ -401,6 +408,8 @@ void launch_fine_variant(const LevelArgs<T>& a, int mode, cudaStream_t st) {
   if constexpr (std::is_same<T, float>::value) {
     if (a.round == 1) { launch_fine_rounded<T, SLOT, REFLECT, TZ, 1>(a, mode, st); return; }
     if (a.round == 2) { launch_fine_rounded<T, SLOT, REFLECT, TZ, 2>(a, mode, st); return; }
+  } else {
+    if (a.dot_out) { launch_fine_rounded<T, SLOT, REFLECT, TZ, 0, true>(a, mode, st); return; }
   }
   launch_fine_rounded<T, SLOT, REFLECT, TZ, 0>(a, mode, st);
 }
@@ -442,6 +451,23 @@ void launch_fine_tc(tf_handle* h, const LevelArgs<float>& a, int mode, cudaStrea
   TF_LAUNCH_CHECK("fine_tc_kernel");
 }
 
+// 8-high node tiles unless 9-high ones pad at least 15 % fewer threads along z: the 9-high
+// variants spill registers at two CTAs per SM.  Measured: on the 352 x 352 x 48 plate (49 node
+// planes: 56 padded with 8, 54 with 9) the 8-high FP32 apply is 17 % faster; on the 96 x 96 x 16
+// plate (17 planes: 24 against 18) the 9-high one is 10 % faster.
+bool fine_nine(const tf_handle* h, int nz) {
+  return h->k0_reflect &&
+         (h->s.fine_tz == 9 || (h->s.fine_tz == 0 && 100 * (((nz + 8) / 9) * 9) < 85 * (((nz + 7) / 8) * 8)));
+}
+
+// Per-column count of the FP64 finest-level operator's curvature partials: its tiles (one node per
+// thread along x, tz nodes high) times the warps of a tile.
+long long fine_dot_stride(const tf_handle* h, int tz) {
+  const Geo& g = h->geo[0];
+  const long long tiles = (long long)((g.nx + FTXT - 1) / FTXT) * ((g.ny + TY - 1) / TY) * ((g.nz + tz - 1) / tz);
+  return tiles * ((FTXT * TY * tz + 31) / 32);
+}
+
 template <typename T>
 void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st) {
   if constexpr (std::is_same<T, float>::value) {
@@ -451,13 +477,7 @@ void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st)
     }
   }
   const int slot = k0_slot(h);
-  const int nz = a.g.nz;
-  // 8-high node tiles unless 9-high ones pad at least 15 % fewer threads along z: the 9-high
-  // variants spill registers at two CTAs per SM.  Measured: on the 352 x 352 x 48 plate (49 node
-  // planes: 56 padded with 8, 54 with 9) the 8-high FP32 apply is 17 % faster; on the 96 x 96 x 16
-  // plate (17 planes: 24 against 18) the 9-high one is 10 % faster.
-  const bool nine = h->k0_reflect &&
-                    (h->s.fine_tz == 9 || (h->s.fine_tz == 0 && 100 * (((nz + 8) / 9) * 9) < 85 * (((nz + 7) / 8) * 8)));
+  const bool nine = fine_nine(h, a.g.nz);
   if (h->k0_reflect) {
     if (nine) {
       if (slot == 0) launch_fine_variant<T, 0, true, 9>(a, mode, st);
@@ -482,12 +502,7 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
     const int threads = TX * TY * tm.tz;
     const unsigned tiles = (unsigned)(tm.tiles_x * tm.tiles_y * tm.tiles_z);
     constexpr int cb = sizeof(T) == 4 ? CB32 : CB64;
-    // column groups of a tile launched side by side (its 27-point coefficients then stream from HBM
-    // once per tile instead of once per group), as long as the tiles fit the grid's y extent
-    const unsigned groups = (unsigned)((a.ncol + cb - 1) / cb);
-    const int groups_first = tiles <= 65535u ? 1 : 0;
-    dim3 grid = groups_first ? dim3(groups, tiles) : dim3(tiles, groups);
-    const size_t smem = sizeof(T) * 3 * HALO * cb;
+    constexpr size_t smem = stencil_smem_bytes<T, cb>();
     auto launch = [&](auto rnd) {
       constexpr int RND = decltype(rnd)::value;
       static bool configured = false;   // per instantiation and process; the attribute is per function
@@ -495,7 +510,7 @@ void launch_level(tf_handle* h, int l, LevelArgs<T> a, int mode, cudaStream_t st
         TF_CUDA_CHECK(cudaFuncSetAttribute(stencil_level_kernel<T, cb, RND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = true;
       }
-      stencil_level_kernel<T, cb, RND><<<grid, threads, smem, st>>>(a, mode, tm, groups_first);
+      stencil_level_kernel<T, cb, RND><<<dim3(tiles, (a.ncol + cb - 1) / cb), threads, smem, st>>>(a, mode, tm);
     };
     if (std::is_same<T, float>::value && a.round == 1) launch(std::integral_constant<int, 1>{});
     else if (std::is_same<T, float>::value && a.round == 2) launch(std::integral_constant<int, 2>{});
@@ -886,6 +901,25 @@ void fine_apply64(tf_handle* h, Hierarchy& hy, const double* u, const double* b,
   launch_level<double>(h, 0, a, mode, s, TIMER_FINE64);
 }
 
+// FP64 PCG operator q = K p that also leaves the partial sums of p . q for the step length
+// (topology_multigrid.py:424) in h->dotp, one per warp of each tile and column: the separate
+// curvature pass over p and q is not needed.
+void fine_apply64_curvature(tf_handle* h, Hierarchy& hy, const double* p, double* q, int ncol, const int* active, cudaStream_t s) {
+  LevelArgs<double> a{};
+  a.g = h->geo[0];
+  a.E = h->moduli64.as<double>();
+  a.mask = hy.lv[0].mask.as<uint8_t>();
+  a.u = p;
+  a.y = q;
+  a.colstride = 3 * a.g.nnode;
+  a.ncol = ncol;
+  a.active = active;
+  const size_t need = sizeof(double) * (size_t)fine_dot_stride(h, fine_nine(h, a.g.nz) ? 9 : 8) * ncol;
+  if (h->dotp.bytes < need) h->dotp.alloc(need);
+  a.dot_out = h->dotp.as<double>();
+  launch_level<double>(h, 0, a, MODE_APPLY, s, TIMER_FINE64);
+}
+
 // FP32 fine operator with mask: the operator of the mixed PCG's FP32 iterations, on the CUDA-core
 // stencil whatever the smoother uses (its accuracy bounds how far an FP32 stretch can reduce the
 // residual between two FP64 recomputations).
@@ -913,6 +947,9 @@ struct PcgResult {
   int steps = 0;
 };
 
+PcgResult pcg_finish(tf_handle* h, Hierarchy& hy, const PcgState& st, int ncol, const std::vector<int>& run, int step, bool running,
+                     cudaStream_t s);
+
 // Batched flexible PCG over `ncol` columns held in h->vb (rhs) / h->vx (solution).
 // `run` selects the columns; with `warm` the current h->vx is the start vector.
 //
@@ -935,6 +972,8 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
   R* r = static_cast<R*>(h->vr.p);
   R* p = static_cast<R*>(h->vp.p);
   R* q = mixed ? static_cast<R*>(h->vz.p) : static_cast<R*>(h->vq.p);
+  // the FP64 operator also forms the curvature p . q (fine_apply64_curvature)
+  constexpr bool fused = !mixed;
   double* t = h->vq.as<double>();   // b - K x in FP64 (shares vq with q in the FP64 PCG: q is consumed first)
   std::vector<int> zeros(ncol, 0);
   TF_CUDA_CHECK(cudaMemcpyAsync(st.active, run.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, s));
@@ -965,11 +1004,16 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
   for (int c = 0; c < ncol; ++c) n_active += run[c];
   while (n_active > 0 && step < limit) {
     if constexpr (mixed) fine_apply32(h, hy, p, q, ncol, st.active, s);
-    else fine_apply64(h, hy, p, nullptr, q, MODE_APPLY, ncol, st.active, nullptr, s);
+    else fine_apply64_curvature(h, hy, p, q, ncol, st.active, s);
     {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
-  pcg_alpha_kernel<R><<<gr, RED_THREADS, 0, s>>>(p, q, n, st);
+  if constexpr (fused) {
+    pcg_alpha_sum_kernel<<<ncol, RED_THREADS, 0, s>>>(h->dotp.as<double>(), fine_dot_stride(h, fine_nine(h, h->geo[0].nz) ? 9 : 8), st);
+    TF_LAUNCH_CHECK("pcg_alpha_sum_kernel");
+  } else {
+    pcg_alpha_kernel<R><<<gr, RED_THREADS, 0, s>>>(p, q, n, st);
     TF_LAUNCH_CHECK("pcg_alpha_kernel");
+  }
     ++step;
     pcg_update_kernel<T, R><<<gr, RED_THREADS, 0, s>>>(h->vx.as<double>(), r, p, q, vbufs<T>(h).x[0].template as<T>(), n, st, tol,
                                                        step, reliable);
@@ -991,12 +1035,20 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
     if (n_active == 0) break;
     precondition<T, R>(h, hy, ncol, st, 0, false, s);
   }
+  return pcg_finish(h, hy, st, ncol, run, step, n_active > 0, s);
+}
+
+// The per-column outcome of a PCG run that took `step` steps: with `running` (the iteration limit
+// stopped it) the columns still active get their final true residual (topology_multigrid.py:450-453).
+PcgResult pcg_finish(tf_handle* h, Hierarchy& hy, const PcgState& st, int ncol, const std::vector<int>& run, int step, bool running,
+                     cudaStream_t s) {
+  const long long n = 3 * h->geo[0].nnode;
   PcgResult res;
   res.steps = step;
-  if (n_active > 0) {
-    // iteration limit: final true residual of the columns still running (topology_multigrid.py:450-453)
+  if (running) {
+    double* t = h->vq.as<double>();
     fine_apply64(h, hy, h->vx.as<double>(), h->vb.as<double>(), t, MODE_RESID, ncol, st.active, nullptr, s);
-    pcg_norm_kernel<<<gr, RED_THREADS, 0, s>>>(t, n, st, st.rzo, 1);
+    pcg_norm_kernel<<<dim3(grid_for(n, RED_THREADS, PCG_BLOCKS), ncol), RED_THREADS, 0, s>>>(t, n, st, st.rzo, 1);
     TF_LAUNCH_CHECK("pcg_norm_kernel");
   }
   std::vector<int> act(ncol), it(ncol);
@@ -1295,6 +1347,135 @@ void check_tensor_core_error(tf_handle* h, cudaStream_t s) {
 
 // Shared body of tf_solve (start from zero) and tf_solve_guess (start from u_dev, the reference's
 // _pcg(..., initial), topology_multigrid.py:407-417).
+// The columns of f_dev whose norm is not negligible against the largest (topology_multigrid.py:350-351)
+// go to `live`; the others to `dead`, and their solutions are zeroed in u_dev.
+void split_columns(tf_handle* h, const double* f_dev, int32_t nrhs, double* u_dev, cudaStream_t s, std::vector<int>& live,
+                   std::vector<int>& dead) {
+  const long long nun = 3 * h->un.nnode;
+  std::vector<double> norms(nrhs, 0.0);
+  if (nrhs > 0) {
+    ensure_scratch(h, nrhs);
+    if (h->solve_small.bytes < sizeof(double) * nrhs) h->solve_small.alloc(sizeof(double) * nrhs);
+    colnorm_kernel<<<dim3(grid_for(nun, RED_THREADS, PCG_BLOCKS), nrhs), RED_THREADS, 0, s>>>(
+        f_dev, nun, h->solve_small.as<double>(), h->partial.as<double>(), h->count.as<unsigned>());
+    TF_LAUNCH_CHECK("colnorm_kernel");
+    TF_CUDA_CHECK(cudaMemcpyAsync(norms.data(), h->solve_small.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
+    TF_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
+  double mx = 0.0;
+  for (double v : norms) {
+    if (!std::isfinite(v)) throw Error(TF_INVALID, "forces must be finite");
+    mx = std::max(mx, v);
+  }
+  live.clear();
+  dead.clear();
+  for (int c = 0; c < nrhs; ++c) (norms[c] > h->s.zero_rhs * std::max(mx, 1e-300) ? live : dead).push_back(c);
+  if (!dead.empty()) {
+    // solve_small is reused in stream order: the norms above were read back before this copy
+    if (h->solve_small.bytes < sizeof(int) * dead.size()) h->solve_small.alloc(sizeof(int) * dead.size());
+    TF_CUDA_CHECK(cudaMemcpyAsync(h->solve_small.p, dead.data(), sizeof(int) * dead.size(), cudaMemcpyHostToDevice, s));
+    zero_flat_cols_kernel<<<dim3(grid_for(nun, 256), (unsigned)dead.size()), 256, 0, s>>>(u_dev, nun, h->solve_small.as<int>());
+    TF_LAUNCH_CHECK("zero_flat_cols_kernel");
+    TF_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
+}
+
+// Columns `cols` of f_dev (and with `warm` of u_dev) into the padded PCG layout h->vb (h->vx).
+void load_columns(tf_handle* h, Hierarchy& hy, const double* f_dev, double* u_dev, const std::vector<int>& cols, bool warm,
+                  cudaStream_t s) {
+  const long long nun = 3 * h->un.nnode;
+  const int nc = static_cast<int>(cols.size());
+  ensure_pcg(h, nc);
+  TF_CUDA_CHECK(cudaMemcpyAsync(h->colmap.p, cols.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
+  pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(f_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
+                                                            h->vb.as<double>(), h->colmap.as<int>());
+  TF_LAUNCH_CHECK("pad_kernel");
+  if (warm) {
+    // the caller's guess, masked like the forces; pcg then starts from r = b - A x
+    pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(u_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
+                                                              h->vx.as<double>(), h->colmap.as<int>());
+    TF_LAUNCH_CHECK("pad_kernel");
+  }
+}
+
+// The precise FP64 re-runs of the columns that missed the tolerance (topology_multigrid.py:376-406),
+// restarting from the previous iterate where it improved on zero (:393).
+void retry_columns(tf_handle* h, Hierarchy& hy, int nc, PcgResult& r, std::vector<double>& history, int& steps, int& retried,
+                   cudaStream_t s) {
+  const long long n = 3 * h->geo[0].nnode;
+  for (int attempt = 0; attempt < h->s.retries; ++attempt) {
+    std::vector<int> failed(nc, 0);
+    int nfail = 0;
+    for (int c = 0; c < nc; ++c)
+      if (!(r.rel[c] < h->s.tolerance)) { failed[c] = 1; ++nfail; }
+    if (!nfail) break;
+    std::vector<int> reset(nc, 0);
+    for (int c = 0; c < nc; ++c) reset[c] = failed[c] && !(r.rel[c] < 1.0);
+    // solve_small is reused in stream order (every user of it runs on stream s)
+    if (h->solve_small.bytes < sizeof(int) * nc) h->solve_small.alloc(sizeof(int) * nc);
+    TF_CUDA_CHECK(cudaMemcpyAsync(h->solve_small.p, reset.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
+    zero_cols_kernel<double><<<cols_grid(n, nc), 256, 0, s>>>(h->vx.as<double>(), n, h->solve_small.as<int>());
+    TF_LAUNCH_CHECK("zero_cols_kernel");
+    PcgResult again = pcg_precise(h, hy, nc, failed, s);
+    for (int c = 0; c < nc; ++c)
+      if (failed[c]) {
+        r.iters[c] += again.iters[c];
+        r.rel[c] = again.rel[c];
+      }
+    history.insert(history.end(), again.history.begin(), again.history.end());
+    steps += again.steps;
+    retried += nfail;
+  }
+}
+
+// Solutions of the block `cols` back to u_dev, and the block's per-column outcome.
+void store_columns(tf_handle* h, double* u_dev, const std::vector<int>& cols, const PcgResult& r, std::vector<int>& iters,
+                   std::vector<double>& rel, cudaStream_t s) {
+  const long long nun = 3 * h->un.nnode;
+  const int nc = static_cast<int>(cols.size());
+  unpad_kernel<<<cols_grid(h->un.nnode, nc), 256, 0, s>>>(h->vx.as<double>(), h->un, h->geo[0], u_dev, nun, h->colmap.as<int>());
+  TF_LAUNCH_CHECK("unpad_kernel");
+  for (int c = 0; c < nc; ++c) {
+    iters[cols[c]] = r.iters[c];
+    rel[cols[c]] = r.rel[c];
+  }
+}
+
+struct SolveTally {
+  std::vector<int> live, dead, iters;
+  std::vector<double> rel, history;
+  int batches = 0, retried = 0, steps = 0;
+};
+
+void fill_solve_report(tf_handle* h, Hierarchy& hy, tf_report* report, int32_t nrhs, const SolveTally& t,
+                       std::chrono::steady_clock::time_point t0) {
+  bool converged = true;
+  for (int c : t.live) converged &= t.rel[c] < h->s.tolerance;
+  if (report) {
+    if (report->iterations)
+      for (int c = 0; c < nrhs; ++c) report->iterations[c] = t.iters[c];
+    if (report->relative_residual)
+      for (int c = 0; c < nrhs; ++c) report->relative_residual[c] = t.rel[c];
+    report->history_len = 0;
+    if (report->history)
+      for (double v : t.history) {
+        if (report->history_len >= report->history_capacity) break;
+        report->history[report->history_len++] = v;
+      }
+    report->converged = converged ? 1 : 0;
+    report->batches = t.batches;
+    report->retried_columns = t.retried;
+    report->zero_rhs_columns = static_cast<int>(t.dead.size());
+    report->steps = t.steps;
+    report->levels = h->nlev;
+    report->coarsest_dofs = hy.n_live;
+    report->setup_s = hy.setup_reported ? 0.0 : hy.setup_s;
+    for (int l = 0; l < 16; ++l) report->lambda_max[l] = (l + 1 < h->nlev) ? hy.lv[l].lambda_max : 0.0;
+    report->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  hy.setup_reported = true;
+}
+
 int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report, void* stream,
                bool warm) {
   return guard(h, [&] {
@@ -1303,119 +1484,119 @@ int solve_impl(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, do
     require(nrhs == 0 || (f_dev && u_dev), "forces and solution must not be NULL");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Hierarchy& hy = get_hierarchy(h, key, s);
-    const long long nun = 3 * h->un.nnode;
-    const long long n = 3 * h->geo[0].nnode;
-    // zero-RHS columns (topology_multigrid.py:350-351)
-    std::vector<double> norms(nrhs, 0.0);
-    if (nrhs > 0) {
-      ensure_scratch(h, nrhs);
-      if (h->solve_small.bytes < sizeof(double) * nrhs) h->solve_small.alloc(sizeof(double) * nrhs);
-      colnorm_kernel<<<dim3(grid_for(nun, RED_THREADS, PCG_BLOCKS), nrhs), RED_THREADS, 0, s>>>(
-          f_dev, nun, h->solve_small.as<double>(), h->partial.as<double>(), h->count.as<unsigned>());
-      TF_LAUNCH_CHECK("colnorm_kernel");
-      TF_CUDA_CHECK(cudaMemcpyAsync(norms.data(), h->solve_small.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
-      TF_CUDA_CHECK(cudaStreamSynchronize(s));
-    }
-    double mx = 0.0;
-    for (double v : norms) {
-      if (!std::isfinite(v)) throw Error(TF_INVALID, "forces must be finite");
-      mx = std::max(mx, v);
-    }
-    std::vector<int> live, dead;
-    for (int c = 0; c < nrhs; ++c) (norms[c] > h->s.zero_rhs * std::max(mx, 1e-300) ? live : dead).push_back(c);
-    std::vector<int> iters(nrhs, 0);
-    std::vector<double> rel(nrhs, 0.0);
-    std::vector<double> history;
-    int batches = 0, retried = 0, steps = 0;
-    if (!dead.empty()) {
-      // solve_small is reused in stream order: the norms above were read back before this copy
-      if (h->solve_small.bytes < sizeof(int) * dead.size()) h->solve_small.alloc(sizeof(int) * dead.size());
-      TF_CUDA_CHECK(cudaMemcpyAsync(h->solve_small.p, dead.data(), sizeof(int) * dead.size(), cudaMemcpyHostToDevice, s));
-      zero_flat_cols_kernel<<<dim3(grid_for(nun, 256), (unsigned)dead.size()), 256, 0, s>>>(u_dev, nun, h->solve_small.as<int>());
-      TF_LAUNCH_CHECK("zero_flat_cols_kernel");
-      TF_CUDA_CHECK(cudaStreamSynchronize(s));
-    }
-    const int chunk = h->s.batch > 0 ? h->s.batch : std::max<int>(1, static_cast<int>(live.size()));
-    for (size_t start = 0; start < live.size(); start += chunk) {
-      const int nc = static_cast<int>(std::min<size_t>(chunk, live.size() - start));
-      std::vector<int> cols(live.begin() + start, live.begin() + start + nc);
-      ensure_pcg(h, nc);
-      TF_CUDA_CHECK(cudaMemcpyAsync(h->colmap.p, cols.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
-      pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(f_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
-                                                                h->vb.as<double>(), h->colmap.as<int>());
-      TF_LAUNCH_CHECK("pad_kernel");
-      if (warm) {
-        // the caller's guess, masked like the forces; pcg then starts from r = b - A x
-        pad_kernel<<<cols_grid(h->geo[0].nnode, nc), 256, 0, s>>>(u_dev, nun, h->un, h->geo[0], hy.lv[0].mask.as<uint8_t>(),
-                                                                  h->vx.as<double>(), h->colmap.as<int>());
-        TF_LAUNCH_CHECK("pad_kernel");
-      }
+    SolveTally t;
+    split_columns(h, f_dev, nrhs, u_dev, s, t.live, t.dead);
+    t.iters.assign(nrhs, 0);
+    t.rel.assign(nrhs, 0.0);
+    const int chunk = h->s.batch > 0 ? h->s.batch : std::max<int>(1, static_cast<int>(t.live.size()));
+    for (size_t start = 0; start < t.live.size(); start += chunk) {
+      const int nc = static_cast<int>(std::min<size_t>(chunk, t.live.size() - start));
+      std::vector<int> cols(t.live.begin() + start, t.live.begin() + start + nc);
+      load_columns(h, hy, f_dev, u_dev, cols, warm, s);
       std::vector<int> run(nc, 1);
       PcgResult r = work_is_double(h) ? pcg<double, double>(h, hy, nc, run, warm, s)
                     : (h->s.pcg_precision == TF_PRECISION_FLOAT32 ? pcg<float, float>(h, hy, nc, run, warm, s)
                                                                   : pcg<float, double>(h, hy, nc, run, warm, s));
-      history.insert(history.end(), r.history.begin(), r.history.end());
-      steps += r.steps;
-      for (int attempt = 0; attempt < h->s.retries; ++attempt) {
-        std::vector<int> failed(nc, 0);
-        int nfail = 0;
-        for (int c = 0; c < nc; ++c)
-          if (!(r.rel[c] < h->s.tolerance)) { failed[c] = 1; ++nfail; }
-        if (!nfail) break;
-        // restart from the previous iterate where it improved on zero (topology_multigrid.py:393)
-        std::vector<int> reset(nc, 0);
-        for (int c = 0; c < nc; ++c) reset[c] = failed[c] && !(r.rel[c] < 1.0);
-        // solve_small is reused in stream order (every user of it runs on stream s)
-        if (h->solve_small.bytes < sizeof(int) * nc) h->solve_small.alloc(sizeof(int) * nc);
-        TF_CUDA_CHECK(cudaMemcpyAsync(h->solve_small.p, reset.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
-        zero_cols_kernel<double><<<cols_grid(n, nc), 256, 0, s>>>(h->vx.as<double>(), n, h->solve_small.as<int>());
-        TF_LAUNCH_CHECK("zero_cols_kernel");
-        PcgResult again = pcg_precise(h, hy, nc, failed, s);
-        for (int c = 0; c < nc; ++c)
-          if (failed[c]) {
-            r.iters[c] += again.iters[c];
-            r.rel[c] = again.rel[c];
-          }
-        history.insert(history.end(), again.history.begin(), again.history.end());
-        steps += again.steps;
-        retried += nfail;
-      }
-      unpad_kernel<<<cols_grid(h->un.nnode, nc), 256, 0, s>>>(h->vx.as<double>(), h->un, h->geo[0], u_dev, nun, h->colmap.as<int>());
-      TF_LAUNCH_CHECK("unpad_kernel");
-      for (int c = 0; c < nc; ++c) {
-        iters[cols[c]] = r.iters[c];
-        rel[cols[c]] = r.rel[c];
-      }
-      ++batches;
+      t.history.insert(t.history.end(), r.history.begin(), r.history.end());
+      t.steps += r.steps;
+      retry_columns(h, hy, nc, r, t.history, t.steps, t.retried, s);
+      store_columns(h, u_dev, cols, r, t.iters, t.rel, s);
+      ++t.batches;
     }
     TF_CUDA_CHECK(cudaStreamSynchronize(s));
     check_tensor_core_error(h, s);
-    bool converged = true;
-    for (int c : live) converged &= rel[c] < h->s.tolerance;
-    if (report) {
-      if (report->iterations)
-        for (int c = 0; c < nrhs; ++c) report->iterations[c] = iters[c];
-      if (report->relative_residual)
-        for (int c = 0; c < nrhs; ++c) report->relative_residual[c] = rel[c];
-      report->history_len = 0;
-      if (report->history)
-        for (double v : history) {
-          if (report->history_len >= report->history_capacity) break;
-          report->history[report->history_len++] = v;
-        }
-      report->converged = converged ? 1 : 0;
-      report->batches = batches;
-      report->retried_columns = retried;
-      report->zero_rhs_columns = static_cast<int>(dead.size());
-      report->steps = steps;
-      report->levels = h->nlev;
-      report->coarsest_dofs = hy.n_live;
-      report->setup_s = hy.setup_reported ? 0.0 : hy.setup_s;
-      for (int l = 0; l < 16; ++l) report->lambda_max[l] = (l + 1 < h->nlev) ? hy.lv[l].lambda_max : 0.0;
-      report->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    }
-    hy.setup_reported = true;
+    fill_solve_report(h, hy, report, nrhs, t, t0);
   });
+}
+
+#include "tf_solve_batch.cuh"
+
+// tf_solve_batch: the instances' set-up (hierarchies, zero columns, the padded right-hand sides) one
+// by one, their PCG runs in lockstep (pcg_batch), then each instance's retries and results as in
+// tf_solve.
+template <typename T>
+void solve_batch_run(tf_handle* const* hs, const uint64_t* keys, int count, const double* const* f_dev, const int32_t* nrhs,
+                     double* const* u_dev, tf_report* reports, cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<BatchSolve> inst(count);
+  std::vector<SolveTally> tally(count);
+  Group all;
+  for (int i = 0; i < count; ++i) {
+    tf_handle* h = hs[i];
+    BatchSolve& b = inst[i];
+    b.h = h;
+    b.hy = &get_hierarchy(h, keys[i], s);
+    SolveTally& t = tally[i];
+    split_columns(h, f_dev[i], nrhs[i], u_dev[i], s, t.live, t.dead);
+    t.iters.assign(nrhs[i], 0);
+    t.rel.assign(nrhs[i], 0.0);
+    b.ncol = static_cast<int>(t.live.size());
+    if (b.ncol == 0) continue;
+    require(h->s.batch <= 0 || h->s.batch >= b.ncol, "tf_solve_batch runs each instance's live columns as one block: "
+                                                      "settings.batch must be 0 or at least the live column count");
+    load_columns(h, *b.hy, f_dev[i], u_dev[i], t.live, false, s);
+    b.run.assign(b.ncol, 1);
+    all.push_back(&b);
+  }
+  if (!all.empty()) pcg_batch<T>(all, s);
+  for (int i = 0; i < count; ++i) {
+    BatchSolve& b = inst[i];
+    SolveTally& t = tally[i];
+    if (b.ncol > 0) {
+      PcgResult& r = b.res;
+      t.history.insert(t.history.end(), r.history.begin(), r.history.end());
+      t.steps += r.steps;
+      retry_columns(b.h, *b.hy, b.ncol, r, t.history, t.steps, t.retried, s);
+      store_columns(b.h, u_dev[i], t.live, r, t.iters, t.rel, s);
+      t.batches = 1;
+    }
+  }
+  TF_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int i = 0; i < count; ++i)
+    fill_solve_report(inst[i].h, *inst[i].hy, reports ? &reports[i] : nullptr, nrhs[i], tally[i], t0);
+}
+
+int solve_batch_impl(tf_handle* const* hs, const uint64_t* keys, int32_t count, const double* const* f_dev, const int32_t* nrhs,
+                     double* const* u_dev, tf_report* reports, void* stream) {
+  std::string where = "tf_solve_batch: ";
+  try {
+    require(count >= 1, "count must be positive");
+    require(hs && keys && f_dev && nrhs && u_dev, "handles, keys, forces, column counts and solutions must not be NULL");
+    for (int i = 0; i < count; ++i) require(hs[i] != nullptr, "handle " + std::to_string(i) + " is NULL");
+    const tf_settings& s0 = hs[0]->s;
+    for (int i = 0; i < count; ++i) {
+      for (int j = 0; j < i; ++j) require(hs[j] != hs[i], "each instance needs its own handle (handles " + std::to_string(j) + " and " +
+                                                            std::to_string(i) + " are the same)");
+      require(nrhs[i] >= 0, "nrhs must be non-negative");
+      require(nrhs[i] == 0 || (f_dev[i] && u_dev[i]), "forces and solution must not be NULL");
+      const tf_settings& si = hs[i]->s;
+      require(si.pcg_precision == TF_PRECISION_FLOAT64, "tf_solve_batch runs the FP64 PCG (settings.pcg_precision float64)");
+      require(!si.tensor_cores, "tf_solve_batch runs the CUDA-core finest-level operator (settings.tensor_cores 0)");
+      require(si.cycle == TF_CYCLE_V, "tf_solve_batch runs V-cycles");
+      require(si.precision == s0.precision && si.smoother == s0.smoother && si.sweeps == s0.sweeps &&
+                  si.chebyshev_degree == s0.chebyshev_degree && si.growth == s0.growth && si.chebyshev_ratio == s0.chebyshev_ratio &&
+                  si.damping == s0.damping,
+              "the instances of a batch share the V-cycle settings (precision, smoother, sweeps, degree, growth, ratio, damping)");
+      require(hs[i]->k0_reflect == hs[0]->k0_reflect && std::memcmp(hs[i]->ke, hs[0]->ke, sizeof(hs[0]->ke)) == 0,
+              "the instances of a batch share the element stiffness ke");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (work_is_double(hs[0])) solve_batch_run<double>(hs, keys, count, f_dev, nrhs, u_dev, reports, s);
+    else solve_batch_run<float>(hs, keys, count, f_dev, nrhs, u_dev, reports, s);
+    return TF_OK;
+  } catch (const Error& e) {
+    const std::string msg = where + e.what();
+    record_unhandled_error(msg);
+    for (int i = 0; hs && i < count; ++i)
+      if (hs[i]) hs[i]->err = msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    const std::string msg = where + e.what();
+    record_unhandled_error(msg);
+    for (int i = 0; hs && i < count; ++i)
+      if (hs[i]) hs[i]->err = msg;
+    return TF_INTERNAL;
+  }
 }
 }  // namespace
 
@@ -1423,6 +1604,11 @@ extern "C" int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t
                         void* stream) {
   if (!h) return TF_INVALID;
   return solve_impl(h, key, f_dev, nrhs, u_dev, report, stream, false);
+}
+
+extern "C" int tf_solve_batch(tf_handle* const* handles, const uint64_t* keys, int32_t count, const double* const* f_dev,
+                              const int32_t* nrhs, double* const* u_dev, tf_report* reports, void* stream) {
+  return solve_batch_impl(handles, keys, count, f_dev, nrhs, u_dev, reports, stream);
 }
 
 extern "C" int tf_solve_guess(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,

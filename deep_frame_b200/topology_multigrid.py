@@ -225,6 +225,38 @@ class GeometricMultigrid:
         report["seconds"] = perf_counter() - started
         return flat, report
 
+    def _report_arrays(self, count):
+        iterations = np.zeros(count, dtype=np.int32)
+        relative = np.zeros(count, dtype=np.float64)
+        history = np.zeros(self.settings["max_iterations"] * (1 + self.settings["retries"]) + 8, dtype=np.float64)
+        report = _lib.TfReport()
+        report.iterations = iterations.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        report.relative_residual = relative.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        report.history = history.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        report.history_capacity = len(history)
+        return report, (iterations, relative, history)
+
+    def _result(self, report, arrays, started):
+        iterations, relative, history = arrays
+        levels = int(report.levels)
+        result = {"iterations": iterations.tolist(), "relative_residual": relative.tolist(),
+                  "converged": bool(report.converged), "history": [history[:report.history_len].tolist()],
+                  "batches": int(report.batches), "retried_columns": int(report.retried_columns),
+                  "zero_rhs_columns": int(report.zero_rhs_columns), "seconds": perf_counter() - started,
+                  "setup_s": float(report.setup_s), "floating": False, "levels": levels,
+                  "coarsest_dofs": int(report.coarsest_dofs), "kernel": 0, "rhs_kernel_component": None,
+                  "kernel_check": [], "lambda_max": [float(report.lambda_max[i]) for i in range(levels - 1)],
+                  "steps": int(report.steps)}
+        self.statistics.append(result)
+        return result
+
+    def _check_forces(self, forces):
+        torch = self.torch
+        if self.moduli is None:
+            raise ValueError("update(moduli) must be called before solve")
+        if forces.dtype != torch.float64 or not forces.is_cuda or not forces.is_contiguous() or forces.shape[-1] != self.ndof:
+            raise ValueError("forces must be a contiguous CUDA float64 [R, ndof] tensor")
+
     def solve_device(self, key, fixed, forces, out=None, support=None, initial=None):
         """Device-resident solve: forces [R, ndof] contiguous CUDA float64; returns (u [R, ndof], report).
 
@@ -240,10 +272,7 @@ class GeometricMultigrid:
         if support is not None and not np.isin(np.asarray(support, dtype=np.int64), np.asarray(fixed, dtype=np.int64)).all():
             raise ValueError("support dofs must be part of fixed")
         started = perf_counter()
-        if self.moduli is None:
-            raise ValueError("update(moduli) must be called before solve")
-        if forces.dtype != torch.float64 or not forces.is_cuda or not forces.is_contiguous() or forces.shape[-1] != self.ndof:
-            raise ValueError("forces must be a contiguous CUDA float64 [R, ndof] tensor")
+        self._check_forces(forces)
         count = forces.shape[0]
         ident = self._key((key, False), fixed)
         out = torch.empty_like(forces) if out is None else out
@@ -252,28 +281,11 @@ class GeometricMultigrid:
                 raise ValueError("initial must be a CUDA float64 tensor shaped like forces")
             if initial.data_ptr() != out.data_ptr():
                 out.copy_(initial)
-        iterations = np.zeros(count, dtype=np.int32)
-        relative = np.zeros(count, dtype=np.float64)
-        history = np.zeros(self.settings["max_iterations"] * (1 + self.settings["retries"]) + 8, dtype=np.float64)
-        report = _lib.TfReport()
-        report.iterations = iterations.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
-        report.relative_residual = relative.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        report.history = history.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        report.history_capacity = len(history)
+        report, arrays = self._report_arrays(count)
         entry = self.lib.tf_solve if initial is None else self.lib.tf_solve_guess
         _lib.check(entry(self.handle, ident, _lib.ptr(forces), count, _lib.ptr(out), ctypes.byref(report), self._stream()),
                    self.handle, "tf_solve" if initial is None else "tf_solve_guess")
-        levels = int(report.levels)
-        result = {"iterations": iterations.tolist(), "relative_residual": relative.tolist(),
-                  "converged": bool(report.converged), "history": [history[:report.history_len].tolist()],
-                  "batches": int(report.batches), "retried_columns": int(report.retried_columns),
-                  "zero_rhs_columns": int(report.zero_rhs_columns), "seconds": perf_counter() - started,
-                  "setup_s": float(report.setup_s), "floating": False, "levels": levels,
-                  "coarsest_dofs": int(report.coarsest_dofs), "kernel": 0, "rhs_kernel_component": None,
-                  "kernel_check": [], "lambda_max": [float(report.lambda_max[i]) for i in range(levels - 1)],
-                  "steps": int(report.steps)}
-        self.statistics.append(result)
-        return out, result
+        return out, self._result(report, arrays, started)
 
     def precondition(self, hierarchy, residual):
         """One V-cycle z = M^-1 r of `hierarchy` on a residual grid [R, 3, padded nodes]."""
@@ -518,6 +530,46 @@ class GeometricMultigrid:
             self.close()
         except Exception:
             pass
+
+
+def solve_batch_device(jobs):
+    """Several independent solves at once (tf_solve_batch): every PCG and V-cycle stage runs as one
+    launch over all of them.  ``jobs`` = [(multigrid, key, fixed, forces)], one GeometricMultigrid
+    (its own handle) per job, forces a contiguous CUDA float64 [R, ndof] tensor; returns
+    [(u [R, ndof], report)] in job order, each what that job's solve_device would return.  The
+    instances share the element stiffness and the V-cycle settings and run the FP64 PCG."""
+    if not jobs:
+        return []
+    torch = jobs[0][0].torch
+    started = perf_counter()
+    count = len(jobs)
+    handles = (ctypes.c_void_p * count)()
+    keys = (ctypes.c_uint64 * count)()
+    forces_p = (ctypes.c_void_p * count)()
+    outs_p = (ctypes.c_void_p * count)()
+    nrhs = (ctypes.c_int32 * count)()
+    reports = (_lib.TfReport * count)()
+    outs, arrays = [], []
+    seen = set()
+    for i, (mg, key, fixed, forces) in enumerate(jobs):
+        if id(mg) in seen:
+            raise ValueError("each job needs its own GeometricMultigrid")
+        seen.add(id(mg))
+        mg._check_forces(forces)
+        keys[i] = mg._key((key, False), fixed)
+        handles[i] = mg.handle
+        out = torch.empty_like(forces)
+        outs.append(out)
+        forces_p[i] = _lib.ptr(forces)
+        outs_p[i] = _lib.ptr(out)
+        nrhs[i] = forces.shape[0]
+        report, held = mg._report_arrays(forces.shape[0])
+        reports[i] = report
+        arrays.append(held)
+    lib = jobs[0][0].lib
+    _lib.check(lib.tf_solve_batch(handles, keys, count, forces_p, nrhs, outs_p, reports, jobs[0][0]._stream()), None,
+               "tf_solve_batch")
+    return [(outs[i], jobs[i][0]._result(reports[i], arrays[i], started)) for i in range(count)]
 
 
 def solve_elasticity(system, multigrid, physical_density, penalization=3.0, min_stiffness_ratio=1e-6):

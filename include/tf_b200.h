@@ -134,6 +134,19 @@ TF_API int tf_solve(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrh
 TF_API int tf_solve_guess(tf_handle* h, uint64_t key, const double* f_dev, int32_t nrhs, double* u_dev, tf_report* report,
                           void* stream);
 
+/* tf_solve over `count` independent instances at once: instance i solves hierarchy keys[i] of
+ * handles[i] for f_dev[i] [nrhs[i]][ndof_i] into u_dev[i], reports[i] (reports may be NULL).
+ * The result of each instance is that of its own tf_solve (the same PCG, convergence test and
+ * retries, topology_multigrid.py:336-454); the difference is the schedule: every PCG and V-cycle
+ * stage runs as one launch over all instances' blocks, in place of one launch per instance
+ * (the reference solves one problem per call, with the columns of one load set batched,
+ * topology_multigrid.py:353-362).  Each instance needs its own handle; all share the element
+ * stiffness ke and the V-cycle settings, run the FP64 PCG (pcg_precision float64) with V-cycles
+ * on the CUDA-core operators, and solve their live columns as one block (settings.batch 0 or at
+ * least that count).  One stream for all. */
+TF_API int tf_solve_batch(tf_handle* const* handles, const uint64_t* keys, int32_t count, const double* const* f_dev,
+                          const int32_t* nrhs, double* const* u_dev, tf_report* reports, void* stream);
+
 /* Mass operator of GeometricMultigrid.eigenpairs (topology_multigrid.py:491-496): y = mask *
  * (sum_e mass_e M0 (mask u)_e + lumped * u), with M0 the `me` given to tf_create, mass_dev the
  * element masses [nelem] (unpadded, C order), lumped_dev the lumped nodal masses [ndof] (may be

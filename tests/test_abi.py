@@ -73,6 +73,12 @@ def test_handleless_failures_carry_a_message(library):
     assert lib.tf_simp(None, 10, 3.0, 1e-9, 1.0, None, None, None, None, None) == 1
     assert lib.tf_last_error(None).startswith(b"tf_simp:")
     assert lib.tf_combine(None, 3, 10, None, 65, None, None) == 1 and lib.tf_last_error(None).startswith(b"tf_combine:")
+    assert lib.tf_solve_batch(None, None, 0, None, None, None, None, None) == 1
+    assert lib.tf_last_error(None).startswith(b"tf_solve_batch: count")
+    handles = (P * 2)()
+    keys, counts, ptrs = (ctypes.c_uint64 * 2)(), (ctypes.c_int32 * 2)(1, 1), (P * 2)()
+    assert lib.tf_solve_batch(handles, keys, 2, ptrs, counts, ptrs, None, None) == 1
+    assert b"handle 0 is NULL" in lib.tf_last_error(None)
 
 
 @pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the path of a host without a CUDA device")
