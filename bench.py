@@ -69,6 +69,7 @@ def parse(argv=None):
     ap.add_argument("--instances", type=int, default=0,
                     help="solve N independent seeded plates of uneven size and RHS count concurrently and report solves/s")
     ap.add_argument("--learned", action="store_true", help="train the learned initial guess and report PCG with / without it")
+    ap.add_argument("--learned-epochs", type=int, default=4, help="training epochs of --learned")
     ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
     ap.add_argument("--simp-compare", action="store_true", help="also run the plain FP64 V-cycle and compare the designs")
     ap.add_argument("--warm-start", type=int, default=0, nargs="?", const=-1,
@@ -614,41 +615,53 @@ def instances(args):
 
 
 def learned_guess(args):
-    """--learned: train the convolutional initial guess on SIMP snapshots of a 48 x 48 x 8 plate (seed 0),
-    then time one covariance solve (2 x 42 columns to 1e-8) from zero and from the network's guess
-    (inference included) on held-out densities: a later design of a seed-1 trajectory at the training
-    size, the seeded 96 x 96 x 16 plate density and the seeded 192 x 192 x 32 plate density."""
+    """--learned: train the four-level convolutional initial guess (channels 16, 32, 48, 64) on about
+    2,000 load-column snapshots of seeded 96 x 96 x 16 covariance-plate SIMP trajectories (seeds 0-2,
+    16 designs each, every second column of both halves), then time one covariance solve (2 x 42
+    columns to 1e-8) from zero and from the network's guess (tensor-core FP16 inference included) on
+    held-out designs: the 12th design of a seed-7 trajectory at 96 x 96 x 16 and the seeded
+    192 x 192 x 32 plate density."""
     import torch
     from deep_frame_b200 import learned, problems
-    settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 2, "growth": 1.5}
-    train_shape = (48, 48, 8)
-    domain, _, cov = problems.plate(train_shape, 0)
+    from deep_frame_b200.elasticity import HexElasticity
+    settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0}
+    train_shape = (96, 96, 16)
+    channels = (16, 32, 48, 64)
     t0 = time.perf_counter()
-    snapshots, live, grid = learned.record_trajectory(domain, cov, 16, multigrid=settings)
+    snapshots, live, grid = [], None, None
+    for seed in (0, 1, 2):
+        domain, _, cov = problems.plate(train_shape, seed)
+        part, live_part, grid = learned.record_trajectory(domain, cov, 16, multigrid=settings, stride=2)
+        snapshots += part
+        live = live_part
     record_s = time.perf_counter() - t0
-    net = learned.GuessNet(channels=(8, 16, 32), seed=0)
+    count = int(sum(1 for _ in learned.samples(snapshots, live, grid)))
+    net = learned.GuessNet(channels=channels, seed=0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    losses = learned.train(net, snapshots, live, grid, epochs=6, batch=8, lr=2e-3)
+    losses = learned.train(net, snapshots, live, grid, epochs=args.learned_epochs, batch=8, lr=2e-3)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
+    del snapshots
+    net.pack()
     cases = {}
-    held_domain, _, held_cov = problems.plate(train_shape, 1)
-    held, _, _ = learned.record_trajectory(held_domain, held_cov, 12, multigrid=settings)
-    cases["plate_48x48x8_seed1_design12"] = learned.compare(net, held_domain, held_cov, held[-1][0], multigrid=settings)
-    for shape in ((96, 96, 16), (192, 192, 32)):
-        dom, density, cv = problems.plate(shape, 0)
-        from deep_frame_b200.elasticity import HexElasticity
-        moduli = HexElasticity(dom, multigrid=settings).moduli(density, 3.0, 1e-9)[0]
-        cases["plate_%dx%dx%d" % shape] = learned.compare(net, dom, cv, moduli, multigrid=settings)
+    held_domain, _, held_cov = problems.plate(train_shape, 7)
+    held, _, _ = learned.record_trajectory(held_domain, held_cov, 12, multigrid=settings, stride=1000)
+    cases["plate_96x96x16_seed7_design12"] = learned.compare(net, held_domain, held_cov, held[-1][0], multigrid=settings)
+    dom, density, cv = problems.plate((192, 192, 32), 0)
+    moduli = HexElasticity(dom, multigrid=settings).moduli(density, 3.0, 1e-9)[0]
+    cases["plate_192x192x32"] = learned.compare(net, dom, cv, moduli, multigrid=settings)
     policy = learned.GuessPolicy(net)
     for row in cases.values():
-        policy.assess(row["network"]["mean_iterations"], row["zero"]["mean_iterations"])
+        policy.assess(row["network"]["mean_iterations"], row["zero"]["mean_iterations"], row["network"]["seconds"], row["zero"]["seconds"])
     line = {"metric": "PCG iterations / seconds to 1e-8 with and without the learned initial guess", "unit": "iterations",
             "n_gpus": 1, "data": "synthetic (SIMP trajectory snapshots of seeded plates)",
-            "config": {"network": "3-level conv encoder/decoder, channels (8, 16, 32), 9 conv layers, FP32, hand-written kernels",
-                       "training": {"shape": list(train_shape), "designs": len(snapshots), "samples": int(sum(1 for _ in learned.samples(snapshots, live, grid))),
-                                    "epochs": 6, "losses": [round(v, 5) for v in losses], "record_s": round(record_s, 2), "train_s": round(train_s, 2)},
+            "config": {"network": f"{len(channels)}-level conv encoder/decoder, channels {channels}, {len(net.specs)} conv layers; "
+                                  "training in FP32 (im2col + own SGEMM), inference on the tensor cores (tcgen05 kind::f16, "
+                                  "FP16 weights and activations, FP32 accumulation)",
+                       "training": {"shape": list(train_shape), "seeds": [0, 1, 2], "designs": 48, "samples": count,
+                                    "epochs": args.learned_epochs, "losses": [round(v, 5) for v in losses],
+                                    "record_s": round(record_s, 2), "train_s": round(train_s, 2)},
                        "solver": settings},
             "cases": {name: {label: {k: (round(v, 4) if isinstance(v, float) else v) for k, v in row[label].items() if k != "iterations"}
                              for label in row} for name, row in cases.items()},

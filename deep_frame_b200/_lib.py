@@ -23,7 +23,7 @@ SYMBOLS += ("tf_filter_create", "tf_filter_apply", "tf_filter_sums", "tf_filter_
             "tf_filter_destroy",
             "tf_filter_last_error", "tf_mma_create", "tf_mma_step", "tf_mma_destroy", "tf_mma_last_error", "tf_simp",
             "tf_chol_create", "tf_chol_factor_csr", "tf_chol_solve", "tf_chol_destroy", "tf_chol_last_error")
-SYMBOLS += ("tf_nn_last_error", "tf_nn_gemm", "tf_nn_im2col", "tf_nn_col2im", "tf_nn_bias_act", "tf_nn_act_back", "tf_nn_pool",
+SYMBOLS += ("tf_nn_last_error", "tf_nn_gemm", "tf_nn_pack16", "tf_nn_conv16", "tf_nn_im2col", "tf_nn_col2im", "tf_nn_bias_act", "tf_nn_act_back", "tf_nn_pool",
             "tf_nn_resample", "tf_nn_mse", "tf_nn_mse_scratch_doubles", "tf_nn_adam")
 TIMER_CLASSES = ("fine_fp64", "fine_work", "coarse", "transfer", "vector", "coarsest", "setup", "energy", "fine_pcg32")
 
@@ -126,6 +126,8 @@ def load():
             "tf_chol_last_error": [P],
             "tf_nn_last_error": [],
             "tf_nn_gemm": [I32, I32, I32, I32, I32, ctypes.c_float, P, I32, P, I32, ctypes.c_float, P, I32, P, I64, P],
+            "tf_nn_pack16": [P, I32, I32, P, I32, I32, P],
+            "tf_nn_conv16": [P, I32, P, P, I32, I32, I32, P, I32, P, P, P],
             "tf_nn_im2col": [P, I32, P, P, P],
             "tf_nn_col2im": [P, I32, P, P, P],
             "tf_nn_bias_act": [P, P, I32, I64, I32, P],

@@ -777,7 +777,10 @@ __global__ void restrict_kernel(Geo fine, Geo coarse, const T* __restrict__ r, l
   restrict_body<T>(vgrid(), fine, coarse, r, fstride, out, cstride, cmask, active, round);
 }
 
-// x_fine += mask * P c  (P = transpose of the restriction)
+// x_fine += mask * P c  (P = transpose of the restriction).  One thread per coarse node I (and
+// column) loads the 8 coarse values of the cell I..I+1 once and updates the up to 8 fine nodes
+// 2I..2I+1 that take their correction from that cell (each fine node belongs to exactly one cell);
+// every fine node sums its coarse contributions in the same order as a per-fine-node loop would.
 template <typename T>
 __device__ __forceinline__ void prolong_add_body(const VGrid vg_,Geo fine, Geo coarse, const T* __restrict__ c, long long cstride, T* __restrict__ x,
                                    long long fstride, const uint8_t* __restrict__ fmask, const int* __restrict__ active, int round) {
@@ -786,45 +789,64 @@ __device__ __forceinline__ void prolong_add_body(const VGrid vg_,Geo fine, Geo c
   if (active && !active[col]) return;
   const T* cc = c + col * cstride;
   T* xc = x + col * fstride;
-  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < fine.nnode; n += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    node_coords(n, fine, i, j, k);
-    int I0[3], I1[3];
-    T w0[3], w1[3];
-    const int idx[3] = {i, j, k};
-    const int lim[3] = {coarse.nx, coarse.ny, coarse.nz};
+  for (long long cn = (long long)blockIdx.x * blockDim.x + threadIdx.x; cn < coarse.nnode; cn += (long long)gridDim.x * blockDim.x) {
+    int I, J, K;
+    node_coords(cn, coarse, I, J, K);
+    const bool hx = I + 1 < coarse.nx, hy = J + 1 < coarse.ny, hz = K + 1 < coarse.nz;
+    T cv[8][3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      if ((idx[d] & 1) == 0) { I0[d] = idx[d] >> 1; w0[d] = T(1); I1[d] = -1; w1[d] = T(0); }
-      else { I0[d] = (idx[d] - 1) >> 1; w0[d] = T(0.5); I1[d] = (idx[d] + 1) >> 1; w1[d] = T(0.5); }
-      if (I1[d] >= lim[d]) { I1[d] = -1; }
-    }
-    T acc0 = T(0), acc1 = T(0), acc2 = T(0);
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int a = 0; a < 2; ++a) {
-      const int ci = a ? I1[0] : I0[0];
-      const T wa = a ? w1[0] : w0[0];
-      if (ci < 0) continue;
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const int cj = b ? I1[1] : I0[1];
-        const T wb = b ? w1[1] : w0[1];
-        if (cj < 0) continue;
+      for (int b = 0; b < 2; ++b)
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          const int ck = q ? I1[2] : I0[2];
-          const T wq = q ? w1[2] : w0[2];
-          if (ck < 0) continue;
-          const T w = wa * wb * wq;
-          const T* p = cc + 3 * (((long long)ci * coarse.ny + cj) * coarse.nz + ck);
-          acc0 += w * p[0]; acc1 += w * p[1]; acc2 += w * p[2];
+          T* v = cv[(a * 2 + b) * 2 + q];
+          v[0] = v[1] = v[2] = T(0);
+          if ((!a || hx) && (!b || hy) && (!q || hz)) {
+            const T* p = cc + 3 * (((long long)(I + a) * coarse.ny + (J + b)) * coarse.nz + (K + q));
+            v[0] = p[0]; v[1] = p[1]; v[2] = p[2];
+          }
+        }
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+      const int i = 2 * I + fi;
+      if (i >= fine.nx) continue;
+#pragma unroll
+      for (int fj = 0; fj < 2; ++fj) {
+        const int j = 2 * J + fj;
+        if (j >= fine.ny) continue;
+#pragma unroll
+        for (int fk = 0; fk < 2; ++fk) {
+          const int k = 2 * K + fk;
+          if (k >= fine.nz) continue;
+          // an even fine index takes coarse node I with weight 1, an odd one I (1/2) and I + 1 (1/2, when it exists)
+          T acc0 = T(0), acc1 = T(0), acc2 = T(0);
+#pragma unroll
+          for (int a = 0; a < 2; ++a) {
+            if (a && (!fi || !hx)) continue;
+            const T wa = fi ? T(0.5) : T(1);
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+              if (b && (!fj || !hy)) continue;
+              const T wb = fj ? T(0.5) : T(1);
+#pragma unroll
+              for (int q = 0; q < 2; ++q) {
+                if (q && (!fk || !hz)) continue;
+                const T wq = fk ? T(0.5) : T(1);
+                const T w = wa * wb * wq;
+                const T* v = cv[(a * 2 + b) * 2 + q];
+                acc0 += w * v[0]; acc1 += w * v[1]; acc2 += w * v[2];
+              }
+            }
+          }
+          const long long n = ((long long)i * fine.ny + j) * fine.nz + k;
+          const unsigned m = fmask ? fmask[n] : 7u;
+          if (m & 1u) xc[3 * n + 0] = round_store(xc[3 * n + 0] + acc0, round);
+          if (m & 2u) xc[3 * n + 1] = round_store(xc[3 * n + 1] + acc1, round);
+          if (m & 4u) xc[3 * n + 2] = round_store(xc[3 * n + 2] + acc2, round);
         }
       }
     }
-    const unsigned m = fmask ? fmask[n] : 7u;
-    if (m & 1u) xc[3 * n + 0] = round_store(xc[3 * n + 0] + acc0, round);
-    if (m & 2u) xc[3 * n + 1] = round_store(xc[3 * n + 1] + acc1, round);
-    if (m & 4u) xc[3 * n + 2] = round_store(xc[3 * n + 2] + acc2, round);
   }
 }
 template <typename T>

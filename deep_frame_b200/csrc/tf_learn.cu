@@ -6,6 +6,7 @@
 // channel-major [C][nx][ny][nz] FP32 on a node grid; pooling halves each extent rounding up
 // (missing children count as zero), upsampling copies a coarse value to its (up to 8) children.
 #include <cmath>
+#include <cuda_fp16.h>
 #include <string>
 
 #include "tf_b200.h"
@@ -247,6 +248,184 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 
 Grid3 grid3(const int32_t s[3]) { return Grid3{s[0], s[1], s[2]}; }
 
+// ---------------------------------------------------------------------------
+// 3 x 3 x 3 convolution on the 5th-generation tensor cores (inference form of the network):
+// y[o][v] = act(bias[o] + sum_{c,t} W[o][c * 27 + t] x[c][v + offset(t)]) as an implicit GEMM
+// with M = 128 consecutive output nodes per CTA, N = the output channels padded to a multiple of
+// 16 (W packed to FP16 [np][kp], kp a multiple of 64), K = input channels x 27 taps in chunks of
+// 64.  Per chunk every thread gathers its node's 64 (channel, tap) inputs, rounds them to FP16 and
+// writes them to shared memory in the UMMA K-major layout (16-byte rows of 8 values, core matrices
+// of 8 rows); the weight chunk is copied beside it; one thread issues four tcgen05.mma kind::f16
+// (K = 16 each) accumulating in FP32 in TMEM and commits them to the chunk buffer's mbarrier, so
+// the gather of the next chunk (double-buffered) overlaps them.  The accumulators come back with
+// tcgen05.ld, one TMEM lane (= output node) per thread.  Every wait is bounded; a timeout sets
+// *err, waits (bounded) for the MMAs in flight and frees the TMEM.
+// ---------------------------------------------------------------------------
+constexpr int CV_M = 128, CV_KC = 64, CV_NMAX = 64, CV_THREADS = 128, CV_TMEM = 64;
+constexpr unsigned CV_SPIN = 1u << 22;
+constexpr int CV_A_BYTES = CV_M * CV_KC * 2;           // 16 KB per stage
+constexpr int CV_B_BYTES = CV_NMAX * CV_KC * 2;        // 8 KB per stage
+constexpr int CV_SMEM = 2 * CV_A_BYTES + 2 * CV_B_BYTES + 64;
+
+__device__ __forceinline__ uint32_t cv_smem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// UMMA shared-memory descriptor, K-major without swizzle (lbo: between 16-byte K columns of core
+// matrices, sbo: between 8-row groups).
+__device__ __forceinline__ uint64_t cv_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  return d;
+}
+
+__device__ __forceinline__ bool cv_wait(uint32_t bar, uint32_t parity) {
+  for (unsigned it = 0; it < CV_SPIN; ++it) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(CV_THREADS) conv16_kernel(const float* __restrict__ x, int cin, Grid3 g, const __half* __restrict__ w16,
+                                                           int cout, int np, int kp, const float* __restrict__ bias, int relu,
+                                                           float* __restrict__ y, int* err) {
+  extern __shared__ __align__(128) unsigned char cv_raw[];
+  unsigned char* sA = cv_raw;                                  // [2][CV_KC / 8][CV_M][16 B]
+  unsigned char* sB = cv_raw + 2 * CV_A_BYTES;                 // [2][CV_KC / 8][np][16 B]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(cv_raw + 2 * CV_A_BYTES + 2 * CV_B_BYTES);
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(bars + 2);
+  int* abort_flag = reinterpret_cast<int*>(bars + 3);
+  const int t = threadIdx.x, warp = t >> 5;
+  const long long n = g.n();
+  const long long v = (long long)blockIdx.x * CV_M + t;
+  const bool live = v < n;
+  int vi = 0, vj = 0, vk = 0;
+  if (live) {
+    vk = static_cast<int>(v % g.nz);
+    const long long r = v / g.nz;
+    vj = static_cast<int>(r % g.ny);
+    vi = static_cast<int>(r / g.ny);
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(cv_smem(&bars[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(cv_smem(&bars[1])));
+    *abort_flag = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(cv_smem(tbase)), "r"(CV_TMEM));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tbase;
+  const int K = cin * 27;
+  const int chunks = kp / CV_KC;
+  const uint32_t idesc = (1u << 4) | (uint32_t(np >> 3) << 17) | (uint32_t(CV_M >> 4) << 24);   // D FP32, A, B FP16, K-major
+  uint32_t phases = 0u;   // bit s: the parity awaited next on stage s's barrier
+  for (int q = 0; q < chunks; ++q) {
+    const int st = q & 1;
+    if (q >= 2) {   // the MMAs of chunk q - 2 have read this stage
+      if (!cv_wait(cv_smem(&bars[st]), (phases >> st) & 1u)) *abort_flag = 1;
+      phases ^= 1u << st;
+      __syncthreads();
+      if (*abort_flag) break;
+    }
+    unsigned char* a = sA + st * CV_A_BYTES;
+    unsigned char* b = sB + st * CV_B_BYTES;
+    // this thread's node: 64 (channel, tap) inputs of the chunk, 8 per 16-byte row
+    int k = q * CV_KC;
+    int c = k / 27, tap = k - 27 * (k / 27);
+#pragma unroll 1
+    for (int j = 0; j < CV_KC / 8; ++j) {
+      uint32_t pk[4];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        float val = 0.0f;
+        if (live && k < K) {
+          const int ii = vi + tap / 9 - 1, jj = vj + (tap / 3) % 3 - 1, kk = vk + tap % 3 - 1;
+          if ((unsigned)ii < (unsigned)g.nx && (unsigned)jj < (unsigned)g.ny && (unsigned)kk < (unsigned)g.nz)
+            val = x[(long long)c * n + ((long long)ii * g.ny + jj) * g.nz + kk];
+        }
+        const uint32_t bits = __half_as_ushort(__float2half_rn(val));
+        pk[e >> 1] = (e & 1) ? (pk[e >> 1] | (bits << 16)) : bits;   // element 2i in the low half
+        ++k;
+        if (++tap == 27) { tap = 0; ++c; }
+      }
+      *reinterpret_cast<uint4*>(a + (j * CV_M + t) * 16) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+    for (int piece = t; piece < np * (CV_KC / 8); piece += CV_THREADS) {
+      const int row = piece / (CV_KC / 8), j = piece % (CV_KC / 8);
+      *reinterpret_cast<uint4*>(b + (j * np + row) * 16) =
+          *reinterpret_cast<const uint4*>(w16 + (long long)row * kp + q * CV_KC + 8 * j);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t aa = cv_smem(a), ba = cv_smem(b);
+#pragma unroll
+      for (int ks = 0; ks < CV_KC / 16; ++ks) {
+        const uint64_t da = cv_desc(aa + 2 * ks * CV_M * 16, CV_M * 16, 128);
+        const uint64_t db = cv_desc(ba + 2 * ks * np * 16, np * 16, 128);
+        const uint32_t acc = (q > 0 || ks > 0) ? 1u : 0u;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                     :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(cv_smem(&bars[st])) : "memory");
+    }
+  }
+  if (!*abort_flag && chunks > 0) {
+    // the last commit covers every MMA this thread issued
+    const int st = (chunks - 1) & 1;
+    if (!cv_wait(cv_smem(&bars[st]), (phases >> st) & 1u)) *abort_flag = 1;
+    __syncthreads();
+  }
+  if (!*abort_flag) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    for (int c0 = 0; c0 < np; c0 += 16) {
+      uint32_t r[16];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+                     "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                   : "r"(tmem + (uint32_t(32 * warp) << 16) + c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (live) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int o = c0 + e;
+          if (o < cout) {
+            float val = __uint_as_float(r[e]) + bias[o];
+            if (relu) val = fmaxf(val, 0.0f);
+            y[(long long)o * n + v] = val;
+          }
+        }
+      }
+    }
+  } else {
+    if (t == 0) atomicExch(err, 1);
+    // let MMAs still in flight finish before the TMEM is released (bounded)
+    for (int st = 0; st < 2; ++st) cv_wait(cv_smem(&bars[st]), (phases >> st) & 1u);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(CV_TMEM));
+}
+
+// w16[o][k] = fp16(w[o][k]) for o < cout, k < K; zero padding up to [np][kp]
+__global__ void pack16_kernel(const float* __restrict__ w, int cout, int K, __half* __restrict__ w16, int np, int kp) {
+  const long long total = (long long)np * kp;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+    const int o = static_cast<int>(idx / kp), k = static_cast<int>(idx % kp);
+    w16[idx] = __float2half_rn((o < cout && k < K) ? w[(long long)o * K + k] : 0.0f);
+  }
+}
+
 }  // namespace
 
 extern "C" const char* tf_nn_last_error(void) { return g_learn_error.c_str(); }
@@ -269,6 +448,39 @@ extern "C" int tf_nn_gemm(int32_t transa, int32_t transb, int32_t m, int32_t n, 
     TF_LAUNCH_CHECK("sgemm_kernel");
     sum_splits_kernel<<<grid_for((long long)m * n, 256), 256, 0, s>>>(work, splits, m, n, alpha, beta, c, ldc);
     TF_LAUNCH_CHECK("sum_splits_kernel");
+  });
+}
+
+extern "C" int tf_nn_pack16(const float* w, int32_t cout, int32_t k, void* w16, int32_t np, int32_t kp, void* stream) {
+  return learn_guard([&] {
+    require(w && w16 && cout >= 1 && k >= 1, "tf_nn_pack16: invalid arguments");
+    require(np >= cout && np % 16 == 0 && np <= CV_NMAX && kp >= k && kp % CV_KC == 0,
+            "tf_nn_pack16: np must be a multiple of 16 in [cout, 64], kp a multiple of 64 >= k");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    pack16_kernel<<<grid_for((long long)np * kp, 256), 256, 0, s>>>(w, cout, k, static_cast<__half*>(w16), np, kp);
+    TF_LAUNCH_CHECK("pack16_kernel");
+  });
+}
+
+extern "C" int tf_nn_conv16(const float* x, int32_t cin, const int32_t shape[3], const void* w16, int32_t cout, int32_t np, int32_t kp,
+                            const float* bias, int32_t relu, float* y, int32_t* err, void* stream) {
+  return learn_guard([&] {
+    require(x && shape && w16 && bias && y && err && cin >= 1 && cout >= 1, "tf_nn_conv16: invalid arguments");
+    require(np >= cout && np % 16 == 0 && np <= CV_NMAX && kp >= 27 * cin && kp % CV_KC == 0,
+            "tf_nn_conv16: np must be a multiple of 16 in [cout, 64], kp a multiple of 64 >= 27 cin");
+    const Grid3 g = grid3(shape);
+    require(g.nx >= 1 && g.ny >= 1 && g.nz >= 1, "tf_nn_conv16: empty grid");
+    const long long blocks = (g.n() + CV_M - 1) / CV_M;
+    require(blocks < (1LL << 31), "tf_nn_conv16: grid too large");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    static bool configured = false;
+    if (!configured) {
+      TF_CUDA_CHECK(cudaFuncSetAttribute(conv16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM));
+      configured = true;
+    }
+    conv16_kernel<<<(unsigned)blocks, CV_THREADS, CV_SMEM, s>>>(x, cin, g, static_cast<const __half*>(w16), cout, np, kp, bias, relu, y,
+                                                                err);
+    TF_LAUNCH_CHECK("conv16_kernel");
   });
 }
 

@@ -553,7 +553,7 @@ void vcycle_batch(const Group& in, cudaStream_t s) {
       return std::make_pair(cols_grid(cg.nnode, b.ncol),
                             TransferRec<T>{fg, cg, v.res[l].template as<T>(), 3 * fg.nnode, v.b[l + 1].template as<T>(), 3 * cg.nnode,
                                            b.hy->lv[l + 1].mask.as<uint8_t>(), b.st.active, store_round(b.h)});
-    return std::make_pair(cols_grid(fg.nnode, b.ncol),
+    return std::make_pair(cols_grid(cg.nnode, b.ncol),
                           TransferRec<T>{fg, cg, v.x[l + 1].template as<T>(), 3 * cg.nnode, v.x[l].template as<T>(), 3 * fg.nnode,
                                          b.hy->lv[l].mask.as<uint8_t>(), b.st.active, store_round(b.h)});
   };

@@ -642,7 +642,7 @@ void vcycle(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int l, int ncol, const in
     }
     vcycle<T>(h, hy, vb, l + 1, ncol, active, st);
     TimedRange tr(h->timers, TIMER_TRANSFER, st);
-    prolong_add_kernel<T><<<cols_grid(fg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.x[l + 1].template as<T>(), 3 * cg.nnode,
+    prolong_add_kernel<T><<<cols_grid(cg.nnode, ncol), 256, 0, st>>>(fg, cg, vb.x[l + 1].template as<T>(), 3 * cg.nnode,
                                                                      vb.x[l].template as<T>(), 3 * fg.nnode,
                                                                      hy.lv[l].mask.as<uint8_t>(), active, store_round(h));
     TF_LAUNCH_CHECK("prolong_add_kernel");

@@ -32,16 +32,25 @@ def _half(shape):
 
 
 class GuessNet:
-    def __init__(self, channels=(8, 16, 32), seed=0, device="cuda"):
+    """The encoder / decoder over len(channels) levels; the default (16, 32, 48, 64) has four."""
+
+    def __init__(self, channels=(16, 32, 48, 64), seed=0, device="cuda"):
         import torch
         self.torch = torch
         self.device = torch.device(device)
         self.lib = _lib.load()
-        c0, c1, c2 = channels
-        self.channels = tuple(channels)
-        # (cin, cout, relu) in execution order
-        self.specs = [(IN_CHANNELS, c0, 1), (c0, c0, 1), (c0, c1, 1), (c1, c1, 1), (c1, c2, 1), (c2, c2, 1),
-                      (c2 + c1, c1, 1), (c1 + c0, c0, 1), (c0, 3, 0)]
+        if len(channels) < 2 or any(int(c) < 1 or int(c) > 64 for c in channels):
+            raise ValueError("channels: at least two levels of 1 to 64 channels")
+        self.channels = tuple(int(c) for c in channels)
+        ch = self.channels
+        # (cin, cout, relu) in execution order: two convolutions per encoder level, one per decoder
+        # level (after the upsampled coarser features are concatenated with the encoder's), a linear head
+        self.specs = [(IN_CHANNELS, ch[0], 1), (ch[0], ch[0], 1)]
+        for lo, hi in zip(ch[:-1], ch[1:]):
+            self.specs += [(lo, hi, 1), (hi, hi, 1)]
+        for level in range(len(ch) - 2, -1, -1):
+            self.specs.append((ch[level + 1] + ch[level], ch[level], 1))
+        self.specs.append((ch[0], 3, 0))
         rng = np.random.default_rng(seed)
         self.params = []
         for cin, cout, relu in self.specs:
@@ -54,6 +63,19 @@ class GuessNet:
         self.step_count = 0
         self.work = torch.empty(0, dtype=torch.float32, device=self.device)
         self.mse_scratch = torch.zeros(int(self.lib.tf_nn_mse_scratch_doubles()) + 1, dtype=torch.float64, device=self.device)
+        self.packed = None
+        self.tc_error = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    def pack(self):
+        """FP16 copies of the weights for the tensor-core inference (tf_nn_pack16); call after training."""
+        torch = self.torch
+        self.packed = []
+        for (cin, cout, _), (w, _) in zip(self.specs, self.params):
+            np_, kp = 16 * ((cout + 15) // 16), 64 * ((27 * cin + 63) // 64)
+            w16 = torch.empty((np_, kp), dtype=torch.float16, device=self.device)
+            self._check(self.lib.tf_nn_pack16(_lib.ptr(w), cout, 27 * cin, _lib.ptr(w16), np_, kp, self._stream()), "tf_nn_pack16")
+            self.packed.append((w16, np_, kp))
+        return self
 
     # ------------------------------------------------------------ plumbing --
     def _stream(self):
@@ -78,6 +100,13 @@ class GuessNet:
         cin, cout, relu = self.specs[index]
         w, b = self.params[index]
         n = int(np.prod(shape))
+        if cache is None and self.packed is not None:
+            # inference on the tensor cores: FP16 operands, FP32 accumulation
+            w16, np_, kp = self.packed[index]
+            y = torch.empty((cout, n), dtype=torch.float32, device=self.device)
+            self._check(self.lib.tf_nn_conv16(_lib.ptr(x), cin, _shape3(shape), _lib.ptr(w16), cout, np_, kp, _lib.ptr(b), relu,
+                                              _lib.ptr(y), _lib.ptr(self.tc_error), self._stream()), "tf_nn_conv16")
+            return y
         col = torch.empty((cin * 27, n), dtype=torch.float32, device=self.device)
         self._check(self.lib.tf_nn_im2col(_lib.ptr(x), cin, _shape3(shape), _lib.ptr(col), self._stream()), "tf_nn_im2col")
         y = torch.empty((cout, n), dtype=torch.float32, device=self.device)
@@ -120,36 +149,54 @@ class GuessNet:
 
     # ------------------------------------------------------------- network --
     def forward(self, x, shape, cache=None):
-        """x: [5, n] FP32 features on the node grid `shape`; returns [3, n]."""
+        """x: [5, n] FP32 features on the node grid `shape`; returns [3, n].  With a cache (training)
+        every convolution runs as im2col + FP32 SGEMM and keeps what backward needs; without one,
+        after pack(), every convolution runs on the tensor cores in FP16."""
         torch = self.torch
-        c0, c1, c2 = self.channels
-        s0 = tuple(int(s) for s in shape)
-        s1 = _half(s0)
-        s2 = _half(s1)
-        e0 = self._conv(1, self._conv(0, x.contiguous(), s0, cache), s0, cache)
-        e1 = self._conv(3, self._conv(2, self._pool(e0, c0, s0), s1, cache), s1, cache)
-        e2 = self._conv(5, self._conv(4, self._pool(e1, c1, s1), s2, cache), s2, cache)
-        d1 = self._conv(6, torch.cat([self._resample(e2, c2, s1, 0), e1]).contiguous(), s1, cache)
-        d0 = self._conv(7, torch.cat([self._resample(d1, c1, s0, 0), e0]).contiguous(), s0, cache)
-        return self._conv(8, d0, s0, cache)
+        ch = self.channels
+        shapes = [tuple(int(s) for s in shape)]
+        for _ in ch[1:]:
+            shapes.append(_half(shapes[-1]))
+        layer = 0
+        skips = []
+        h = x.contiguous()
+        for level, c in enumerate(ch):
+            if level > 0:
+                h = self._pool(h, ch[level - 1], shapes[level - 1])
+            h = self._conv(layer, h, shapes[level], cache)
+            h = self._conv(layer + 1, h, shapes[level], cache)
+            layer += 2
+            skips.append(h)
+        for level in range(len(ch) - 2, -1, -1):
+            up = self._resample(h, ch[level + 1], shapes[level], 0)
+            h = self._conv(layer, torch.cat([up, skips[level]]).contiguous(), shapes[level], cache)
+            layer += 1
+        y = self._conv(layer, h, shapes[0], cache)
+        if cache is None and self.packed is not None and int(self.tc_error.item()):
+            raise _lib.TfError(5, "tf_nn_conv16: a tensor-core wait timed out")
+        return y
 
     def backward(self, dy, shape, cache, accumulate):
         """Gradients of all parameters (added to the stored ones when accumulate) from dy = dL/d output."""
-        c0, c1, c2 = self.channels
-        s0 = tuple(int(s) for s in shape)
-        s1 = _half(s0)
-        dd0 = self._conv_back(8, dy.contiguous(), cache, accumulate)
-        dcat0 = self._conv_back(7, dd0, cache, accumulate)
-        dd1 = self._resample(dcat0[:c1].contiguous(), c1, s0, 2)
-        de0 = dcat0[c1:].clone()
-        dcat1 = self._conv_back(6, dd1, cache, accumulate)
-        de2 = self._resample(dcat1[:c2].contiguous(), c2, s1, 2)
-        de1 = dcat1[c2:].clone()
-        dp2 = self._conv_back(4, self._conv_back(5, de2, cache, accumulate), cache, accumulate)
-        de1 += self._resample(dp2, c1, s1, 1)
-        dp1 = self._conv_back(2, self._conv_back(3, de1, cache, accumulate), cache, accumulate)
-        de0 += self._resample(dp1, c0, s0, 1)
-        self._conv_back(0, self._conv_back(1, de0, cache, accumulate), cache, accumulate)
+        ch = self.channels
+        shapes = [tuple(int(s) for s in shape)]
+        for _ in ch[1:]:
+            shapes.append(_half(shapes[-1]))
+        layer = len(self.specs) - 1
+        g = self._conv_back(layer, dy.contiguous(), cache, accumulate)
+        dskip = [None] * len(ch)
+        for level in range(len(ch) - 1):   # decoder, finest first (reverse of the forward order)
+            layer -= 1
+            dcat = self._conv_back(layer, g, cache, accumulate)
+            dskip[level] = dcat[ch[level + 1]:].clone()
+            g = self._resample(dcat[:ch[level + 1]].contiguous(), ch[level + 1], shapes[level], 2)
+        for level in range(len(ch) - 1, -1, -1):   # encoder, coarsest first
+            if dskip[level] is not None:
+                g = g + dskip[level]
+            layer -= 2
+            g = self._conv_back(layer, self._conv_back(layer + 1, g, cache, accumulate), cache, accumulate)
+            if level > 0:
+                g = self._resample(g, ch[level - 1], shapes[level - 1], 1)
 
     def loss(self, y, target, weight=None, want_grad=True):
         """Mean squared error over the weighted entries; returns (loss tensor [1] FP64, dL/dy or None)."""
@@ -205,32 +252,56 @@ def target(u):
 
 
 class GuessPolicy:
-    """Use the network's guess only while it saves PCG iterations over the comparison start."""
+    """Use the network's guess only while it pays: at least one PCG iteration fewer than the
+    comparison start and, when the times are given, less time with its inference included."""
 
     def __init__(self, net):
         self.net, self.enabled, self.record = net, True, []
 
-    def assess(self, iterations_with, iterations_without):
+    def assess(self, iterations_with, iterations_without, seconds_with=None, seconds_without=None):
         self.record.append((int(iterations_with), int(iterations_without)))
-        if iterations_with >= iterations_without:
+        if iterations_with > iterations_without - 1:
+            self.enabled = False
+        if seconds_with is not None and seconds_without is not None and seconds_with >= seconds_without:
             self.enabled = False
         return self.enabled
 
 
 # ------------------------------------------------------------ training data --
-def record_trajectory(domain, covariance, iterations, multigrid=None, device="cuda", keep=None):
-    """Run the covariance SIMP + MMA loop and keep, per iteration, the element moduli and every group's
-    (forces, displacements) on the host: [(moduli, {key: (forces [R, ndof], u [R, ndof])})]."""
+def record_trajectory(domain, covariance, iterations, multigrid=None, device="cuda", stride=1):
+    """Run the covariance SIMP + MMA loop and keep, per iteration, the node stiffness of the design
+    and of every group every `stride`-th load column's sample on the device: the network input
+    (force / max|force|, node stiffness, node live flag: [5, n] FP32) and target (u / rms(u):
+    [3, n] FP32).  Returns (snapshots, live, shape) with snapshots = [(moduli, [(key, x, t)])] and
+    live = {key: (node live [n], dof live [3, n] FP32 on the device)}."""
+    import torch
     from .optimize import CovarianceSimp
     loop = CovarianceSimp(domain, covariance, volume_fraction=0.15, filter_radius=1.5, move=0.2,
                           multigrid={**(multigrid or {}), "device": str(device)})
+    system = loop.system
+    live = {}
+    for key in system.groups:
+        node_live, dof_live = _live_nodes(system, key)
+        live[key] = (torch.as_tensor(node_live, device=device), torch.as_tensor(dof_live, device=device))
     snapshots = []
     original = loop.model.solve_all
 
     def solve_and_keep(initial=None):
         solved = original(initial)
-        groups = {key: (forces.cpu().numpy(), u.cpu().numpy()) for key, _, forces, u, _ in solved}
-        snapshots.append((loop.moduli.cpu().numpy().copy(), groups))
+        moduli = loop.moduli.cpu().numpy().copy()
+        stiffness = torch.as_tensor(node_stiffness(moduli, system.shape).reshape(1, -1).astype(np.float32), device=device)
+        kept = []
+        for key, _, forces, u, _ in solved:
+            for j in range(0, forces.shape[0], stride):
+                f = forces[j].reshape(-1, 3).to(torch.float32)
+                scale = f.abs().max()
+                if float(scale) == 0.0:
+                    continue
+                v = u[j].reshape(-1, 3).to(torch.float64)
+                rms = v.pow(2).mean().sqrt().clamp_min(1e-300)
+                x = torch.cat([(f / scale).T, stiffness, live[key][0][None, :]]).contiguous()
+                kept.append((key, x, (v / rms).to(torch.float32).T.contiguous()))
+        snapshots.append((moduli, kept))
         return solved
 
     loop.model.solve_all = solve_and_keep
@@ -238,10 +309,9 @@ def record_trajectory(domain, covariance, iterations, multigrid=None, device="cu
         loop.run(iterations)
     finally:
         loop.model.solve_all = original
-    system = loop.system
-    live = {key: _live_nodes(system, key) for key in system.groups}
+    shape = system.shape
     loop.close()
-    return snapshots, live, system.shape
+    return snapshots, live, shape
 
 
 def _live_nodes(system, key):
@@ -253,23 +323,16 @@ def _live_nodes(system, key):
 
 
 def samples(snapshots, live, shape):
-    """Yield (x [5, n], target [3, n], weight [3, n]) FP32 for every column of every snapshot."""
-    for moduli, groups in snapshots:
-        stiffness = node_stiffness(moduli, shape)
-        for key, (forces, u) in groups.items():
-            node_live, dof_live = live[key]
-            for j in range(forces.shape[0]):
-                if not np.any(forces[j]):
-                    continue
-                x, _ = features(forces[j], stiffness, node_live)
-                t, _ = target(u[j])
-                yield x, t, dof_live
+    """Yield (x [5, n], target [3, n], weight [3, n]) device FP32 for every kept column of every snapshot."""
+    for _, kept in snapshots:
+        for key, x, t in kept:
+            yield x, t, live[key][1]
 
 
 def train(net, snapshots, live, shape, epochs=6, batch=8, lr=2e-3, seed=0):
     """Adam on the mean squared error of u / rms(u); returns the mean loss of every epoch."""
     torch = net.torch
-    data = [tuple(torch.as_tensor(a, device=net.device) for a in item) for item in samples(snapshots, live, shape)]
+    data = list(samples(snapshots, live, shape))
     order = np.random.default_rng(seed).permutation(len(data))
     node_shape = tuple(s + 1 for s in shape)
     history = []
@@ -295,25 +358,26 @@ def train(net, snapshots, live, shape, epochs=6, batch=8, lr=2e-3, seed=0):
 
 def predict(net, multigrid, key, fixed, forces, moduli, shape, live):
     """Initial guesses [R, ndof] FP64 for a group's force block: the network's shape, scaled per column
-    to the energy-optimal multiple (one masked operator apply for all columns)."""
+    to the energy-optimal multiple (one masked operator apply for all columns).  The features are
+    formed on the device; with pack() done the network runs on the tensor cores."""
     torch = net.torch
-    stiffness = node_stiffness(moduli, shape)
-    node_live, dof_live = live
+    node_live, dof_live = (torch.as_tensor(a, device=forces.device) for a in live)
+    stiffness = torch.as_tensor(node_stiffness(moduli, shape).reshape(1, -1).astype(np.float32), device=forces.device)
     node_shape = tuple(s + 1 for s in shape)
-    host = forces.cpu().numpy()
-    shapes = np.zeros_like(host)
-    for j in range(host.shape[0]):
-        if not np.any(host[j]):
+    shapes = torch.zeros_like(forces)
+    for j in range(forces.shape[0]):
+        f = forces[j].reshape(-1, 3).to(torch.float32)
+        scale = f.abs().max()
+        if float(scale) == 0.0:
             continue
-        x, _ = features(host[j], stiffness, node_live)
-        y = net.forward(torch.as_tensor(x, device=net.device), node_shape).cpu().numpy()
-        shapes[j] = (y * dof_live).T.reshape(-1)
-    guess = torch.as_tensor(shapes, dtype=torch.float64, device=forces.device)
-    applied = multigrid.apply_device(guess.contiguous(), key, fixed)
-    energy = (guess * applied).sum(1)
-    work = (guess * forces).sum(1)
+        x = torch.cat([(f / scale).T, stiffness, node_live[None, :].to(torch.float32)]).contiguous()
+        y = net.forward(x, node_shape)
+        shapes[j] = (y * dof_live).T.reshape(-1).to(torch.float64)
+    applied = multigrid.apply_device(shapes.contiguous(), key, fixed)
+    energy = (shapes * applied).sum(1)
+    work = (shapes * forces).sum(1)
     alpha = torch.where(energy > 0, work / energy.clamp_min(1e-300), torch.zeros_like(energy))
-    return (alpha[:, None] * guess).contiguous()
+    return (alpha[:, None] * shapes).contiguous()
 
 
 def compare(net, domain, covariance, design_moduli, multigrid=None, device="cuda"):

@@ -283,6 +283,15 @@ TF_API const char* tf_nn_last_error(void);
  * partial tiles in `work` (>= m * n floats, up to 64 * m * n used) summed in a fixed order. */
 TF_API int tf_nn_gemm(int32_t transa, int32_t transb, int32_t m, int32_t n, int32_t k, float alpha, const float* a, int32_t lda,
                       const float* b, int32_t ldb, float beta, float* c, int32_t ldc, float* work, int64_t work_floats, void* stream);
+/* Inference form of a 3 x 3 x 3 convolution on the tensor cores (tcgen05 kind::f16, FP16 operands,
+ * FP32 accumulation): y[o][v] = act(bias[o] + sum_{c,tap} W[o][c * 27 + tap] x[c][v + offset(tap)])
+ * (act = ReLU when relu != 0), x [cin][n] and y [cout][n] FP32 on the node grid `shape`; the
+ * weights are packed first by tf_nn_pack16 from FP32 W [cout][27 cin] to FP16 [np][kp] (np a
+ * multiple of 16 in [cout, 64], kp a multiple of 64, zero padding).  *err (device int) is set when
+ * a bounded wait on the tensor cores timed out. */
+TF_API int tf_nn_pack16(const float* w, int32_t cout, int32_t k, void* w16, int32_t np, int32_t kp, void* stream);
+TF_API int tf_nn_conv16(const float* x, int32_t cin, const int32_t shape[3], const void* w16, int32_t cout, int32_t np, int32_t kp,
+                        const float* bias, int32_t relu, float* y, int32_t* err, void* stream);
 /* col[(c * 27 + tap)][v] = in[c][v + offset(tap)], 3 x 3 x 3 taps, zero outside; col2im is its adjoint. */
 TF_API int tf_nn_im2col(const float* in, int32_t channels, const int32_t shape[3], float* col, void* stream);
 TF_API int tf_nn_col2im(const float* col, int32_t channels, const int32_t shape[3], float* out, void* stream);

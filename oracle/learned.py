@@ -12,7 +12,6 @@ def forward(params, x, shape, channels):
     """params: [(w [cout, cin*27], b [cout])] torch tensors; x: [5, n] tensor; returns [3, n]."""
     import torch
     import torch.nn.functional as F
-    c0, c1, c2 = channels
     s0 = tuple(int(s) for s in shape)
 
     def conv(i, v, s, relu=True):
@@ -31,16 +30,19 @@ def forward(params, x, shape, channels):
         return v.repeat_interleave(2, 1).repeat_interleave(2, 2).repeat_interleave(2, 3)[:, :s[0], :s[1], :s[2]]
 
     g = x.reshape(5, *s0)
-    e0 = conv(1, conv(0, g, s0), s0)
-    p1 = pool(e0)
-    s1 = tuple(p1.shape[1:])
-    e1 = conv(3, conv(2, p1, s1), s1)
-    p2 = pool(e1)
-    s2 = tuple(p2.shape[1:])
-    e2 = conv(5, conv(4, p2, s2), s2)
-    d1 = conv(6, torch.cat([up(e2, s1), e1]), s1)
-    d0 = conv(7, torch.cat([up(d1, s0), e0]), s0)
-    return conv(8, d0, s0, relu=False).reshape(3, -1)
+    layer, skips, shapes = 0, [], [s0]
+    h = g
+    for level in range(len(channels)):
+        if level > 0:
+            h = pool(h)
+            shapes.append(tuple(h.shape[1:]))
+        h = conv(layer + 1, conv(layer, h, shapes[level]), shapes[level])
+        layer += 2
+        skips.append(h)
+    for level in range(len(channels) - 2, -1, -1):
+        h = conv(layer, torch.cat([up(h, shapes[level]), skips[level]]), shapes[level])
+        layer += 1
+    return conv(layer, h, s0, relu=False).reshape(3, -1)
 
 
 def loss_and_grads(params_np, x, target, weight, shape, channels):

@@ -40,3 +40,7 @@ def test_guess_policy_drops_the_network_once_it_stops_saving_iterations():
     assert not policy.assess(15, 15) and not policy.enabled                       # no saving: dropped
     assert not policy.assess(5, 15)                                               # and stays dropped
     assert policy.record == [(12, 15), (15, 15), (5, 15)]
+    # a fraction of an iteration is no saving, and neither is a saving that costs time
+    assert not learned.GuessPolicy(net=None).assess(165.93, 165.94)
+    assert not learned.GuessPolicy(net=None).assess(20, 25, seconds_with=1.9, seconds_without=0.8)
+    assert learned.GuessPolicy(net=None).assess(20, 25, seconds_with=0.6, seconds_without=0.8)
