@@ -68,6 +68,9 @@ def parse(argv=None):
     ap.add_argument("--schedule", default=SCHEDULE, metavar="DEGREE,GROWTH", help="Chebyshev smoother schedule of both arms")
     ap.add_argument("--instances", type=int, default=0,
                     help="solve N independent seeded plates of uneven size and RHS count concurrently and report solves/s")
+    ap.add_argument("--instance-sizes", choices=("plate", "small"), default="plate",
+                    help="grids of --instances: 64 x 64 x 12 ... 160 x 160 x 24 with 6-42 columns per half (plate), "
+                         "or 16 x 16 x 4 ... 48 x 48 x 8 with 3-12 columns (small)")
     ap.add_argument("--learned", action="store_true", help="train the learned initial guess and report PCG with / without it")
     ap.add_argument("--learned-epochs", type=int, default=4, help="training epochs of --learned")
     ap.add_argument("--simp", type=int, default=0, help="run N SIMP + MMA iterations (default plate 128 x 128 x 24) instead")
@@ -500,7 +503,8 @@ def simp(args):
 
 def instances(args):
     """--instances N: N independent seeded plate instances (grids from 64 x 64 x 12 to 160 x 160 x 24,
-    6 to 42 load columns per half), each with its own solver handle, solved to 1e-8 three ways: as one
+    6 to 42 load columns per half; with --instance-sizes small from 16 x 16 x 4 to 48 x 48 x 8, 3 to 12
+    columns), each with its own solver handle, solved to 1e-8 three ways: as one
     batch (tf_solve_batch: every PCG and V-cycle stage one launch over all instances; one batch per
     mirror half), one after another on one stream, and concurrently on one host thread and CUDA
     stream per instance.  After one untimed round of each (buffers, hierarchies, constant slots) the
@@ -512,11 +516,15 @@ def instances(args):
     from deep_frame_b200.elasticity import HexElasticity
     from deep_frame_b200.topology_multigrid import solve_batch_device
     rng = np.random.default_rng(2026)
-    sizes = [(64, 64, 12), (80, 80, 12), (96, 96, 16), (112, 112, 16), (128, 128, 16), (128, 128, 24), (144, 144, 24), (160, 160, 24)]
+    if args.instance_sizes == "small":
+        sizes, columns = [(16, 16, 4), (24, 24, 4), (24, 24, 6), (32, 32, 6), (32, 32, 8), (40, 40, 8), (48, 48, 8)], (3, 13)
+    else:
+        sizes, columns = [(64, 64, 12), (80, 80, 12), (96, 96, 16), (112, 112, 16), (128, 128, 16), (128, 128, 24), (144, 144, 24),
+                          (160, 160, 24)], (6, 43)
     specs = []
     for i in range(args.instances):
         shape = sizes[int(rng.integers(len(sizes)))]
-        specs.append((shape, int(rng.integers(6, 43)), i))
+        specs.append((shape, int(rng.integers(*columns)), i))
     settings = {"tolerance": 1e-8, "smoother": "chebyshev", "chebyshev_degree": 1, "growth": 2.0}
     work = []
     for shape, rhs, seed in specs:
@@ -603,7 +611,7 @@ def instances(args):
     line = {"metric": "independent uneven instances: solves/s", "value": round(len(work) / batch_seconds, 4), "unit": "solves/s", "n_gpus": 1,
             "higher_is_better": True, "data": "synthetic",
             "config": {"instances": [{"shape": list(item["shape"]), "rhs_per_half": item["rhs"], "pcg_iterations": item.get("iterations")}
-                                     for item in work], "tolerance": 1e-8,
+                                     for item in work], "sizes": args.instance_sizes, "tolerance": 1e-8,
                        "batched": "tf_solve_batch: one launch per PCG / V-cycle stage over all instances, one batch per mirror half"},
             "seconds": round(batch_seconds, 4), "column_solves_per_s": round(columns / batch_seconds, 2),
             "serial_seconds": round(serial_seconds, 4), "speedup_vs_serial": round(serial_seconds / batch_seconds, 3),
