@@ -66,6 +66,9 @@ def parse(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--autotune", action="store_true", help="pick the smoother schedule with the autotuner instead of --schedule")
     ap.add_argument("--schedule", default=SCHEDULE, metavar="DEGREE,GROWTH", help="Chebyshev smoother schedule of both arms")
+    ap.add_argument("--coarsest-dofs", type=int, default=0,
+                    help="coarsest-grid size of both arms (default: the library's 8000; the reference's default is 80000, "
+                         "factored banded above 24000)")
     ap.add_argument("--instances", type=int, default=0,
                     help="solve N independent seeded plates of uneven size and RHS count concurrently and report solves/s")
     ap.add_argument("--instance-sizes", choices=("plate", "small"), default="plate",
@@ -168,9 +171,12 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def schedule_settings(text):
+def schedule_settings(text, coarsest_dofs=None):
     degree, growth = text.split(",")
-    return {"smoother": "chebyshev", "chebyshev_degree": int(degree), "growth": float(growth)}
+    out = {"smoother": "chebyshev", "chebyshev_degree": int(degree), "growth": float(growth)}
+    if coarsest_dofs:
+        out["coarsest_dofs"] = int(coarsest_dofs)
+    return out
 
 
 def fast_settings(args):
@@ -250,7 +256,7 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    smoother = schedule_settings(args.schedule)
+    smoother = schedule_settings(args.schedule, args.coarsest_dofs)
     spec, system, model, density = build_problem(args.config, device, {**fast_settings(args), **smoother})
     moduli_host, derivative = system.moduli(density, 3.0, 1e-9)
     moduli = torch.as_tensor(moduli_host, device=device)

@@ -366,6 +366,47 @@ __global__ void coarsest_assemble_kernel(Geo g, const double* __restrict__ B, co
   }
 }
 
+// The same coarsest Galerkin matrix in band storage (the lower band of (A + A^T) / 2:
+// AB[c * (bw + 1) + (r - c)] = A[r][c] for 0 <= r - c <= bw, live-dof numbering), for coarsest grids
+// too large for a dense factor.  Thread r forms row r's entries left of the diagonal and their
+// transposed counterparts, so every band entry is written once (no atomics, deterministic).
+__global__ void coarsest_assemble_band_kernel(Geo g, const double* __restrict__ B, const int* __restrict__ live_of_dof,
+                                              const long long* __restrict__ live_dofs, int n, int bw, double* __restrict__ AB) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long dof = live_dofs[t];
+    const long long node = dof / 3;
+    const int a = static_cast<int>(dof % 3);
+    int i, j, k;
+    node_coords(node, g, i, j, k);
+    for (int di = -1; di <= 1; ++di)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int dk = -1; dk <= 1; ++dk) {
+          const int ni = i + di, nj = j + dj, nk = k + dk;
+          if (!((unsigned)ni < (unsigned)g.nx && (unsigned)nj < (unsigned)g.ny && (unsigned)nk < (unsigned)g.nz)) continue;
+          const long long m = ((long long)ni * g.ny + nj) * g.nz + nk;
+          double v[3] = {0.0, 0.0, 0.0}, vt[3] = {0.0, 0.0, 0.0};
+          for (int e = 0; e < 8; ++e) {
+            const int ox = e >> 2, oy = (e >> 1) & 1, oz = e & 1;
+            const int cx = 1 - ox + di, cy = 1 - oy + dj, cz = 1 - oz + dk;
+            if (cx < 0 || cx > 1 || cy < 0 || cy > 1 || cz < 0 || cz > 1) continue;
+            const int ei = i - 1 + ox, ej = j - 1 + oy, ek = k - 1 + oz;
+            if (!((unsigned)ei < (unsigned)g.ex && (unsigned)ej < (unsigned)g.ey && (unsigned)ek < (unsigned)g.ez)) continue;
+            const double* b = B + (((long long)ei * g.ey + ej) * g.ez + ek) * 576;
+            const int cn = corner_id(1 - ox, 1 - oy, 1 - oz), cm = corner_id(cx, cy, cz);
+            for (int q = 0; q < 3; ++q) {
+              v[q] += b[(3 * cn + a) * 24 + 3 * cm + q];
+              vt[q] += b[(3 * cm + q) * 24 + 3 * cn + a];
+            }
+          }
+          for (int q = 0; q < 3; ++q) {
+            const int col = live_of_dof[3 * m + q];
+            if (col < 0 || col > t || t - col > bw) continue;
+            AB[(long long)col * (bw + 1) + (t - col)] = col == t ? v[q] : 0.5 * (v[q] + vt[q]);
+          }
+        }
+  }
+}
+
 // gather live coarsest dofs of the active columns into FP64 [ncol][n]
 template <typename T>
 __device__ __forceinline__ void coarsest_gather_body(const VGrid vg_,const T* __restrict__ src, long long stride, const long long* __restrict__ live, int n,

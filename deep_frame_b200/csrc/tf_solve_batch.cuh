@@ -515,21 +515,28 @@ void coarsest_batch(const Group& in, cudaStream_t s) {
                                                                         b.st.active});
   }), dim3(256), 0, s, "coarsest_gather_batch");
   std::vector<TrimulJob> jobs;
+  Group dense;
   for (BatchSolve* b : live) {
+    if (b->hy->band) {   // banded coarsest factors: one substitution launch per instance
+      band_solve(b->hy->X.as<double>(), b->hy->n_live, b->hy->bw, b->h->cb.as<double>(), b->h->cy.as<double>(), b->ncol, s);
+      continue;
+    }
     const size_t need = dense_trimul_work(b->hy->n_live, b->ncol);
     if (b->h->trimul_work.bytes < need) b->h->trimul_work.alloc(need);
     jobs.push_back(TrimulJob{b->hy->X.as<double>(), b->h->cb.as<double>(), b->h->cy.as<double>(), b->h->trimul_work.as<double>(),
                              b->hy->n_live, b->ncol, b->st.active});
+    dense.push_back(b);
   }
   // x = X^T (X b) with X = L^-1: cb -> cy, then cy -> cb
   dense_trimul_batch(jobs.data(), (int)jobs.size(), 0, s);
   for (size_t i = 0; i < jobs.size(); ++i) {
-    jobs[i].B = live[i]->h->cy.as<double>();
-    jobs[i].C = live[i]->h->cb.as<double>();
+    jobs[i].B = dense[i]->h->cy.as<double>();
+    jobs[i].C = dense[i]->h->cb.as<double>();
   }
   dense_trimul_batch(jobs.data(), (int)jobs.size(), 1, s);
   launch_batched<ScatterRec<T>>(coarsest_scatter_batch<T>, records<ScatterRec<T>>(live, [&](BatchSolve& b) {
-    return std::make_pair(cols_grid(b.hy->n_live, b.ncol), ScatterRec<T>{b.h->cb.as<double>(), b.hy->live.as<long long>(), b.hy->n_live,
+    const double* solved = b.hy->band ? b.h->cy.as<double>() : b.h->cb.as<double>();
+    return std::make_pair(cols_grid(b.hy->n_live, b.ncol), ScatterRec<T>{solved, b.hy->live.as<long long>(), b.hy->n_live,
                                                                          vbufs<T>(b.h).x[last(b)].template as<T>(), nd(b), b.st.active,
                                                                          store_round(b.h)});
   }), dim3(256), 0, s, "coarsest_scatter_batch");

@@ -35,7 +35,8 @@ thread_local std::string g_last_create_error;
 
 constexpr int CB32 = 6;                  // columns per CTA of the FP32 Galerkin-level operator
 constexpr int CB64 = 2;                  // columns per CTA of the FP64 Galerkin-level operator
-constexpr long long DENSE_LIMIT = 24000;  // largest dense coarsest factor (4.6 GB in FP64)
+constexpr long long DENSE_LIMIT = 24000;  // largest dense coarsest factor (4.6 GB in FP64); banded above
+constexpr double BAND_LIMIT_BYTES = 32e9;  // largest banded coarsest factor
 
 struct Level {
   Geo g{};
@@ -53,8 +54,10 @@ struct Hierarchy {
   std::vector<Level> lv;
   int n_live = 0;
   DevBuf live;      // int64 [n_live]: live dofs of the coarsest level
-  DevBuf X;         // FP64 [n_live][n_live] inverse Cholesky factor
+  DevBuf X;         // FP64 [n_live][n_live] inverse Cholesky factor, or the banded factor (band)
   DevBuf A, live_of, bits;  // set-up scratch kept for the next rebuild
+  bool band = false;        // coarsest factor banded (n_live above the dense limit)
+  int bw = 0;               // its bandwidth in the live-dof numbering
   double setup_s = 0.0;
   bool setup_reported = false;
   bool valid = false;
@@ -551,11 +554,18 @@ void coarsest_solve(tf_handle* h, Hierarchy& hy, VBufs<T>& vb, int ncol, const i
   dim3 g1 = cols_grid(n, ncol);
   coarsest_gather_kernel<T><<<g1, 256, 0, st>>>(b, nd, hy.live.as<long long>(), n, h->cb.as<double>(), active);
   TF_LAUNCH_CHECK("coarsest_gather_kernel");
-  const size_t need = dense_trimul_work(n, ncol);
-  if (h->trimul_work.bytes < need) h->trimul_work.alloc(need);
-  dense_trimul(hy.X.as<double>(), h->cb.as<double>(), h->cy.as<double>(), n, ncol, 0, active, h->trimul_work.as<double>(), st);
-  dense_trimul(hy.X.as<double>(), h->cy.as<double>(), h->cb.as<double>(), n, ncol, 1, active, h->trimul_work.as<double>(), st);
-  coarsest_scatter_kernel<T><<<g1, 256, 0, st>>>(h->cb.as<double>(), hy.live.as<long long>(), n, x, nd, active, store_round(h));
+  const double* solved = h->cb.as<double>();
+  if (hy.band) {
+    // forward and backward substitution with the banded factor, one CTA per column
+    band_solve(hy.X.as<double>(), n, hy.bw, h->cb.as<double>(), h->cy.as<double>(), ncol, st);
+    solved = h->cy.as<double>();
+  } else {
+    const size_t need = dense_trimul_work(n, ncol);
+    if (h->trimul_work.bytes < need) h->trimul_work.alloc(need);
+    dense_trimul(hy.X.as<double>(), h->cb.as<double>(), h->cy.as<double>(), n, ncol, 0, active, h->trimul_work.as<double>(), st);
+    dense_trimul(hy.X.as<double>(), h->cy.as<double>(), h->cb.as<double>(), n, ncol, 1, active, h->trimul_work.as<double>(), st);
+  }
+  coarsest_scatter_kernel<T><<<g1, 256, 0, st>>>(solved, hy.live.as<long long>(), n, x, nd, active, store_round(h));
   TF_LAUNCH_CHECK("coarsest_scatter_kernel");
 }
 
@@ -778,9 +788,38 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
         live.push_back(3 * n + a);
       }
   const long long nl = static_cast<long long>(live.size());
-  if (nl > DENSE_LIMIT)
-    throw Error(TF_INVALID, "coarsest grid has " + std::to_string(nl) + " live dofs; the dense coarsest factor allows at most " +
-                                std::to_string(DENSE_LIMIT) + " (raise max_levels or lower coarsest_dofs)");
+  // above the dense limit the coarsest factor is banded: its bandwidth is the largest live-index
+  // distance between two coupled dofs (nodes within one step of each other)
+  hy.band = nl > DENSE_LIMIT;
+  hy.bw = 0;
+  if (hy.band) {
+    long long bw = 0;
+    for (long long t = 0; t < nl; ++t) {
+      const long long node = live[t] / 3;
+      int i, j, k;
+      {
+        const long long r = node / cl.g.nz;
+        k = static_cast<int>(node - r * cl.g.nz);
+        j = static_cast<int>(r % cl.g.ny);
+        i = static_cast<int>(r / cl.g.ny);
+      }
+      for (int di = -1; di <= 1; ++di)
+        for (int dj = -1; dj <= 1; ++dj)
+          for (int dk = -1; dk <= 1; ++dk) {
+            const int ni = i + di, nj = j + dj, nk = k + dk;
+            if (ni < 0 || nj < 0 || nk < 0 || ni >= cl.g.nx || nj >= cl.g.ny || nk >= cl.g.nz) continue;
+            const long long m = ((long long)ni * cl.g.ny + nj) * cl.g.nz + nk;
+            for (int q = 0; q < 3; ++q) {
+              const int col = live_of[3 * m + q];
+              if (col >= 0) bw = std::max(bw, std::abs(t - col));
+            }
+          }
+    }
+    require(8.0 * (double)nl * (double)(bw + 1) <= BAND_LIMIT_BYTES,
+            "coarsest grid has " + std::to_string(nl) + " live dofs with bandwidth " + std::to_string(bw) +
+                ": its banded factor exceeds 32 GB (raise max_levels or lower coarsest_dofs)");
+    hy.bw = static_cast<int>(bw);
+  }
   hy.n_live = static_cast<int>(nl);
   int* info = reinterpret_cast<int*>(h->scal.as<double>() + 8);
   if (nl > 0) {
@@ -790,16 +829,25 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     dlive_of.ensure(sizeof(int) * cl.ndof);
     TF_CUDA_CHECK(cudaMemcpyAsync(dlive_of.p, live_of.data(), sizeof(int) * cl.ndof, cudaMemcpyHostToDevice, st));
     DevBuf& A = hy.A;
-    A.ensure(sizeof(double) * nl * nl);
-    TF_CUDA_CHECK(cudaMemsetAsync(A.p, 0, A.bytes, st));
-    coarsest_assemble_kernel<<<grid_for(nl, 128), 128, 0, st>>>(cl.g, cl.blocks64.as<double>(), dlive_of.as<int>(),
-                                                                hy.live.as<long long>(), static_cast<int>(nl), A.as<double>());
-    TF_LAUNCH_CHECK("coarsest_assemble_kernel");
-    dense_symmetrize(A.as<double>(), static_cast<int>(nl), st);
-    TF_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int), st));
-    hy.X.ensure(sizeof(double) * nl * nl);
-    const size_t fwork = dense_factor_work(static_cast<int>(nl));
-    if (h->factor_work.bytes < fwork) h->factor_work.alloc(fwork);
+    if (hy.band) {
+      hy.X.ensure(sizeof(double) * nl * (size_t)(hy.bw + 1));
+      TF_CUDA_CHECK(cudaMemsetAsync(hy.X.p, 0, hy.X.bytes, st));
+      coarsest_assemble_band_kernel<<<grid_for(nl, 128), 128, 0, st>>>(cl.g, cl.blocks64.as<double>(), dlive_of.as<int>(),
+                                                                       hy.live.as<long long>(), static_cast<int>(nl), hy.bw,
+                                                                       hy.X.as<double>());
+      TF_LAUNCH_CHECK("coarsest_assemble_band_kernel");
+    } else {
+      A.ensure(sizeof(double) * nl * nl);
+      TF_CUDA_CHECK(cudaMemsetAsync(A.p, 0, A.bytes, st));
+      coarsest_assemble_kernel<<<grid_for(nl, 128), 128, 0, st>>>(cl.g, cl.blocks64.as<double>(), dlive_of.as<int>(),
+                                                                  hy.live.as<long long>(), static_cast<int>(nl), A.as<double>());
+      TF_LAUNCH_CHECK("coarsest_assemble_kernel");
+      dense_symmetrize(A.as<double>(), static_cast<int>(nl), st);
+      TF_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int), st));
+      hy.X.ensure(sizeof(double) * nl * nl);
+      const size_t fwork = dense_factor_work(static_cast<int>(nl));
+      if (h->factor_work.bytes < fwork) h->factor_work.alloc(fwork);
+    }
     if (!h->side) {
       TF_CUDA_CHECK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
       TF_CUDA_CHECK(cudaEventCreateWithFlags(&h->side_fork, cudaEventDisableTiming));
@@ -807,7 +855,8 @@ void build_hierarchy(tf_handle* h, uint64_t key, Hierarchy& hy, cudaStream_t st)
     }
     TF_CUDA_CHECK(cudaEventRecord(h->side_fork, st));
     TF_CUDA_CHECK(cudaStreamWaitEvent(h->side, h->side_fork, 0));
-    dense_cholesky_inverse(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), info, h->factor_work.as<double>(), h->side);
+    if (hy.band) band_cholesky(hy.X.as<double>(), static_cast<int>(nl), hy.bw, info, h->side);
+    else dense_cholesky_inverse(A.as<double>(), hy.X.as<double>(), static_cast<int>(nl), info, h->factor_work.as<double>(), h->side);
     TF_CUDA_CHECK(cudaEventRecord(h->side_join, h->side));
   }
   // lambda_max(D^-1 A) of every smoothed level, in the work precision

@@ -222,3 +222,41 @@ def test_sixteen_bit_storage_refuses_the_tensor_core_apply(cuda):
     k0 = hex8.element_matrices((1, 1, 1), 0.3)[0]
     with pytest.raises(ValueError, match="tensor_cores"):
         GeometricMultigrid((8, 4, 4), (1, 1, 1), k0, {"precision": "bfloat16", "tensor_cores": True})
+
+
+def test_banded_coarsest_factor(cuda):
+    """A coarsest grid above the dense limit (24,000 live dofs) is factored banded.  With
+    coarsest_dofs = 40,000 the 56 x 56 x 24 cantilever keeps two levels, the coarsest with about
+    32,800 live dofs; its solve equals the default hierarchy's (dense coarsest factor, more levels,
+    itself held to direct solves above), and a batched solve of it next to a dense-coarsest instance
+    equals the two own solves."""
+    import torch
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid, solve_batch_device
+    shape = (56, 56, 24)
+    k0, _, moduli, fixed, force = cantilever(shape)
+    rng = np.random.default_rng(11)
+    forces = np.column_stack([force, rng.normal(size=force.size)])
+    band = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 40000, "tolerance": 1e-10})
+    dense = GeometricMultigrid(shape, (1, 1, 1), k0, {"tolerance": 1e-10})
+    for mg in (band, dense):
+        mg.update(moduli)
+    u_band, rep_band = band.solve("clamped", fixed, forces)
+    u_dense, rep_dense = dense.solve("clamped", fixed, forces)
+    assert rep_band["converged"] and rep_dense["converged"]
+    assert rep_band["levels"] == 2 and rep_band["coarsest_dofs"] > 24000
+    assert rep_dense["levels"] > 2 and rep_dense["coarsest_dofs"] <= 8000
+    for c in range(forces.shape[1]):
+        assert np.linalg.norm(u_band[:, c] - u_dense[:, c]) < 1e-7 * np.linalg.norm(u_dense[:, c])
+    small_shape = (16, 8, 8)
+    k1, _, m1, f1, g1 = cantilever(small_shape, seed=3)
+    small = GeometricMultigrid(small_shape, (1, 1, 1), k1, {"coarsest_dofs": 200, "tolerance": 1e-10})
+    small.update(m1)
+    jobs = [(band, "clamped", fixed, torch.as_tensor(forces.T.copy(), device="cuda")),
+            (small, "clamped", f1, torch.as_tensor(g1[None, :].copy(), device="cuda"))]
+    own = [mg.solve_device(key, fx, f) for mg, key, fx, f in jobs]
+    batched = solve_batch_device(jobs)
+    for (a, _), (b, rep) in zip(own, batched):
+        assert rep["converged"]
+        assert float((a - b).norm() / a.norm()) < 1e-7
+    for mg in (band, dense, small):
+        mg.close()
