@@ -54,7 +54,7 @@ def parse(argv=None):
     ap.add_argument("--pcg", default="float64", choices=["float64", "float32"],
                     help="fast path's PCG iterations: FP64, or FP32 with FP64 reliable residual updates")
     ap.add_argument("--tensor-cores", action="store_true", help="fast path's finest-level V-cycle applies on tcgen05")
-    ap.add_argument("--fine-tz", type=int, default=0, choices=[0, 8, 9],
+    ap.add_argument("--fine-tz", type=int, default=0, choices=[0, 7, 8, 9],
                     help="node-tile height of the finest-level operator in both arms (0: the library's choice)")
     ap.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 arm (default min(steps, 3))")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 arm")

@@ -343,7 +343,9 @@ __device__ __forceinline__ void stage_tiles(T* __restrict__ s, const Geo& g, con
 // reads distinct banks; no index needs a runtime division.
 constexpr int FTXT = 4;   // threads along x
 template <typename T, int TZ> struct FineTile {
-  static constexpr int P = sizeof(T) == 4 ? (TZ == 8 ? 24 : 41) : (TZ == 8 ? 24 : 25);   // row pitch (elements)
+  // row pitch (elements): conflict-free warp reads for 8-high tiles; 7- and 9-high tiles mix x rows
+  // in a warp and reach two-way conflicts at best (7 high: rows packed, P = 9)
+  static constexpr int P = TZ == 7 ? 9 : (sizeof(T) == 4 ? (TZ == 8 ? 24 : 41) : (TZ == 8 ? 24 : 25));
 };
 
 template <typename T, int NPT, typename KC>
@@ -413,9 +415,9 @@ template <typename T, int SLOT, bool REFLECT, int TZ, int NPT, int RND, bool PCG
 __device__ __forceinline__ void fine_level_body(const VGrid vg_, const LevelArgs<T>& a, int mode, TileMap tm, int cpb) {
   TF_VGRID(vg_);
   static_assert(!PCG || sizeof(T) == 8, "the fused PCG step is an FP64 operator");
-  constexpr int FMAXH = NPT == 1 ? 3 : 4;   // halo nodes staged per thread and column
   constexpr int TXN = FTXT * NPT;                 // tile nodes along x
   constexpr int SHX = TXN + 2, SHY = TY + 2;      // staged halo extents
+  constexpr int FMAXH = (SHX * SHY * (TZ + 2) + FTXT * TY * TZ - 1) / (FTXT * TY * TZ);   // halo nodes staged per thread
   constexpr int P = FineTile<T, TZ>::P;
   constexpr int PLANE = SHX * SHY * P;
   constexpr int SEX = TXN + 1, SEY = TY + 1, SEZ = TZ + 1;

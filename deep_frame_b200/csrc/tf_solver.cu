@@ -457,10 +457,12 @@ void launch_fine_tc(tf_handle* h, const LevelArgs<float>& a, int mode, cudaStrea
 // 8-high node tiles unless 9-high ones pad at least 15 % fewer threads along z: the 9-high
 // variants spill registers at two CTAs per SM.  Measured: on the 352 x 352 x 48 plate (49 node
 // planes: 56 padded with 8, 54 with 9) the 8-high FP32 apply is 17 % faster; on the 96 x 96 x 16
-// plate (17 planes: 24 against 18) the 9-high one is 10 % faster.
-bool fine_nine(const tf_handle* h, int nz) {
-  return h->k0_reflect &&
-         (h->s.fine_tz == 9 || (h->s.fine_tz == 0 && 100 * (((nz + 8) / 9) * 9) < 85 * (((nz + 7) / 8) * 8)));
+// plate (17 planes: 24 against 18) the 9-high one is 10 % faster.  7-high tiles only on request
+// (settings.fine_tz = 7).
+int fine_tile_height(const tf_handle* h, int nz) {
+  if (!h->k0_reflect) return 8;
+  if (h->s.fine_tz == 7 || h->s.fine_tz == 8 || h->s.fine_tz == 9) return h->s.fine_tz;
+  return 100 * (((nz + 8) / 9) * 9) < 85 * (((nz + 7) / 8) * 8) ? 9 : 8;
 }
 
 // Per-column count of the FP64 finest-level operator's curvature partials: its tiles (one node per
@@ -480,11 +482,14 @@ void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st)
     }
   }
   const int slot = k0_slot(h);
-  const bool nine = fine_nine(h, a.g.nz);
+  const int tz = fine_tile_height(h, a.g.nz);
   if (h->k0_reflect) {
-    if (nine) {
+    if (tz == 9) {
       if (slot == 0) launch_fine_variant<T, 0, true, 9>(a, mode, st);
       else launch_fine_variant<T, 1, true, 9>(a, mode, st);
+    } else if (tz == 7) {
+      if (slot == 0) launch_fine_variant<T, 0, true, 7>(a, mode, st);
+      else launch_fine_variant<T, 1, true, 7>(a, mode, st);
     } else {
       if (slot == 0) launch_fine_variant<T, 0, true, 8>(a, mode, st);
       else launch_fine_variant<T, 1, true, 8>(a, mode, st);
@@ -963,7 +968,7 @@ void fine_apply64_curvature(tf_handle* h, Hierarchy& hy, const double* p, double
   a.colstride = 3 * a.g.nnode;
   a.ncol = ncol;
   a.active = active;
-  const size_t need = sizeof(double) * (size_t)fine_dot_stride(h, fine_nine(h, a.g.nz) ? 9 : 8) * ncol;
+  const size_t need = sizeof(double) * (size_t)fine_dot_stride(h, fine_tile_height(h, a.g.nz)) * ncol;
   if (h->dotp.bytes < need) h->dotp.alloc(need);
   a.dot_out = h->dotp.as<double>();
   launch_level<double>(h, 0, a, MODE_APPLY, s, TIMER_FINE64);
@@ -1057,7 +1062,7 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
     {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
   if constexpr (fused) {
-    pcg_alpha_sum_kernel<<<ncol, RED_THREADS, 0, s>>>(h->dotp.as<double>(), fine_dot_stride(h, fine_nine(h, h->geo[0].nz) ? 9 : 8), st);
+    pcg_alpha_sum_kernel<<<ncol, RED_THREADS, 0, s>>>(h->dotp.as<double>(), fine_dot_stride(h, fine_tile_height(h, h->geo[0].nz)), st);
     TF_LAUNCH_CHECK("pcg_alpha_sum_kernel");
   } else {
     pcg_alpha_kernel<R><<<gr, RED_THREADS, 0, s>>>(p, q, n, st);
@@ -1174,7 +1179,7 @@ void validate_settings(const tf_settings& s) {
   require(s.pcg_precision == TF_PRECISION_FLOAT64 || s.precision != TF_PRECISION_FLOAT64,
           "float32 PCG iterations need the float32 work precision");
   require(std::isfinite(s.reliable) && s.reliable > 0 && s.reliable < 1, "reliable must be in (0, 1)");
-  require(s.fine_tz == 0 || s.fine_tz == 8 || s.fine_tz == 9, "fine_tz must be 0, 8 or 9");
+  require(s.fine_tz == 0 || s.fine_tz == 7 || s.fine_tz == 8 || s.fine_tz == 9, "fine_tz must be 0, 7, 8 or 9");
 }
 
 }  // namespace

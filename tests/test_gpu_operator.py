@@ -80,3 +80,31 @@ def test_element_energy_matches_oracle(cuda):
     assert padded.shape == (4,) + mg.padded
     assert np.max(np.abs(padded[:, :shape[0], :shape[1], :shape[2]].reshape(4, -1) - expected)) < 1e-12 * np.max(np.abs(expected))
     mg.close()
+
+
+@pytest.mark.parametrize("fine_tz", [7, 8, 9])
+def test_tile_heights_give_the_same_operator(cuda, fine_tz):
+    """Every finest-level tile height (7, 8, 9 nodes along z; a tuning choice) applies the same
+    FP64 operator (1e-12 vs the assembled matrix) and gives the same FP32-V-cycle PCG solve."""
+    from deep_frame_b200.topology_multigrid import GeometricMultigrid
+    shape = (12, 10, 20)
+    k0, _, _ = hex8.element_matrices((1, 1, 1), 0.3)
+    moduli = _moduli(shape, 4, 0.05)
+    matrix = op.assemble(shape, k0, moduli)
+    vectors = np.random.default_rng(5).normal(size=(matrix.shape[0], 3))
+    vectors[~op.live_dofs(shape, moduli)] = 0
+    mg = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 300, "fine_tz": fine_tz, "tolerance": 1e-10})
+    mg.update(moduli)
+    expected = matrix @ vectors
+    assert np.linalg.norm(mg.product(vectors) - expected) < 1e-12 * np.linalg.norm(expected)
+    fixed_nodes = np.flatnonzero(hex8.node_points(shape, (1, 1, 1))[:, 0] == 0)
+    fixed = (3 * fixed_nodes[:, None] + np.arange(3)).ravel()
+    forces = np.random.default_rng(6).normal(size=(matrix.shape[0], 2))
+    u, report = mg.solve("x0", fixed, forces)
+    ref = GeometricMultigrid(shape, (1, 1, 1), k0, {"coarsest_dofs": 300, "fine_tz": 8, "tolerance": 1e-10})
+    ref.update(moduli)
+    u8, report8 = ref.solve("x0", fixed, forces)
+    assert report["converged"] and abs(report["iterations"][0] - report8["iterations"][0]) <= 1
+    assert np.linalg.norm(u - u8) < 1e-8 * np.linalg.norm(u8)
+    mg.close()
+    ref.close()
