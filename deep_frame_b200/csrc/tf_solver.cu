@@ -457,12 +457,17 @@ void launch_fine_tc(tf_handle* h, const LevelArgs<float>& a, int mode, cudaStrea
 // 8-high node tiles unless 9-high ones pad at least 15 % fewer threads along z: the 9-high
 // variants spill registers at two CTAs per SM.  Measured: on the 352 x 352 x 48 plate (49 node
 // planes: 56 padded with 8, 54 with 9) the 8-high FP32 apply is 17 % faster; on the 96 x 96 x 16
-// plate (17 planes: 24 against 18) the 9-high one is 10 % faster.  7-high tiles only on request
-// (settings.fine_tz = 7).
-int fine_tile_height(const tf_handle* h, int nz) {
+// plate (17 planes: 24 against 18) the 9-high one is 10 % faster.  The FP32 operator also takes
+// 7-high tiles where they pad at least 10 % fewer threads than 8-high ones (352 x 352 x 48: 49
+// planes exactly, 731 against 755 ms per evaluation); the FP64 operator does not (784 against
+// 672 ms there: its 7-high tiles are slower despite the padding).  settings.fine_tz forces one.
+int fine_tile_height(const tf_handle* h, int nz, bool fp64) {
   if (!h->k0_reflect) return 8;
   if (h->s.fine_tz == 7 || h->s.fine_tz == 8 || h->s.fine_tz == 9) return h->s.fine_tz;
-  return 100 * (((nz + 8) / 9) * 9) < 85 * (((nz + 7) / 8) * 8) ? 9 : 8;
+  const int pad8 = ((nz + 7) / 8) * 8, pad9 = ((nz + 8) / 9) * 9, pad7 = ((nz + 6) / 7) * 7;
+  if (100 * pad9 < 85 * pad8) return 9;
+  if (!fp64 && 10 * pad7 <= 9 * pad8) return 7;
+  return 8;
 }
 
 // Per-column count of the FP64 finest-level operator's curvature partials: its tiles (one node per
@@ -482,7 +487,7 @@ void launch_fine(tf_handle* h, const LevelArgs<T>& a, int mode, cudaStream_t st)
     }
   }
   const int slot = k0_slot(h);
-  const int tz = fine_tile_height(h, a.g.nz);
+  const int tz = fine_tile_height(h, a.g.nz, std::is_same<T, double>::value);
   if (h->k0_reflect) {
     if (tz == 9) {
       if (slot == 0) launch_fine_variant<T, 0, true, 9>(a, mode, st);
@@ -968,7 +973,7 @@ void fine_apply64_curvature(tf_handle* h, Hierarchy& hy, const double* p, double
   a.colstride = 3 * a.g.nnode;
   a.ncol = ncol;
   a.active = active;
-  const size_t need = sizeof(double) * (size_t)fine_dot_stride(h, fine_tile_height(h, a.g.nz)) * ncol;
+  const size_t need = sizeof(double) * (size_t)fine_dot_stride(h, fine_tile_height(h, a.g.nz, true)) * ncol;
   if (h->dotp.bytes < need) h->dotp.alloc(need);
   a.dot_out = h->dotp.as<double>();
   launch_level<double>(h, 0, a, MODE_APPLY, s, TIMER_FINE64);
@@ -1062,7 +1067,7 @@ PcgResult pcg(tf_handle* h, Hierarchy& hy, int ncol, const std::vector<int>& run
     {
   TimedRange tr_(h->timers, TIMER_VECTOR, s);
   if constexpr (fused) {
-    pcg_alpha_sum_kernel<<<ncol, RED_THREADS, 0, s>>>(h->dotp.as<double>(), fine_dot_stride(h, fine_tile_height(h, h->geo[0].nz)), st);
+    pcg_alpha_sum_kernel<<<ncol, RED_THREADS, 0, s>>>(h->dotp.as<double>(), fine_dot_stride(h, fine_tile_height(h, h->geo[0].nz, true)), st);
     TF_LAUNCH_CHECK("pcg_alpha_sum_kernel");
   } else {
     pcg_alpha_kernel<R><<<gr, RED_THREADS, 0, s>>>(p, q, n, st);

@@ -78,8 +78,8 @@ typedef struct tf_settings {
                                  precision): FP32 PCG iterations and operator, x in FP64, FP64 true residuals replacing the
                                  iterated one (reliable updates) and deciding convergence; no counterpart in the reference */
   int32_t fine_tz;            /* node-tile height (along z) of the finest-level operator: 7, 8, 9, or 0 = 8 unless 9 pads
-                                 at least 15 % fewer threads along z (the 9-high variants spill registers); a tuning
-                                 choice that never changes results */
+                                 at least 15 % fewer threads along z (the 9-high variants spill registers) or, for the
+                                 FP32 operator, 7 pads at least 10 % fewer; a tuning choice that never changes results */
 } tf_settings;
 
 /* Solve report (deep_frame/topology_multigrid.py:367-373).  Arrays are caller-owned. */
