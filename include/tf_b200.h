@@ -143,7 +143,7 @@ TF_API int tf_solve_guess(tf_handle* h, uint64_t key, const double* f_dev, int32
  * topology_multigrid.py:353-362).  Each instance needs its own handle; all share the element
  * stiffness ke and the V-cycle settings, run the FP64 PCG (pcg_precision float64) with V-cycles
  * on the CUDA-core operators, and solve their live columns as one block (settings.batch 0 or at
- * least that count).  One stream for all. */
+ * least that count).  One stream for all.  Each report's `seconds` is the whole batch's time. */
 TF_API int tf_solve_batch(tf_handle* const* handles, const uint64_t* keys, int32_t count, const double* const* f_dev,
                           const int32_t* nrhs, double* const* u_dev, tf_report* reports, void* stream);
 
