@@ -170,3 +170,17 @@ def test_cpu_leg_of_a_workload_beyond_the_host_measures_the_small_plate(monkeypa
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert seen == ["plate_96x96x16"] and line["config"]["workload"] == "plate_352x352x48"
     assert line["cpu_baseline"]["workload"] == "plate_96x96x16" and "not plate_352x352x48" in line["cpu_baseline"]["sample"]
+
+
+def test_options_of_the_side_benchmarks():
+    """The batch, tile-height and coarsest-size options parse and reach the solver settings."""
+    args = bench.parse(["--instances", "32", "--instance-sizes", "small", "--fine-tz", "7", "--coarsest-dofs", "80000"])
+    assert args.instances == 32 and args.instance_sizes == "small" and args.fine_tz == 7 and args.coarsest_dofs == 80000
+    assert bench.fast_settings(args)["fine_tz"] == 7
+    schedule = bench.schedule_settings(args.schedule, args.coarsest_dofs)
+    assert schedule["coarsest_dofs"] == 80000 and schedule["smoother"] == "chebyshev"
+    assert "coarsest_dofs" not in bench.schedule_settings(args.schedule, 0)
+    defaults = bench.parse([])
+    assert defaults.instance_sizes == "plate" and defaults.fine_tz == 0 and defaults.learned_epochs == 4
+    with pytest.raises(SystemExit):
+        bench.parse(["--fine-tz", "6"])
