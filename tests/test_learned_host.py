@@ -2,6 +2,7 @@
 policy that drops it when it stops saving PCG iterations.  No GPU (the layers are tested on the
 device by test_gpu_learned.py)."""
 import numpy as np
+import pytest
 
 from deep_frame_b200 import learned
 
@@ -44,3 +45,19 @@ def test_guess_policy_drops_the_network_once_it_stops_saving_iterations():
     assert not learned.GuessPolicy(net=None).assess(165.93, 165.94)
     assert not learned.GuessPolicy(net=None).assess(20, 25, seconds_with=1.9, seconds_without=0.8)
     assert learned.GuessPolicy(net=None).assess(20, 25, seconds_with=0.6, seconds_without=0.8)
+
+
+def test_network_layers_for_any_depth_match_the_oracle_network():
+    """The layer list of a four-level network (two convolutions per encoder level, one per decoder
+    level, a linear head) is the one the oracle's forward pass consumes, in the same order."""
+    import torch
+    from oracle import learned as olearn
+    net = learned.GuessNet(channels=(16, 32, 48, 64), seed=0, device="cpu")
+    assert net.specs == [(5, 16, 1), (16, 16, 1), (16, 32, 1), (32, 32, 1), (32, 48, 1), (48, 48, 1), (48, 64, 1), (64, 64, 1),
+                         (112, 48, 1), (80, 32, 1), (48, 16, 1), (16, 3, 0)]
+    shape = (9, 7, 5)
+    params = [(torch.tensor(w.numpy(), dtype=torch.float64), torch.tensor(b.numpy(), dtype=torch.float64)) for w, b in net.params]
+    y = olearn.forward(params, torch.zeros((5, int(np.prod(shape))), dtype=torch.float64), shape, net.channels)
+    assert tuple(y.shape) == (3, int(np.prod(shape)))
+    with pytest.raises(ValueError):
+        learned.GuessNet(channels=(16,), device="cpu")
